@@ -1,0 +1,376 @@
+"""Benchmark: batched uneven-size Cholesky + cho_solve, matrices per second.
+
+Workload (the batched leg of the headline metric): 100,000 SPD matrices per
+GPU, n_i uniform in [8, 128], A_i = G G^T / n + n I with G iid N(0,1), 4
+right-hand sides iid N(0,1), float64.  One step = one pass of the batched
+factor + solve over the whole batch (plan built once, outside the timing).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own 100,000-matrix shard (weak
+scaling, no collective on the data path); the time is the max over ranks.
+
+Printed: one JSON line on rank 0 with the metric, the device-timed value
+(inputs resident in HBM), the end-to-end value through the public API with
+host<->device copies, the roofline of the batched kernel against the
+measured HBM peak, and the oracle's CPU time on a bounded sample.
+`--impl reference` times numax's own CPU algorithm for the path (the oracle,
+a C restatement of numax's Array-tier cholesky + cholesky_solve run per
+matrix over all host cores) instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched uneven Cholesky+cho_solve throughput (100k SPD, n~U[8,128], 4 RHS)"
+UNIT = "matrices/s"
+COUNT = 100_000
+NMIN, NMAX, NRHS = 8, 128, 4
+SEED = 20260303
+PROFILE = os.path.join(ROOT, "profiles", "batched_potrf_f64_100k.md")
+
+
+def draw_sizes(count, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return rng.integers(NMIN, NMAX + 1, size=count).astype(np.int32)
+
+
+def make_batch_torch(ns, nrhs, dtype, device, seed):
+    """Ragged A (G G^T/n + n I per matrix) and B, generated size group by
+    size group with a seeded torch generator on `device`."""
+    import torch
+    from numax_b200.batched import ragged_offsets
+    a_off = torch.from_numpy(ragged_offsets(ns)).to(device)
+    total_a = int((ns.astype(np.int64) ** 2).sum())
+    total_b = int(ns.astype(np.int64).sum()) * nrhs
+    A = torch.empty(total_a, dtype=dtype, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    ns_t = torch.from_numpy(ns).to(device)
+    for n in np.unique(ns):
+        idx = torch.nonzero(ns_t == int(n)).flatten()
+        g = torch.randn((idx.numel(), int(n), int(n)), generator=gen, dtype=torch.float64,
+                        device=device)
+        m = g @ g.transpose(1, 2) / n + n * torch.eye(int(n), dtype=torch.float64, device=device)
+        pos = a_off[idx][:, None] + torch.arange(int(n) * int(n), device=device)[None, :]
+        A[pos.flatten()] = m.reshape(-1).to(dtype)
+        del g, m, pos
+    B = torch.randn(total_b, generator=gen, dtype=torch.float64, device=device).to(dtype)
+    return A, B
+
+
+def algorithmic_bytes(ns, nrhs, esize):
+    """Bytes one pass must move: read lower(A), write lower(L), read B,
+    write X (n*nrhs each), write info."""
+    n = ns.astype(np.int64)
+    return int((esize * (n * (n + 1) // 2 * 2 + 2 * nrhs * n)).sum() + 4 * len(ns))
+
+
+def algorithmic_flops(ns, nrhs):
+    n = ns.astype(np.float64)
+    return float((n ** 3 / 3 + 2 * nrhs * n ** 2).sum())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags)
+                          if f.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows)}
+
+
+def read_traffic():
+    """Per-launch DRAM bytes from the committed ncu summary, if any."""
+    try:
+        text = open(PROFILE).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline_sample(ns_all, seed, target_s=10.0):
+    """Oracle (numax's Array-tier algorithm, C, OpenMP over matrices) on a
+    bounded sample of the workload; returns (mats/s, threads, sample text)."""
+    from oracle import oracle as O
+    threads = O.max_threads()
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+
+    def sample(count):
+        ns = ns_all[:count]
+        mats, rhs = [], []
+        for n in ns:
+            g = rng.standard_normal((n, n))
+            mats.append((g @ g.T / n + n * np.eye(n)).ravel())
+            rhs.append(rng.standard_normal(n * NRHS))
+        return ns, np.concatenate(mats), np.concatenate(rhs)
+
+    ns, A, B = sample(min(2000, len(ns_all)))
+    t0 = time.perf_counter()
+    O.batched_cholesky_solve(ns, A, B, NRHS, want_l=True, threads=threads)
+    dt = time.perf_counter() - t0
+    count = int(min(len(ns_all), max(2000, 2000 * target_s / max(dt, 1e-6))))
+    count = min(count, 60000)
+    ns, A, B = sample(count)
+    t0 = time.perf_counter()
+    O.batched_cholesky_solve(ns, A, B, NRHS, want_l=True, threads=threads)
+    dt = time.perf_counter() - t0
+    return count / dt, threads, (f"first {count} matrices of the workload's size sequence, "
+                                 f"float64, {NRHS} RHS, one pass, {dt:.2f} s")
+
+
+def run_reference(args):
+    """numax's own CPU algorithm for the path (the oracle), rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import build as obuild, oracle as O
+    obuild.build()
+    threads = O.max_threads()
+    ns_all = draw_sizes(COUNT, SEED)
+    per_step = int(os.environ.get("NMX_REF_SAMPLE", "8000"))
+    rng = np.random.Generator(np.random.PCG64(SEED + 11))
+    ns = ns_all[:per_step]
+    mats, rhs = [], []
+    for n in ns:
+        g = rng.standard_normal((n, n))
+        mats.append((g @ g.T / n + n * np.eye(n)).ravel())
+        rhs.append(rng.standard_normal(n * NRHS))
+    A, B = np.concatenate(mats), np.concatenate(rhs)
+    for _ in range(args.warmup):
+        O.batched_cholesky_solve(ns, A, B, NRHS, want_l=True, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.batched_cholesky_solve(ns, A, B, NRHS, want_l=True, threads=threads)
+    dt = time.perf_counter() - t0
+    value = per_step * args.steps / dt
+    sample = (f"each step: first {per_step} matrices of the {COUNT}-matrix workload "
+              f"(n~U[8,128], float64, {NRHS} RHS), Array-tier cholesky+cholesky_solve per matrix")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (PCG64 seeded)",
+        "config": {"workload": "batched uneven Cholesky + cho_solve", "count": COUNT,
+                   "n_range": [NMIN, NMAX], "nrhs": NRHS, "parallelism": f"cpu{threads}",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import numax_b200 as nb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    esize = 8 if args.dtype == "f64" else 4
+
+    ns = draw_sizes(args.count, SEED + rank)
+    A, B = make_batch_torch(ns, NRHS, dtype, dev, SEED + 1000 * rank)
+    L = torch.empty_like(A)
+    X = torch.empty_like(B)
+    info = torch.empty(len(ns), dtype=torch.int32, device=dev)
+    plan = nb.CholeskySolveBatch(ns, nrhs=NRHS, dtype=dtype, device=dev)
+    launches_per_step = len(set(min(3, (int(n) - 1) // 32) for n in np.unique(ns)))
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(args.warmup, 3)):
+        plan.run(A, B, X, info, L)
+    torch.cuda.synchronize(dev)
+    bad = int((info != 0).sum().item())
+    if bad:
+        raise RuntimeError(f"{bad} matrices reported non-positive pivots")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-timed: inputs resident in HBM (A, L ~ 4.7 GB each >> L2) ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier()
+    with ClockSampler(local) as clocks:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for s in range(args.steps):
+            ev[s][0].record(stream)
+            plan.run(A, B, X, info, L)
+            ev[s][1].record(stream)
+        t_end.record(stream)
+        barrier()
+    total_s = max_over_ranks(t_start.elapsed_time(t_end) / 1e3)
+    launch_s = float(np.mean([a.elapsed_time(b) for a, b in ev])) / 1e3
+    value = world * len(ns) * args.steps / total_s
+
+    # ---- end to end through the public API: pinned host in, host out --------
+    hA = A.cpu().pin_memory()
+    hB = B.cpu().pin_memory()
+    hX = torch.empty(X.shape, dtype=dtype).pin_memory()
+    hI = torch.empty(info.shape, dtype=torch.int32).pin_memory()
+    dA = torch.empty_like(A)
+    dB = torch.empty_like(B)
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def e2e_step():
+        dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        plan(dA, dB, X, info, L)  # synchronous public call
+        hX.copy_(X, non_blocking=True)
+        hI.copy_(info, non_blocking=True)
+        stream.synchronize()
+
+    e2e_step()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_value = world * len(ns) * e2e_steps / e2e_s
+    h2d = (hA.numel() + hB.numel()) * esize
+    d2h = hX.numel() * esize + hI.numel() * 4
+    np.testing.assert_array_equal(hI.numpy(), 0)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    abytes = algorithmic_bytes(ns, NRHS, esize)
+    achieved = abytes / launch_s / 1e9
+    traffic = read_traffic()
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import build as obuild
+        obuild.build()
+        rate, threads, sample = cpu_baseline_sample(ns, SEED)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": total_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
+        "data": "synthetic (seeded torch generator, A=GG^T/n+nI, B~N(0,1))",
+        "config": {"workload": "batched uneven Cholesky + cho_solve", "count_per_gpu": len(ns),
+                   "n_range": [NMIN, NMAX], "nrhs": NRHS, "parallelism": f"shard{world}",
+                   "l2": "inputs larger than L2 (A and L %.1f GB each)" % (A.numel() * esize / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": abytes,
+                     "launch_ms": launch_s * 1e3,
+                     "fp_rate_tflops": algorithmic_flops(ns, NRHS) / launch_s / 1e12},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--count", type=int, default=COUNT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

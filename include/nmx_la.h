@@ -1,0 +1,110 @@
+/*
+ * nmx_la.h -- C ABI of the B200-native dense-factorization library
+ * (libnmxla.so, sm_100a).
+ *
+ * This is the boundary numax's Mojo host code binds through `external_call`
+ * (or any FFI: ctypes, cffi, a C/C++ caller).  Every entry point takes plain
+ * pointers and sizes; matrices are ROW-MAJOR with an explicit leading
+ * dimension, exactly as numax's `Tensor.tile()` views are
+ * (numax/core/tensor.mojo:636-660).  Pointers named as device pointers must
+ * be CUDA device (or managed) memory on the context's device.
+ *
+ * Return convention (LAPACK-like, numax's `info` semantics):
+ *     0        success
+ *    <0        -(1-based index of the first invalid argument); nothing was
+ *              launched
+ *    >0        a factorization's `info` where the entry point documents one
+ *              (otherwise info goes to a device word the caller reads)
+ *   NMX_ERR_*  a CUDA/runtime failure (large negative codes below)
+ * nmx_last_error_string() describes the most recent failure on the calling
+ * thread.
+ *
+ * Asynchrony: every call that takes a `stream` (a cudaStream_t passed as
+ * void*) enqueues work on it and returns without synchronizing, unless its
+ * comment says otherwise.  numax's calls are synchronous; the wrappers in
+ * the Python and Mojo front ends synchronize to keep that behaviour.
+ */
+#ifndef NMX_LA_H
+#define NMX_LA_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NMX_API __attribute__((visibility("default")))
+#else
+#define NMX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NMX_ERR_CUDA (-1000)       /* a CUDA runtime call failed */
+#define NMX_ERR_ALLOC (-1001)      /* device or host allocation failed */
+#define NMX_ERR_UNSUPPORTED (-1002)/* device is not sm_100 / feature absent */
+#define NMX_ERR_INTERNAL (-1003)   /* internal error (bounded wait expired, ...) */
+
+#define NMX_F32 0
+#define NMX_F64 1
+
+typedef struct nmx_context *nmx_ctx;
+typedef struct nmx_batched_plan_s *nmx_batched_plan;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  The context owns its workspace
+ * and cached plans; it is the stand-in for numax's DeviceContext
+ * (numax/core/tensorlike.mojo:116-126).  Not shared across threads without
+ * external locking. */
+NMX_API int nmx_create(int device, nmx_ctx *out);
+NMX_API int nmx_destroy(nmx_ctx ctx);
+/* Human-readable description of the last failure on this thread ("" if none). */
+NMX_API const char *nmx_last_error_string(void);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+NMX_API int nmx_version(void);
+
+/* ---- batched uneven-size Cholesky + cho_solve ---------------------------
+ *
+ * Replaces numax's `map_blocks[step=cholesky+cholesky_solve, gpu=True]`
+ * (numax/core/functional.mojo:691-834 over the Array-tier bodies
+ * numax/linalg/_array/cholesky.mojo:26-92), which runs one fixed-n problem
+ * per GPU thread with n <= 64 known at compile time.  Here n varies per
+ * matrix (1 <= n_i <= 128) and the batch is one plan.
+ *
+ * Ragged layout: matrix i is n_i x n_i row-major at element offset
+ * a_off[i] = sum_{j<i} n_j^2 of A; its right-hand sides are n_i x nrhs
+ * row-major at b_off[i] = sum_{j<i} n_j * nrhs of B and X.
+ *
+ * Semantics per matrix are the Array tier's: only the lower triangle of A_i
+ * is read; l_jj = sqrt(guard_nonzero(d, 1e-30)) (a negative pivot gives NaN,
+ * an exactly-zero one 1e-15); solves divide by guard_nonzero(l_ii, 1e-30).
+ * On return the lower triangle of L_i holds the factor (the upper triangle
+ * of L_i is not written; L may alias A for an in-place factorization),
+ * X_i = A_i^-1 B_i, and info[i] is the 1-based index of the first pivot
+ * d <= 0 (0 if none) -- the `info` rule of numax's potrf_diag
+ * (numax/linalg/panel.mojo:216-286), which the Array tier lacks.
+ */
+
+/* Build a plan: sorts the batch by size, picks per-bucket schedules from the
+ * autotune table, uploads the schedule.  n_host: count sizes on the HOST.
+ * dtype: NMX_F32 / NMX_F64.  nrhs: 0..8. */
+NMX_API int nmx_potrf_potrs_batched_plan(nmx_ctx ctx, int dtype, int64_t count, const int32_t *n_host,
+                                 int nrhs, nmx_batched_plan *out);
+NMX_API int nmx_batched_plan_destroy(nmx_batched_plan plan);
+/* Elements of A (sum n_i^2) and of B/X (sum n_i*nrhs) the plan expects. */
+NMX_API int nmx_batched_plan_sizes(nmx_batched_plan plan, int64_t *a_elems, int64_t *b_elems);
+
+/* Run the plan on device buffers.  A and B are read; L (lower triangles),
+ * X and info (count int32) are written.  L may alias A, X may alias B. */
+NMX_API int nmx_potrf_potrs_batched_f64(nmx_ctx ctx, nmx_batched_plan plan, const double *A,
+                                        double *L, const double *B, double *X, int32_t *info,
+                                        void *stream);
+NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A,
+                                        float *L, const float *B, float *X, int32_t *info,
+                                        void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NMX_LA_H */

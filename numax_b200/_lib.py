@@ -1,0 +1,100 @@
+"""ctypes binding of libnmxla.so, the sm_100a library behind numax_b200.
+
+Every compute call goes through the C ABI declared in include/nmx_la.h.
+There is no CPU fallback: if the shared library is missing or no sm_100
+device is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnmxla.so")
+
+NMX_F32 = 0
+NMX_F64 = 1
+NMX_ERR_CUDA = -1000
+NMX_ERR_ALLOC = -1001
+NMX_ERR_UNSUPPORTED = -1002
+NMX_ERR_INTERNAL = -1003
+
+_lock = threading.Lock()
+_lib = None
+
+vp = C.c_void_p
+i32 = C.c_int32
+i64 = C.c_int64
+ci = C.c_int
+
+# name -> (restype, argtypes); mirrors include/nmx_la.h
+SIGNATURES = {
+    "nmx_create": (ci, [ci, C.POINTER(vp)]),
+    "nmx_destroy": (ci, [vp]),
+    "nmx_last_error_string": (C.c_char_p, []),
+    "nmx_version": (ci, []),
+    "nmx_potrf_potrs_batched_plan": (ci, [vp, ci, i64, vp, ci, C.POINTER(vp)]),
+    "nmx_batched_plan_destroy": (ci, [vp]),
+    "nmx_batched_plan_sizes": (ci, [vp, C.POINTER(i64), C.POINTER(i64)]),
+    "nmx_potrf_potrs_batched_f64": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "nmx_potrf_potrs_batched_f32": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
+}
+
+
+class NmxError(RuntimeError):
+    """A failure reported by libnmxla (argument error or CUDA failure)."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed ({code}): {msg}")
+        self.code = code
+
+
+def load() -> C.CDLL:
+    """Load libnmxla.so (building nothing: it must have been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `python -m numax_b200.build` "
+                    "(numax_b200 has no CPU fallback)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    s = load().nmx_last_error_string()
+    return s.decode() if s else ""
+
+
+def check(fn: str, code: int) -> int:
+    """Raise NmxError on a negative status; return info (>= 0) otherwise."""
+    if code < 0:
+        raise NmxError(fn, code, last_error())
+    return code
+
+
+def call(name: str, *args) -> int:
+    return check(name, getattr(load(), name)(*args))
+
+
+_contexts: dict[int, int] = {}
+
+
+def context(device: int) -> int:
+    """The process-wide nmx context of CUDA device `device` (created lazily)."""
+    with _lock:
+        h = _contexts.get(device)
+    if h is None:
+        out = vp()
+        call("nmx_create", device, C.byref(out))
+        with _lock:
+            _contexts.setdefault(device, out.value)
+            h = _contexts[device]
+    return h

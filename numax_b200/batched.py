@@ -1,0 +1,141 @@
+"""Batched uneven-size factorizations over ragged batches on one B200.
+
+The numax spelling of a batch of small Cholesky solves is
+`map_blocks[step=solve_step, gpu=True](problems, out)` with the Array-tier
+`cholesky` + `cholesky_solve` inside `step`
+(numax/core/functional.mojo:691-834; examples/advanced/batched_solve.mojo:
+75-104): one fixed, compile-time n <= 64 per launch, one problem per GPU
+thread.  Here a batch holds matrices of different orders (1..128) in a
+ragged row-major layout and runs as one plan:
+
+    plan = CholeskySolveBatch(ns, nrhs=4, dtype=torch.float64)
+    L_in_A, X, info = plan(A, B)          # A, B: flat CUDA tensors
+
+Ragged layout: matrix i occupies A[a_off[i] : a_off[i] + n_i*n_i] row-major,
+a_off = exclusive prefix sum of n_i^2; its right-hand sides occupy
+B[b_off[i] : b_off[i] + n_i*nrhs] row-major (n_i x nrhs), b_off the prefix
+sum of n_i*nrhs.  `ragged_offsets` computes both.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_DT = {torch.float64: (_lib.NMX_F64, "f64"), torch.float32: (_lib.NMX_F32, "f32")}
+
+
+def ragged_offsets(ns, cols=None) -> np.ndarray:
+    """Element offsets of a ragged batch: matrix i is n_i x (cols or n_i)."""
+    ns = np.asarray(ns, dtype=np.int64)
+    sizes = ns * (ns if cols is None else cols)
+    off = np.zeros(len(ns), dtype=np.int64)
+    if len(ns) > 1:
+        off[1:] = np.cumsum(sizes)[:-1]
+    return off
+
+
+def _resolve_device(device) -> torch.device:
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise ValueError(f"numax_b200 runs on CUDA devices only, not {device}")
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    return device
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _check_tensor(name, t, dtype, numel, device):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if t.device != device:
+        raise ValueError(f"{name} is on {t.device}, expected {device}")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} has dtype {t.dtype}, expected {dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() < numel:
+        raise ValueError(f"{name} has {t.numel()} elements, the batch needs {numel}")
+
+
+class CholeskySolveBatch:
+    """A reusable plan for `cholesky` + `cholesky_solve` over a ragged batch.
+
+    Per matrix the arithmetic follows numax's Array tier
+    (numax/linalg/_array/cholesky.mojo:26-92): only the lower triangle of A_i
+    is read, the diagonal is floored by guard_nonzero(d, 1e-30) before the
+    square root (so a negative pivot yields NaN rather than raising), and the
+    solves divide by guard_nonzero(l_ii, 1e-30).  On top of numax, `info[i]`
+    reports the first pivot d <= 0 (1-based; 0 = positive definite), the
+    rule of numax's potrf_diag (numax/linalg/panel.mojo:216-286).
+    """
+
+    def __init__(self, ns, nrhs: int = 4, dtype=torch.float64, device=None):
+        if dtype not in _DT:
+            raise TypeError("dtype must be torch.float32 or torch.float64")
+        self.device = _resolve_device(device)
+        self.dtype = dtype
+        self.nrhs = int(nrhs)
+        self.ns = np.ascontiguousarray(ns, dtype=np.int32)
+        self.count = int(self.ns.size)
+        self._ctx = _lib.context(self.device.index)
+        h = C.c_void_p()
+        code, self._suffix = _DT[dtype]
+        _lib.call("nmx_potrf_potrs_batched_plan", self._ctx, code, self.count,
+                  self.ns.ctypes.data if self.count else None, self.nrhs, C.byref(h))
+        self._plan = h.value
+        a, b = C.c_int64(), C.c_int64()
+        _lib.call("nmx_batched_plan_sizes", self._plan, C.byref(a), C.byref(b))
+        self.a_elems, self.b_elems = a.value, b.value
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan:
+            try:
+                _lib.load().nmx_batched_plan_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    def run(self, A: torch.Tensor, B: torch.Tensor | None, X: torch.Tensor | None = None,
+            info: torch.Tensor | None = None, L: torch.Tensor | None = None):
+        """Enqueue on the current stream.  The factors' lower triangles go to
+        L (default: A itself, in place; the upper triangles are not written).
+        Returns (L, X, info) without synchronizing."""
+        _check_tensor("A", A, self.dtype, self.a_elems, self.device)
+        if L is None:
+            L = A
+        _check_tensor("L", L, self.dtype, self.a_elems, self.device)
+        if self.nrhs:
+            _check_tensor("B", B, self.dtype, self.b_elems, self.device)
+            if X is None:
+                X = torch.empty(self.b_elems, dtype=self.dtype, device=self.device)
+            _check_tensor("X", X, self.dtype, self.b_elems, self.device)
+        if info is None:
+            info = torch.empty(self.count, dtype=torch.int32, device=self.device)
+        _check_tensor("info", info, torch.int32, self.count, self.device)
+        _lib.call(f"nmx_potrf_potrs_batched_{self._suffix}", self._ctx, self._plan, A.data_ptr(),
+                  L.data_ptr(), B.data_ptr() if self.nrhs else None,
+                  X.data_ptr() if self.nrhs else None, info.data_ptr(), _stream_ptr(self.device))
+        return L, X, info
+
+    def __call__(self, A, B, X=None, info=None, L=None):
+        """Synchronous, like numax: factor (in place unless L is given),
+        solve, synchronize, return (L, X, info)."""
+        out = self.run(A, B, X, info, L)
+        torch.cuda.current_stream(self.device).synchronize()
+        return out
+
+
+def cholesky_solve_batched(ns, A, B, nrhs: int = 4):
+    """One-shot form: plan, run, synchronize.  Returns (A with L, X, info)."""
+    plan = CholeskySolveBatch(ns, nrhs=nrhs, dtype=A.dtype, device=A.device)
+    return plan(A, B)

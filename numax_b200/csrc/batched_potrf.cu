@@ -1,0 +1,471 @@
+// Batched uneven-size Cholesky + cho_solve (sm_100a).
+//
+// Replaces numax's map_blocks[step = cholesky + cholesky_solve, gpu=True]
+// (numax/core/functional.mojo:691-834 driving the Array-tier bodies
+// numax/linalg/_array/cholesky.mojo:26-92 and
+// numax/linalg/_array/triangular.mojo:24-63), which runs one fixed-n
+// problem per GPU thread out of registers.  Here each matrix of a ragged
+// batch (n_i in 1..128) is staged into shared memory and factored by a whole
+// CTA, blocked by 16 columns:
+//
+//   for each 16-column block k:
+//     one warp factors the 16x16 diagonal block and forms its inverse W,
+//     every thread solves rows of the panel below against W^T (a small GEMM),
+//     all threads apply the symmetric trailing update in 4x4 register tiles.
+//
+// The right-hand sides ride along as nrhs extra rows under the matrix, so the
+// forward substitution L y = b falls out of the panel solves for free; the
+// back substitution L^T x = y then walks the blocks upward reusing the
+// stored diagonal-block inverses.
+//
+// Scheduling: the plan sorts the batch by size (largest first) into buckets
+// by n; each bucket is a persistent grid sized by occupancy that pulls
+// matrices from an atomic work counter, so the big matrices start first and
+// the small ones fill the tail.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "nmx_common.cuh"
+
+namespace nmx {
+
+constexpr int kPotrfMaxN = 128;
+constexpr int kPotrfMaxRhs = 8;
+constexpr int kDiagNB = 16;
+
+struct BatchedPotrfArgs {
+    const int32_t *order;  // matrix indices, bucket-contiguous, largest first
+    const int32_t *ns;
+    const int64_t *a_off;
+    const int64_t *b_off;
+    const void *A;
+    void *L;
+    const void *B;
+    void *X;
+    int32_t *info;
+    int nrhs;
+};
+
+// Shared-memory words (of T) one CTA needs for matrices up to nmax.
+__host__ __device__ inline int potrf_smem_elems(int nmax, int nrhs) {
+    int ld = nmax | 1;
+    return (nmax + nrhs) * ld + nmax + kDiagNB * kPotrfMaxRhs;
+}
+
+// Factor the kb x kb diagonal block at (k, k) in place (lower), one warp.
+// Stores W = inverse of the block's L: W[i][j] (i > j) transposed into the
+// unused upper triangle at S[(k+j)*ld + k+i], W[j][j] = 1/l_jj in dinv[k+j].
+template <typename T>
+__device__ __forceinline__ void potrf_diag_warp(T *S, int ld, int k, int kb, T *dinv, int lane,
+                                                int *s_info) {
+    const T floor_ = pivot_floor<T>::value;
+    for (int j = 0; j < kb; ++j) {
+        T d = S[(k + j) * ld + k + j];
+        if (lane == 0 && d <= T(0) && *s_info == 0) *s_info = k + j + 1;
+        T ljj = sqrt(guard_nonzero(d, floor_));
+        __syncwarp();
+        if (lane > j && lane < kb) S[(k + lane) * ld + k + j] = S[(k + lane) * ld + k + j] / ljj;
+        if (lane == j) S[(k + j) * ld + k + j] = ljj;
+        __syncwarp();
+        if (lane > j && lane < kb) {
+            T lij = S[(k + lane) * ld + k + j];
+            for (int c = j + 1; c <= lane; ++c)
+                S[(k + lane) * ld + k + c] -= lij * S[(k + c) * ld + k + j];
+        }
+        __syncwarp();
+    }
+    // Column `lane` of W = L^-1: W[j][j] = 1/l_jj, W[i][j] = -(sum_{p=j}^{i-1} l_ip W[p][j]) / l_ii.
+    if (lane < kb) {
+        const int j = lane;
+        T w[kDiagNB];
+#pragma unroll
+        for (int i = 0; i < kDiagNB; ++i) w[i] = T(0);
+        T wjj = T(1) / guard_nonzero(S[(k + j) * ld + k + j], floor_);
+        dinv[k + j] = wjj;
+#pragma unroll
+        for (int i = 0; i < kDiagNB; ++i) {
+            if (i == j) w[i] = wjj;
+            if (i > j && i < kb) {
+                T s = T(0);
+#pragma unroll
+                for (int p = 0; p < kDiagNB; ++p)
+                    if (p >= j && p < i) s += S[(k + i) * ld + k + p] * w[p];
+                w[i] = -s / guard_nonzero(S[(k + i) * ld + k + i], floor_);
+                S[(k + j) * ld + k + i] = w[i];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <typename T, int NT>
+__device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *dinv, T *xb,
+                                int *s_info) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    const int n = args.ns[mi];
+    const int nrhs = args.nrhs;
+    const int ld = n | 1;
+    const int R = n + nrhs;  // rows of the augmented block [A; B^T]
+    const T *A = static_cast<const T *>(args.A) + args.a_off[mi];
+    T *L = static_cast<T *>(args.L) + args.a_off[mi];
+    const T *B = static_cast<const T *>(args.B) + args.b_off[mi];
+    T *X = static_cast<T *>(args.X) + args.b_off[mi];
+    if (tid == 0) *s_info = 0;
+
+    // Stage the lower triangle (row i: i+1 contiguous elements) and B^T.
+    for (int i = warp; i < n; i += NW)
+        for (int j = lane; j <= i; j += 32) S[i * ld + j] = A[(int64_t)i * n + j];
+    for (int e = tid; e < n * nrhs; e += NT) {
+        int j = e / nrhs, r = e - j * nrhs;
+        S[(n + r) * ld + j] = B[e];
+    }
+    __syncthreads();
+
+    for (int k = 0; k < n; k += kDiagNB) {
+        const int kb = min(kDiagNB, n - k);
+        if (warp == 0) potrf_diag_warp<T>(S, ld, k, kb, dinv, lane, s_info);
+        __syncthreads();
+
+        // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T.
+        const int r0 = k + kb;
+        for (int r = r0 + tid; r < R; r += NT) {
+            T a[kDiagNB];
+#pragma unroll
+            for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[r * ld + k + j] : T(0);
+#pragma unroll
+            for (int j = 0; j < kDiagNB; ++j) {
+                if (j < kb) {
+                    T out = a[j] * dinv[k + j];
+#pragma unroll
+                    for (int i = 0; i < kDiagNB; ++i)
+                        if (i < j) out += a[i] * S[(k + i) * ld + k + j];
+                    S[r * ld + k + j] = out;
+                }
+            }
+        }
+        __syncthreads();
+
+        // Trailing update of the augmented trapezoid: rows [r0, R), cols
+        // [r0, min(i+1, n)), S[i][j] -= sum_p S[i][k+p] S[j][k+p], 4x4 tiles.
+        const int TR = (int)ceil_div(R - r0, 4), TN = (int)ceil_div(n - r0, 4);
+        if (TN > 0) {
+            const int tri = TN * (TN + 1) / 2;
+            const int tiles = tri + (TR - TN) * TN;
+            for (int e = tid; e < tiles; e += NT) {
+                int ti, tj;
+                if (e < tri) {
+                    ti = (int)((sqrtf(8.f * e + 1.f) - 1.f) * 0.5f);
+                    while (ti * (ti + 1) / 2 > e) --ti;
+                    while ((ti + 1) * (ti + 2) / 2 <= e) ++ti;
+                    tj = e - ti * (ti + 1) / 2;
+                } else {
+                    int e2 = e - tri;
+                    ti = TN + e2 / TN;
+                    tj = e2 - (ti - TN) * TN;
+                }
+                const int i0 = r0 + 4 * ti, j0 = r0 + 4 * tj;
+                T acc[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+                int ir[4], jr[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    ir[a] = min(i0 + a, R - 1) * ld + k;
+                    jr[a] = min(j0 + a, n - 1) * ld + k;
+                }
+                for (int p = 0; p < kb; ++p) {
+                    T x[4], y[4];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        x[a] = S[ir[a] + p];
+                        y[a] = S[jr[a] + p];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+                }
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        int i = i0 + a, j = j0 + b;
+                        if (i < R && j < n && j <= i) S[i * ld + j] -= acc[a][b];
+                    }
+            }
+        }
+        __syncthreads();
+    }
+
+    // Rows n..n+nrhs of S now hold y^T = (L^-1 B)^T.  Back substitution
+    // L^T x = y, 16-row blocks bottom-up, with the stored block inverses.
+    for (int k = ((n - 1) / kDiagNB) * kDiagNB; k >= 0; k -= kDiagNB) {
+        const int kb = min(kDiagNB, n - k);
+        // x_blk = W^T y_blk, W the block's inverse.
+        if (tid < kb * nrhs) {
+            int j = tid / nrhs, c = tid - j * nrhs;
+            const T *y = S + (n + c) * ld + k;
+            T s = dinv[k + j] * y[j];
+            for (int i = j + 1; i < kb; ++i) s += S[(k + j) * ld + k + i] * y[i];
+            xb[j * kPotrfMaxRhs + c] = s;
+        }
+        __syncthreads();
+        if (tid < kb * nrhs) {
+            int j = tid / nrhs, c = tid - j * nrhs;
+            S[(n + c) * ld + k + j] = xb[j * kPotrfMaxRhs + c];
+        }
+        // y[0:k] -= L[k:k+kb, 0:k]^T x_blk
+        for (int e = tid; e < k * nrhs; e += NT) {
+            int i = e / nrhs, c = e - i * nrhs;
+            T s = T(0);
+            for (int j = 0; j < kb; ++j) s += S[(k + j) * ld + i] * xb[j * kPotrfMaxRhs + c];
+            S[(n + c) * ld + i] -= s;
+        }
+        __syncthreads();
+    }
+
+    // Write back L (lower triangle) and X.
+    for (int i = warp; i < n; i += NW)
+        for (int j = lane; j <= i; j += 32) L[(int64_t)i * n + j] = S[i * ld + j];
+    for (int e = tid; e < n * nrhs; e += NT) {
+        int j = e / nrhs, r = e - j * nrhs;
+        X[e] = S[(n + r) * ld + j];
+    }
+    if (tid == 0) args.info[mi] = *s_info;
+    __syncthreads();
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) potrf_potrs_batched_kernel(BatchedPotrfArgs args, int begin,
+                                                                 int end, int nmax,
+                                                                 int *counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *S = reinterpret_cast<T *>(smem_raw);
+    const int ld = nmax | 1;
+    T *dinv = S + (nmax + args.nrhs) * ld;
+    T *xb = dinv + nmax;
+    __shared__ int s_item, s_info;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = begin + s_item;
+        __syncthreads();
+        if (item >= end) break;
+        potrf_potrs_one<T, NT>(args, args.order[item], S, dinv, xb, &s_info);
+    }
+}
+
+}  // namespace nmx
+
+// ---- plan -------------------------------------------------------------------
+
+struct nmx_batched_plan_s {
+    int device = 0;
+    int dtype = NMX_F64;
+    int64_t count = 0;
+    int nrhs = 0;
+    int64_t a_elems = 0, b_elems = 0;
+    void *dev = nullptr;  // one allocation for the schedule
+    int32_t *d_order = nullptr, *d_n = nullptr, *d_counters = nullptr;
+    int64_t *d_aoff = nullptr, *d_boff = nullptr;
+    struct Bucket {
+        int begin, end, nmax, threads, grid;
+        size_t smem;
+    };
+    std::vector<Bucket> buckets;
+};
+
+namespace nmx {
+
+static const int kBucketEdges[] = {32, 64, 96, 128};
+
+static int potrf_threads_for(int nmax) { return nmax <= 32 ? 64 : (nmax <= 64 ? 128 : 256); }
+
+template <typename T>
+static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s::Bucket &b,
+                         int *counter, cudaStream_t st) {
+    switch (b.threads) {
+#define NMX_CASE(NTV)                                                                        \
+    case NTV:                                                                                \
+        potrf_potrs_batched_kernel<T, NTV><<<b.grid, NTV, b.smem, st>>>(args, b.begin, b.end, \
+                                                                        b.nmax, counter);    \
+        break;
+        NMX_CASE(64)
+        NMX_CASE(128)
+        NMX_CASE(256)
+#undef NMX_CASE
+        default:
+            set_error("unsupported thread count %d", b.threads);
+            return NMX_ERR_INTERNAL;
+    }
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
+    for (auto &b : p->buckets) {
+        b.threads = potrf_threads_for(b.nmax);
+        b.smem = sizeof(T) * (size_t)potrf_smem_elems(b.nmax, p->nrhs);
+        int per_sm = 0;
+        switch (b.threads) {
+#define NMX_OCC(NTV)                                                                           \
+    case NTV:                                                                                  \
+        NMX_CUDA_TRY(cudaFuncSetAttribute(potrf_potrs_batched_kernel<T, NTV>,                  \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                          (int)ctx->smem_optin));                              \
+        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                            \
+            &per_sm, potrf_potrs_batched_kernel<T, NTV>, NTV, b.smem));                        \
+        break;
+            NMX_OCC(64)
+            NMX_OCC(128)
+            NMX_OCC(256)
+#undef NMX_OCC
+        }
+        if (per_sm < 1) {
+            set_error("bucket nmax=%d does not fit on an SM (smem %zu)", b.nmax, b.smem);
+            return NMX_ERR_UNSUPPORTED;
+        }
+        int64_t work = b.end - b.begin;
+        b.grid = (int)std::min<int64_t>(work, (int64_t)per_sm * ctx->sm_count);
+    }
+    return 0;
+}
+
+template <typename T>
+static int run_potrf_potrs(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const T *B,
+                           T *X, int32_t *info, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    NMX_ARG_CHECK(plan->dtype == (sizeof(T) == 8 ? NMX_F64 : NMX_F32), 2,
+                  "plan was built for the other dtype");
+    NMX_ARG_CHECK(A != nullptr || plan->count == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(L != nullptr || plan->count == 0, 4, "L is NULL");
+    NMX_ARG_CHECK(B != nullptr || plan->nrhs == 0 || plan->count == 0, 5, "B is NULL");
+    NMX_ARG_CHECK(X != nullptr || plan->nrhs == 0 || plan->count == 0, 6, "X is NULL");
+    NMX_ARG_CHECK(info != nullptr || plan->count == 0, 7, "info is NULL");
+    if (plan->count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BatchedPotrfArgs args{plan->d_order, plan->d_n, plan->d_aoff, plan->d_boff, A,
+                          L,             B,         X,            info,         plan->nrhs};
+    NMX_CUDA_TRY(cudaMemsetAsync(plan->d_counters, 0, sizeof(int32_t) * plan->buckets.size(), st));
+    for (size_t bi = 0; bi < plan->buckets.size(); ++bi) {
+        int rc = launch_bucket<T>(args, plan->buckets[bi], plan->d_counters + bi, st);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+}  // namespace nmx
+
+extern "C" {
+
+int nmx_potrf_potrs_batched_plan(nmx_ctx ctx, int dtype, int64_t count, const int32_t *n_host,
+                                 int nrhs, nmx_batched_plan *out) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(dtype == NMX_F32 || dtype == NMX_F64, 2, "dtype must be NMX_F32 or NMX_F64");
+    NMX_ARG_CHECK(count >= 0 && count < (int64_t(1) << 31), 3, "count out of range");
+    NMX_ARG_CHECK(n_host != nullptr || count == 0, 4, "n_host is NULL");
+    NMX_ARG_CHECK(nrhs >= 0 && nrhs <= kPotrfMaxRhs, 5, "nrhs must be in 0..8");
+    NMX_ARG_CHECK(out != nullptr, 6, "out is NULL");
+    for (int64_t i = 0; i < count; ++i)
+        NMX_ARG_CHECK(n_host[i] >= 1 && n_host[i] <= kPotrfMaxN, 4, "every n_i must be in 1..128");
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    auto *p = new (std::nothrow) nmx_batched_plan_s();
+    if (!p) return NMX_ERR_ALLOC;
+    p->device = ctx->device;
+    p->dtype = dtype;
+    p->count = count;
+    p->nrhs = nrhs;
+    std::vector<int64_t> aoff(count), boff(count);
+    int64_t a = 0, b = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        aoff[i] = a;
+        boff[i] = b;
+        a += (int64_t)n_host[i] * n_host[i];
+        b += (int64_t)n_host[i] * nrhs;
+    }
+    p->a_elems = a;
+    p->b_elems = b;
+    // Bucket-contiguous order, largest n first inside each bucket, buckets
+    // from the largest down (longest-processing-time first).
+    std::vector<int32_t> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return n_host[x] > n_host[y]; });
+    int64_t pos = 0;
+    for (int e = 3; e >= 0 && pos < count; --e) {
+        int lo = e == 0 ? 0 : kBucketEdges[e - 1];
+        int64_t begin = pos;
+        while (pos < count && n_host[order[pos]] > lo) ++pos;
+        if (pos > begin)
+            p->buckets.push_back({(int)begin, (int)pos, n_host[order[begin]], 0, 0, 0});
+    }
+    size_t nb = p->buckets.size();
+    size_t bytes = sizeof(int32_t) * (2 * count + nb + 1) + sizeof(int64_t) * (2 * count) + 64;
+    cudaError_t e = cudaMalloc(&p->dev, bytes);
+    if (e != cudaSuccess) {
+        delete p;
+        set_error("plan cudaMalloc: %s", cudaGetErrorString(e));
+        return NMX_ERR_ALLOC;
+    }
+    char *base = static_cast<char *>(p->dev);
+    p->d_aoff = reinterpret_cast<int64_t *>(base);
+    p->d_boff = p->d_aoff + count;
+    p->d_order = reinterpret_cast<int32_t *>(p->d_boff + count);
+    p->d_n = p->d_order + count;
+    p->d_counters = p->d_n + count;
+    int rc = 0;
+    if (count) {
+        if (cudaMemcpy(p->d_aoff, aoff.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(p->d_boff, boff.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(p->d_order, order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(p->d_n, n_host, sizeof(int32_t) * count, cudaMemcpyHostToDevice)) {
+            set_error("plan upload failed");
+            rc = NMX_ERR_CUDA;
+        }
+    }
+    if (!rc) rc = dtype == NMX_F64 ? configure_buckets<double>(ctx, p) : configure_buckets<float>(ctx, p);
+    if (rc) {
+        cudaFree(p->dev);
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return 0;
+}
+
+int nmx_batched_plan_destroy(nmx_batched_plan plan) {
+    if (!plan) return 0;
+    nmx::DeviceGuard g(plan->device);
+    if (plan->dev) cudaFree(plan->dev);
+    delete plan;
+    return 0;
+}
+
+int nmx_batched_plan_sizes(nmx_batched_plan plan, int64_t *a_elems, int64_t *b_elems) {
+    NMX_ARG_CHECK(plan != nullptr, 1, "plan is NULL");
+    if (a_elems) *a_elems = plan->a_elems;
+    if (b_elems) *b_elems = plan->b_elems;
+    return 0;
+}
+
+int nmx_potrf_potrs_batched_f64(nmx_ctx ctx, nmx_batched_plan plan, const double *A, double *L,
+                                const double *B, double *X, int32_t *info, void *stream) {
+    return nmx::run_potrf_potrs<double>(ctx, plan, A, L, B, X, info, stream);
+}
+
+int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A, float *L,
+                                const float *B, float *X, int32_t *info, void *stream) {
+    return nmx::run_potrf_potrs<float>(ctx, plan, A, L, B, X, info, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+// Context lifecycle and error reporting for libnmxla.so.
+#include <cstring>
+
+#include "nmx_common.cuh"
+
+namespace nmx {
+
+static thread_local char g_last_error[1024] = {0};
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+void clear_error() { g_last_error[0] = 0; }
+
+}  // namespace nmx
+
+int nmx_context::ensure_workspace(size_t bytes) {
+    if (bytes <= workspace_bytes) return 0;
+    if (workspace) cudaFree(workspace);
+    workspace = nullptr;
+    workspace_bytes = 0;
+    size_t rounded = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
+    cudaError_t e = cudaMalloc(&workspace, rounded);
+    if (e != cudaSuccess) {
+        nmx::set_error("workspace cudaMalloc(%zu): %s", rounded, cudaGetErrorString(e));
+        return NMX_ERR_ALLOC;
+    }
+    workspace_bytes = rounded;
+    return 0;
+}
+
+extern "C" {
+
+const char *nmx_last_error_string(void) { return nmx::g_last_error; }
+
+int nmx_version(void) { return 100; }
+
+int nmx_create(int device, nmx_ctx *out) {
+    NMX_ARG_CHECK(out != nullptr, 2, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    NMX_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    NMX_ARG_CHECK(device >= 0 && device < ndev, 1, "no such CUDA device");
+    nmx::DeviceGuard g(device);
+    cudaDeviceProp prop;
+    NMX_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        nmx::set_error("device %d is sm_%d%d; libnmxla is built for sm_100a only", device,
+                       prop.major, prop.minor);
+        return NMX_ERR_UNSUPPORTED;
+    }
+    nmx_context *ctx = new (std::nothrow) nmx_context();
+    if (!ctx) return NMX_ERR_ALLOC;
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->cc_major = prop.major;
+    ctx->cc_minor = prop.minor;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    *out = ctx;
+    nmx::clear_error();
+    return 0;
+}
+
+int nmx_destroy(nmx_ctx ctx) {
+    if (!ctx) return 0;
+    {
+        nmx::DeviceGuard g(ctx->device);
+        if (ctx->workspace) cudaFree(ctx->workspace);
+    }
+    delete ctx;
+    return 0;
+}
+
+}  // extern "C"

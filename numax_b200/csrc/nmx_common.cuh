@@ -1,0 +1,96 @@
+// Shared internals of libnmxla.so: error reporting, the context, small
+// device helpers.  Not part of the public ABI (include/nmx_la.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/nmx_la.h"
+
+namespace nmx {
+
+// ---- error reporting --------------------------------------------------------
+
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define NMX_CUDA_TRY(expr)                                                              \
+    do {                                                                                \
+        cudaError_t _e = (expr);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            ::nmx::set_error("%s:%d: %s -> %s", __FILE__, __LINE__, #expr,               \
+                             cudaGetErrorString(_e));                                   \
+            return NMX_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+
+#define NMX_ARG_CHECK(cond, idx, msg)                                                   \
+    do {                                                                                \
+        if (!(cond)) {                                                                  \
+            ::nmx::set_error("argument %d: %s", (idx), (msg));                          \
+            return -(idx);                                                              \
+        }                                                                               \
+    } while (0)
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace nmx
+
+// The context: device, SM count, a grow-only workspace owned for the
+// context's lifetime (numax allocates per call, numax/linalg/lu.mojo:582-584;
+// here the context keeps it so repeated calls allocate nothing).
+struct nmx_context {
+    int device = 0;
+    int sm_count = 0;
+    int cc_major = 0, cc_minor = 0;
+    size_t smem_optin = 0;
+    void *workspace = nullptr;
+    size_t workspace_bytes = 0;
+    // Returns a device buffer of at least `bytes`, reusing the context's.
+    int ensure_workspace(size_t bytes);
+};
+
+namespace nmx {
+
+// ---- device helpers ---------------------------------------------------------
+
+// guard_nonzero(x, floor) = copysign(max_of(|x|, floor), x), with numax's
+// max_of being an exact selection where |x| >= floor wins
+// (numax/core/numeric.mojo:263-366).  A NaN propagates.
+template <typename T>
+__device__ __forceinline__ T guard_nonzero(T x, T floor_) {
+    T ax = fabs(x);
+    T m = (ax >= floor_ || ax != ax) ? ax : floor_;
+    return copysign(m, x);
+}
+
+template <typename T>
+struct pivot_floor;
+template <>
+struct pivot_floor<double> {
+    static constexpr double value = 1e-30;
+};
+template <>
+struct pivot_floor<float> {
+    static constexpr float value = 1e-30f;
+};
+
+__host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace nmx

@@ -1,0 +1,131 @@
+"""Batched uneven Cholesky + cho_solve on the GPU vs the oracle (numax's
+Array-tier cholesky/cholesky_solve run per matrix on the CPU).
+
+Tolerances (north star): normwise relative 1e-12 for float64, 1e-5 for
+float32, on L (lower triangle) and X per matrix."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float64: 1e-12, np.float32: 1e-5}
+
+
+def make_batch(ns, nrhs, dtype, seed):
+    """A_i = G G^T / n + n I with G iid N(0,1); B iid N(0,1) (PCG64)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mats, rhs = [], []
+    for n in ns:
+        g = rng.standard_normal((n, n))
+        mats.append((g @ g.T / n + n * np.eye(n)).astype(dtype).ravel())
+        rhs.append(rng.standard_normal(n * nrhs).astype(dtype))
+    return np.concatenate(mats), np.concatenate(rhs) if nrhs else np.zeros(0, dtype)
+
+
+def run_gpu(ns, A, B, nrhs, alias=False):
+    import numax_b200 as nb
+    dt = torch.float64 if A.dtype == np.float64 else torch.float32
+    dA = torch.from_numpy(A.copy()).cuda()
+    dB = torch.from_numpy(B.copy()).cuda() if nrhs else None
+    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=dt)
+    X = dB if alias else None
+    dA, dX, info = plan(dA, dB, X)
+    return dA.cpu().numpy(), (dX.cpu().numpy() if nrhs else None), info.cpu().numpy()
+
+
+def relerr(got, want):
+    d = np.linalg.norm(want)
+    return np.linalg.norm(got - want) / (d if d > 0 else 1.0)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_batched_potrf_potrs_matches_oracle(oracle, dtype):
+    edge = [1, 2, 3, 7, 8, 15, 16, 17, 31, 32, 33, 47, 48, 63, 64, 65, 95, 96, 97, 127, 128]
+    rng = np.random.Generator(np.random.PCG64(5))
+    ns = np.array(edge + list(rng.integers(1, 129, size=300)), dtype=np.int32)
+    rng.shuffle(ns)
+    nrhs = 4
+    A, B = make_batch(ns, nrhs, dtype, seed=9)
+    gotA, gotX, info = run_gpu(ns, A, B, nrhs)
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, nrhs)
+    ao, bo = oracle.ragged_offsets(ns), oracle.ragged_offsets(ns, nrhs)
+    tol = TOL[dtype]
+    assert (info == 0).all()
+    worst_l = worst_x = 0.0
+    for i, n in enumerate(ns):
+        gl = np.tril(gotA[ao[i]:ao[i] + n * n].reshape(n, n))
+        wl = np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))
+        # The upper triangle of A is left untouched.
+        np.testing.assert_array_equal(np.triu(gotA[ao[i]:ao[i] + n * n].reshape(n, n), 1),
+                                      np.triu(A[ao[i]:ao[i] + n * n].reshape(n, n), 1))
+        worst_l = max(worst_l, relerr(gl, wl))
+        worst_x = max(worst_x, relerr(gotX[bo[i]:bo[i] + n * nrhs], wantX[bo[i]:bo[i] + n * nrhs]))
+    assert worst_l <= tol, worst_l
+    assert worst_x <= tol, worst_x
+
+
+@pytest.mark.parametrize("nrhs", [0, 1, 8])
+def test_batched_rhs_counts_and_aliasing(oracle, nrhs):
+    ns = np.array([5, 128, 33, 1, 64, 100], dtype=np.int32)
+    A, B = make_batch(ns, nrhs, np.float64, seed=nrhs)
+    gotA, gotX, info = run_gpu(ns, A, B, nrhs, alias=nrhs > 0)
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B if nrhs else np.zeros(0), nrhs)
+    ao = oracle.ragged_offsets(ns)
+    for i, n in enumerate(ns):
+        assert relerr(np.tril(gotA[ao[i]:ao[i] + n * n].reshape(n, n)),
+                      np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= 1e-12
+    if nrhs:
+        assert relerr(gotX, wantX) <= 1e-12
+
+
+def test_batched_not_positive_definite_info_and_nan(oracle):
+    # numax's later-block failure (tests/linalg/test_tensor_linalg.mojo:700-741):
+    # positive definite leading 2x2, fails at index 3 -> info 4.
+    bad = np.array([4.0, 1.0, 0.0, 0.0, 1.0, 4.0, 0.0, 0.0, 0.0, 0.0, 1.0, 3.0,
+                    0.0, 0.0, 3.0, 1.0])
+    good_ns = np.array([20, 70], dtype=np.int32)
+    goodA, goodB = make_batch(good_ns, 2, np.float64, seed=1)
+    ns = np.array([20, 4, 70], dtype=np.int32)
+    A = np.concatenate([goodA[:400], bad, goodA[400:]])
+    B = np.concatenate([goodB[:40], np.ones(8), goodB[40:]])
+    gotA, gotX, info = run_gpu(ns, A, B, 2)
+    assert list(info) == [0, 4, 0]
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, 2)
+    # Array-tier semantics: NaN exactly where the oracle has NaN.
+    np.testing.assert_array_equal(np.isnan(gotX), np.isnan(wantX))
+    L4 = gotA[400:416].reshape(4, 4)
+    np.testing.assert_allclose(np.tril(L4)[:2, :2], np.tril(wantL[400:416].reshape(4, 4))[:2, :2],
+                               rtol=1e-14)
+    assert np.isnan(L4[3, 3])
+
+
+def test_batched_reads_only_lower_triangle(oracle):
+    ns = np.array([9, 40, 128], dtype=np.int32)
+    A, B = make_batch(ns, 4, np.float64, seed=3)
+    ao = oracle.ragged_offsets(ns)
+    garbage = A.copy()
+    for i, n in enumerate(ns):
+        m = garbage[ao[i]:ao[i] + n * n].reshape(n, n)
+        m[np.triu_indices(n, 1)] = np.nan
+    gA, gX, _ = run_gpu(ns, A, B, 4)
+    hA, hX, _ = run_gpu(ns, garbage, B, 4)
+    np.testing.assert_array_equal(gX, hX)
+    for i, n in enumerate(ns):
+        np.testing.assert_array_equal(np.tril(gA[ao[i]:ao[i] + n * n].reshape(n, n)),
+                                      np.tril(hA[ao[i]:ao[i] + n * n].reshape(n, n)))
+
+
+def test_batched_rejects_bad_arguments():
+    import numax_b200 as nb
+    with pytest.raises(nb._lib.NmxError):
+        nb.CholeskySolveBatch(np.array([129], dtype=np.int32), nrhs=4)
+    with pytest.raises(nb._lib.NmxError):
+        nb.CholeskySolveBatch(np.array([0], dtype=np.int32), nrhs=4)
+    with pytest.raises(nb._lib.NmxError):
+        nb.CholeskySolveBatch(np.array([4], dtype=np.int32), nrhs=9)
+    plan = nb.CholeskySolveBatch(np.array([4, 5], dtype=np.int32), nrhs=1)
+    with pytest.raises(ValueError):
+        plan(torch.zeros(10, dtype=torch.float64, device="cuda"),
+             torch.zeros(9, dtype=torch.float64, device="cuda"))
