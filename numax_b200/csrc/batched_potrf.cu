@@ -307,18 +307,32 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
     return 0;
 }
 
+// Let a kernel use all the opt-in shared memory not taken by its static
+// shared variables (the largest bucket's size decides the launch).
+template <typename K>
+static cudaError_t set_max_dynamic_smem(K kernel, nmx_ctx ctx) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(ctx->smem_optin - fa.sharedSizeBytes));
+}
+
 template <typename T>
 static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
     for (auto &b : p->buckets) {
         b.threads = potrf_threads_for(b.nmax);
         b.smem = sizeof(T) * (size_t)potrf_smem_elems(b.nmax, p->nrhs);
+        if (b.smem + 64 > ctx->smem_optin) {
+            set_error("bucket nmax=%d needs %zu B of shared memory (> %zu)", b.nmax, b.smem,
+                      ctx->smem_optin);
+            return NMX_ERR_UNSUPPORTED;
+        }
         int per_sm = 0;
         switch (b.threads) {
 #define NMX_OCC(NTV)                                                                           \
     case NTV:                                                                                  \
-        NMX_CUDA_TRY(cudaFuncSetAttribute(potrf_potrs_batched_kernel<T, NTV>,                  \
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,         \
-                                          (int)ctx->smem_optin));                              \
+        NMX_CUDA_TRY(set_max_dynamic_smem(potrf_potrs_batched_kernel<T, NTV>, ctx));        \
         NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                            \
             &per_sm, potrf_potrs_batched_kernel<T, NTV>, NTV, b.smem));                        \
         break;
