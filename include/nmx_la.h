@@ -49,6 +49,7 @@ extern "C" {
 
 typedef struct nmx_context *nmx_ctx;
 typedef struct nmx_batched_plan_s *nmx_batched_plan;
+typedef struct nmx_syevj_plan_s *nmx_syevj_plan;
 
 /* ---- context ------------------------------------------------------------ */
 
@@ -102,6 +103,60 @@ NMX_API int nmx_potrf_potrs_batched_f64(nmx_ctx ctx, nmx_batched_plan plan, cons
 NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A,
                                         float *L, const float *B, float *X, int32_t *info,
                                         void *stream);
+
+/* ---- batched uneven-size symmetric eigensolver (Jacobi) -----------------
+ *
+ * Replaces numax's Array-tier `eigh[T, n, sweeps=12]` run one matrix per GPU
+ * thread (numax/linalg/_array/eigen.mojo:316-392; launched through `map` in
+ * examples/advanced/quantum_well.mojo:149-157).  float32 data, float64
+ * rotation angles (numax's formula, numax/linalg/_array/eigen.mojo:34-75)
+ * and a float64 off-diagonal-norm stopping test.  Parallel (round-robin)
+ * ordering replaces numax's cyclic order, so eigenvalues agree to rounding
+ * but their unsorted order may differ; `sort` = 1 returns them ascending
+ * with V's columns permuted to match (numpy.linalg.eigh's order).
+ *
+ * Ragged layout: A_i and V_i are n_i x n_i row-major at a_off[i] = sum n_j^2;
+ * W_i (n_i values) at w_off[i] = sum n_j.  1 <= n_i <= 64.  The whole matrix
+ * is read (numax's eigh assumes symmetry and does not check it).  V's columns
+ * are the eigenvectors.  sweeps[i] (optional, may be NULL) receives the
+ * number of sweeps run.  A sweep runs while off(A) > tol * ||A||_F and fewer
+ * than max_sweeps sweeps have run.
+ */
+NMX_API int nmx_syevj_batched_plan(nmx_ctx ctx, int64_t count, const int32_t *n_host,
+                                   nmx_syevj_plan *out);
+NMX_API int nmx_syevj_plan_destroy(nmx_syevj_plan plan);
+NMX_API int nmx_syevj_plan_sizes(nmx_syevj_plan plan, int64_t *a_elems, int64_t *w_elems);
+NMX_API int nmx_syevj_batched_f32(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
+                                  float *V, int32_t *sweeps, double tol, int max_sweeps, int sort,
+                                  void *stream);
+
+/* ---- dense LU with partial pivoting, and its solve ----------------------
+ *
+ * nmx_getrf_*: factor the n x n row-major A (leading dimension lda) in place
+ * into P L U -- numax's lu_factor (numax/linalg/lu.mojo:454-701) with its
+ * getrf2 recursive panel (numax/linalg/panel.mojo:445-586) taken over the
+ * whole matrix.  On return A holds L strictly below the diagonal (unit
+ * diagonal implicit) and U on and above it; ipiv[j] (0-based, device int32)
+ * is the row interchanged with row j, applied across the full width in
+ * order (numax/linalg/lu.mojo:114-122); *info (device int32) is the 1-based
+ * index of the first column with no nonzero pivot candidate, 0 otherwise.
+ * The pivot rule is numax's: largest |a|, the lowest row on ties
+ * (numax/linalg/panel.mojo:350-388).  A zero pivot is floored to 1e-30 for
+ * the division and the factorization continues, so a singular A yields
+ * non-finite solves rather than an error (numax/linalg/lu.mojo:96-98).
+ *
+ * nmx_getrs_*: B := A^-1 B for the n x nrhs row-major B (ldb), from the
+ * factors: interchanges, unit-lower solve, upper solve -- numax's LU.solve
+ * (numax/linalg/lu.mojo:181-354).
+ */
+NMX_API int nmx_getrf_f64(nmx_ctx ctx, int64_t n, double *A, int64_t lda, int32_t *ipiv,
+                          int32_t *info, void *stream);
+NMX_API int nmx_getrf_f32(nmx_ctx ctx, int64_t n, float *A, int64_t lda, int32_t *ipiv,
+                          int32_t *info, void *stream);
+NMX_API int nmx_getrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *LU, int64_t lda,
+                          const int32_t *ipiv, double *B, int64_t ldb, void *stream);
+NMX_API int nmx_getrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *LU, int64_t lda,
+                          const int32_t *ipiv, float *B, int64_t ldb, void *stream);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,8 @@ sm_100a.  There is no CPU fallback; without the built library or an sm_100
 device the calls raise.
 """
 from . import _lib
-from .batched import CholeskySolveBatch, cholesky_solve_batched, ragged_offsets
+from .batched import (CholeskySolveBatch, EighBatch, cholesky_solve_batched, eigh_batched,
+                      ragged_offsets)
 
-__all__ = ["CholeskySolveBatch", "cholesky_solve_batched", "ragged_offsets"]
+__all__ = ["CholeskySolveBatch", "EighBatch", "cholesky_solve_batched", "eigh_batched",
+           "ragged_offsets"]

@@ -139,3 +139,69 @@ def cholesky_solve_batched(ns, A, B, nrhs: int = 4):
     """One-shot form: plan, run, synchronize.  Returns (A with L, X, info)."""
     plan = CholeskySolveBatch(ns, nrhs=nrhs, dtype=A.dtype, device=A.device)
     return plan(A, B)
+
+
+class EighBatch:
+    """A reusable plan for the symmetric eigensolver over a ragged batch
+    (float32 data, n_i in 1..64).
+
+    numax's Array-tier `eigh[T, n, sweeps=12]`
+    (numax/linalg/_array/eigen.mojo:316-392) runs 12 fixed cyclic Jacobi
+    sweeps per matrix inside one GPU thread.  This runs parallel-order Jacobi
+    with float64 rotation angles and a float64 off-diagonal stopping test
+    (sweeps stop once off(A) <= tol * ||A||_F, at most `max_sweeps`).
+    Eigenvalues are the final diagonal; with sort=False they come in the
+    solver's diagonal order (numax's convention: unsorted), with sort=True
+    ascending and V's columns permuted to match.
+    """
+
+    def __init__(self, ns, device=None):
+        self.device = _resolve_device(device)
+        self.ns = np.ascontiguousarray(ns, dtype=np.int32)
+        self.count = int(self.ns.size)
+        self._ctx = _lib.context(self.device.index)
+        h = C.c_void_p()
+        _lib.call("nmx_syevj_batched_plan", self._ctx, self.count,
+                  self.ns.ctypes.data if self.count else None, C.byref(h))
+        self._plan = h.value
+        a, w = C.c_int64(), C.c_int64()
+        _lib.call("nmx_syevj_plan_sizes", self._plan, C.byref(a), C.byref(w))
+        self.a_elems, self.w_elems = a.value, w.value
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan:
+            try:
+                _lib.load().nmx_syevj_plan_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    def run(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
+            sort: bool = False):
+        """Enqueue on the current stream; returns (W, V, sweeps)."""
+        _check_tensor("A", A, torch.float32, self.a_elems, self.device)
+        if W is None:
+            W = torch.empty(self.w_elems, dtype=torch.float32, device=self.device)
+        if V is None:
+            V = torch.empty(self.a_elems, dtype=torch.float32, device=self.device)
+        if sweeps is None:
+            sweeps = torch.empty(self.count, dtype=torch.int32, device=self.device)
+        _check_tensor("W", W, torch.float32, self.w_elems, self.device)
+        _check_tensor("V", V, torch.float32, self.a_elems, self.device)
+        _check_tensor("sweeps", sweeps, torch.int32, self.count, self.device)
+        _lib.call("nmx_syevj_batched_f32", self._ctx, self._plan, A.data_ptr(), W.data_ptr(),
+                  V.data_ptr(), sweeps.data_ptr(), float(tol), int(max_sweeps), int(bool(sort)),
+                  _stream_ptr(self.device))
+        return W, V, sweeps
+
+    def __call__(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
+                 sort: bool = False):
+        out = self.run(A, W, V, sweeps, tol, max_sweeps, sort)
+        torch.cuda.current_stream(self.device).synchronize()
+        return out
+
+
+def eigh_batched(ns, A, tol: float = 1e-7, max_sweeps: int = 20, sort: bool = False):
+    """One-shot form of EighBatch: returns (W, V, sweeps)."""
+    return EighBatch(ns, device=A.device)(A, tol=tol, max_sweeps=max_sweeps, sort=sort)

@@ -1,4 +1,6 @@
 // Context lifecycle and error reporting for libnmxla.so.
+#include <cublas_v2.h>
+
 #include <cstring>
 
 #include "nmx_common.cuh"
@@ -15,6 +17,28 @@ void set_error(const char *fmt, ...) {
 }
 
 void clear_error() { g_last_error[0] = 0; }
+
+int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out) {
+    if (!ctx->cublas) {
+        cublasHandle_t h;
+        cublasStatus_t s = cublasCreate(&h);
+        if (s != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasCreate failed (%d)", (int)s);
+            return NMX_ERR_CUDA;
+        }
+        // Default math: FP64/FP32 products stay in their own precision (no
+        // TF32 tensor-op substitution, which needs CUBLAS_TF32_TENSOR_OP_MATH).
+        cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+        ctx->cublas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) {
+        set_error("cublasSetStream failed");
+        return NMX_ERR_CUDA;
+    }
+    *out = h;
+    return 0;
+}
 
 }  // namespace nmx
 
@@ -70,6 +94,7 @@ int nmx_destroy(nmx_ctx ctx) {
     {
         nmx::DeviceGuard g(ctx->device);
         if (ctx->workspace) cudaFree(ctx->workspace);
+        if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
     }
     delete ctx;
     return 0;

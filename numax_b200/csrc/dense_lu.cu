@@ -1,0 +1,504 @@
+// Dense LU with partial pivoting and the LU solve (sm_100a), row-major.
+//
+// numax's lu_factor (numax/linalg/lu.mojo:454-701) is right-looking and
+// blocked (block 16 on a device) with a recursive panel getrf2
+// (numax/linalg/panel.mojo:445-586) whose leaves are a single-CTA
+// getrf_panel (numax/linalg/panel.mojo:289-431); its cubic term is MAX's
+// matmul.  Here the recursion is taken all the way up -- getrf2 over the
+// whole matrix -- so every cubic term is one large GEMM, and the leaves
+// (32 columns) are factored by a cooperative kernel that spreads the panel's
+// rows over every SM:
+//
+//   per column: each CTA finds its local max |a| (first maximum, lower row
+//   on ties: numax's pivot rule), publishes the candidate row, one grid-wide
+//   barrier, every CTA picks the same winner, the two owners exchange rows,
+//   every CTA scales and rank-1 updates its own rows.
+//
+// One barrier per column; the published rows are double-buffered by column
+// parity so a fast CTA never overwrites what a slow one still reads.
+// Interchanges are recorded LAPACK-style (pivots[j] = row swapped with j,
+// 0-based) and applied across the full width, as numax does: inside the leaf
+// to the leaf's columns, then by a laswp kernel to every other column.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "dense_common.cuh"
+
+namespace nmx {
+
+constexpr int kLeafW = 32;      // leaf panel width
+constexpr int kLeafThreads = 256;
+constexpr int kTrsmLeaf = 32;
+
+template <typename T>
+struct LeafScratch {
+    T *cand_rows;     // [2][G][kLeafW]
+    T *col_rows;      // [2][kLeafW]
+    T *cand_mag;      // [2][G]
+    int *cand_row;    // [2][G]
+    unsigned *bar;
+    int *err;
+};
+
+// Cooperative leaf: factor columns [c, c+w) over rows [c, n) in place.
+template <typename T>
+__global__ void __launch_bounds__(kLeafThreads)
+    getrf_leaf_kernel(T *A, int64_t lda, int n, int c, int w, int rows_per_cta, int32_t *ipiv,
+                      int32_t *info, LeafScratch<T> sc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ldl = kLeafW + 1;
+    T *loc = reinterpret_cast<T *>(smem_raw);           // rows_per_cta x ldl
+    T *prow = loc + (size_t)rows_per_cta * ldl;          // pivot row (w)
+    __shared__ T s_mag[kLeafThreads / 32];
+    __shared__ int s_row[kLeafThreads / 32];
+    __shared__ int s_flag, s_piv, s_wcta;
+    __shared__ T s_wmag;
+
+    const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int r0 = c + cta * rows_per_cta;                     // first global row owned
+    const int nloc = max(0, min(rows_per_cta, n - r0));        // rows owned
+
+    for (int e = tid; e < nloc * w; e += kLeafThreads) {
+        int r = e / w, j = e - r * w;
+        loc[r * ldl + j] = A[(int64_t)(r0 + r) * lda + c + j];
+    }
+    __syncthreads();
+
+    for (int j = 0; j < w; ++j) {
+        const int col = c + j;
+        const int slot = j & 1;
+        // Local argmax over owned rows with global index >= col.
+        T best = T(-1);
+        int brow = INT32_MAX;
+        for (int r = tid; r < nloc; r += kLeafThreads) {
+            int gr = r0 + r;
+            if (gr < col) continue;
+            T m = fabs(loc[r * ldl + j]);
+            if (!(m > T(0))) continue;  // zero/NaN never pivots (numax: strict > from 0)
+            if (m > best || (m == best && gr < brow)) {
+                best = m;
+                brow = gr;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            T om = __shfl_xor_sync(0xffffffffu, best, o);
+            int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            if (om > best || (om == best && orow < brow)) {
+                best = om;
+                brow = orow;
+            }
+        }
+        if (lane == 0) {
+            s_mag[warp] = best;
+            s_row[warp] = brow;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            best = lane < kLeafThreads / 32 ? s_mag[lane] : T(-1);
+            brow = lane < kLeafThreads / 32 ? s_row[lane] : INT32_MAX;
+            for (int o = 16; o > 0; o >>= 1) {
+                T om = __shfl_xor_sync(0xffffffffu, best, o);
+                int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                if (om > best || (om == best && orow < brow)) {
+                    best = om;
+                    brow = orow;
+                }
+            }
+            if (lane == 0) {
+                sc.cand_mag[slot * G + cta] = best;
+                sc.cand_row[slot * G + cta] = brow;
+                s_row[0] = brow;
+            }
+        }
+        __syncthreads();
+        // Publish the candidate row, and row `col` if this CTA owns it.
+        {
+            const int brow_l = s_row[0] - r0;
+            if (s_row[0] != INT32_MAX && tid < w)
+                sc.cand_rows[((size_t)slot * G + cta) * kLeafW + tid] = loc[brow_l * ldl + tid];
+            if (col >= r0 && col < r0 + nloc && tid < w)
+                sc.col_rows[slot * kLeafW + tid] = loc[(col - r0) * ldl + tid];
+        }
+        if (!grid_barrier(sc.bar, (unsigned)j, (unsigned)G, sc.err, &s_flag)) return;
+
+        // Every CTA reduces the same candidates in the same order: same winner.
+        if (warp == 0) {
+            best = T(-1);
+            brow = INT32_MAX;
+            int bcta = -1;
+            for (int g = lane; g < G; g += 32) {
+                T m = sc.cand_mag[slot * G + g];
+                int rr = sc.cand_row[slot * G + g];
+                if (m > best || (m == best && rr < brow)) {
+                    best = m;
+                    brow = rr;
+                    bcta = g;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                T om = __shfl_xor_sync(0xffffffffu, best, o);
+                int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                int octa = __shfl_xor_sync(0xffffffffu, bcta, o);
+                if (om > best || (om == best && orow < brow)) {
+                    best = om;
+                    brow = orow;
+                    bcta = octa;
+                }
+            }
+            if (lane == 0) {
+                s_piv = brow;
+                s_wcta = bcta;
+                s_wmag = best;
+            }
+        }
+        __syncthreads();
+        // No positive magnitude anywhere: numax keeps row `col` as the pivot.
+        const bool none = s_piv == INT32_MAX;
+        const int piv = none ? col : s_piv;
+        if (tid < w)
+            prow[tid] = none ? sc.col_rows[slot * kLeafW + tid]
+                             : sc.cand_rows[((size_t)slot * G + s_wcta) * kLeafW + tid];
+        __syncthreads();
+        if (piv != col) {
+            if (col >= r0 && col < r0 + nloc && tid < w) loc[(col - r0) * ldl + tid] = prow[tid];
+            if (piv >= r0 && piv < r0 + nloc && tid < w)
+                loc[(piv - r0) * ldl + tid] = sc.col_rows[slot * kLeafW + tid];
+        }
+        if (cta == 0 && tid == 0) {
+            ipiv[col] = piv;
+            if (none && *info == 0) *info = col + 1;
+        }
+        __syncthreads();
+        T p = prow[j];
+        if (p == T(0)) p = pivot_floor<T>::value;
+        for (int r = tid; r < nloc; r += kLeafThreads) {
+            const int gr = r0 + r;
+            if (gr <= col) continue;
+            T l = loc[r * ldl + j] / p;
+            loc[r * ldl + j] = l;
+            for (int jj = j + 1; jj < w; ++jj) loc[r * ldl + jj] -= l * prow[jj];
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nloc * w; e += kLeafThreads) {
+        int r = e / w, j = e - r * w;
+        A[(int64_t)(r0 + r) * lda + c + j] = loc[r * ldl + j];
+    }
+}
+
+// Apply interchanges ipiv[c..c+w) to the columns outside [c, c+w) of rows of
+// A (ncols wide).  One thread per column, swaps in order.
+template <typename T>
+__global__ void laswp_kernel(T *A, int64_t lda, int ncols, int c, int w, const int32_t *ipiv,
+                             int skip_lo, int skip_hi) {
+    int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncols || (col >= skip_lo && col < skip_hi)) return;
+    for (int s = 0; s < w; ++s) {
+        int r1 = c + s, r2 = ipiv[c + s];
+        if (r1 != r2) {
+            T a = A[(int64_t)r1 * lda + col];
+            A[(int64_t)r1 * lda + col] = A[(int64_t)r2 * lda + col];
+            A[(int64_t)r2 * lda + col] = a;
+        }
+    }
+}
+
+// X := L^-1 X for the w x w (w <= 32) lower block L at (r, r) of A (unit or
+// not) and X = rows [r, r+w) x cols [c0, c1) of B.  One thread per column.
+template <typename T, bool UNIT>
+__global__ void trsm_lower_leaf_kernel(const T *A, int64_t lda, int r, int w, T *B, int64_t ldb,
+                                       int c0, int c1) {
+    __shared__ T Ls[kTrsmLeaf][kTrsmLeaf + 1];
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        int i = e / w, j = e - i * w;
+        Ls[i][j] = A[(int64_t)(r + i) * lda + r + j];
+    }
+    __syncthreads();
+    int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= c1) return;
+    T x[kTrsmLeaf];
+#pragma unroll
+    for (int i = 0; i < kTrsmLeaf; ++i) x[i] = i < w ? B[(int64_t)(r + i) * ldb + col] : T(0);
+#pragma unroll
+    for (int i = 0; i < kTrsmLeaf; ++i) {
+        if (i < w) {
+            T s = x[i];
+#pragma unroll
+            for (int p = 0; p < kTrsmLeaf; ++p)
+                if (p < i) s -= Ls[i][p] * x[p];
+            x[i] = UNIT ? s : s / Ls[i][i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kTrsmLeaf; ++i)
+        if (i < w) B[(int64_t)(r + i) * ldb + col] = x[i];
+}
+
+// X := U^-1 X for the w x w upper block U at (r, r) of A (non-unit), or
+// with TRANS the transpose of the lower block stored there (L^T).
+template <typename T, bool TRANS>
+__global__ void trsm_upper_leaf_kernel(const T *A, int64_t lda, int r, int w, T *B, int64_t ldb,
+                                       int c0, int c1) {
+    __shared__ T Us[kTrsmLeaf][kTrsmLeaf + 1];
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        int i = e / w, j = e - i * w;
+        T v = A[(int64_t)(r + i) * lda + r + j];
+        if (TRANS)
+            Us[j][i] = v;
+        else
+            Us[i][j] = v;
+    }
+    __syncthreads();
+    int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= c1) return;
+    T x[kTrsmLeaf];
+#pragma unroll
+    for (int i = 0; i < kTrsmLeaf; ++i) x[i] = i < w ? B[(int64_t)(r + i) * ldb + col] : T(0);
+#pragma unroll
+    for (int s = 0; s < kTrsmLeaf; ++s) {
+        const int i = kTrsmLeaf - 1 - s;
+        if (i < w) {
+            T v = x[i];
+#pragma unroll
+            for (int p = 0; p < kTrsmLeaf; ++p)
+                if (p > i && p < w) v -= Us[i][p] * x[p];
+            x[i] = v / Us[i][i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kTrsmLeaf; ++i)
+        if (i < w) B[(int64_t)(r + i) * ldb + col] = x[i];
+}
+
+// ---- host drivers -------------------------------------------------------
+
+template <typename T>
+struct LuRun {
+    nmx_ctx ctx;
+    cudaStream_t st;
+    cublasHandle_t h;
+    T *A;
+    int64_t lda;
+    int n;
+    int32_t *ipiv;
+    int32_t *info;
+    LeafScratch<T> sc;
+    int max_ctas;
+};
+
+template <typename T>
+static int leaf(LuRun<T> &R, int c, int w) {
+    const int m = R.n - c;
+    int G = (int)std::min<int64_t>(R.max_ctas, ceil_div(m, 32));
+    G = std::max(G, 1);
+    int rpc = (int)ceil_div(m, G);
+    G = (int)ceil_div(m, rpc);
+    size_t smem = sizeof(T) * ((size_t)rpc * (kLeafW + 1) + kLeafW);
+    if (smem > R.ctx->smem_optin - 1024) {
+        set_error("matrix order %d too large for the leaf panel (%zu B shared)", R.n, smem);
+        return NMX_ERR_UNSUPPORTED;
+    }
+    NMX_CUDA_TRY(cudaMemsetAsync(R.sc.bar, 0, sizeof(unsigned), R.st));
+    void *args[] = {&R.A, &R.lda, &R.n, &c, &w, &rpc, &R.ipiv, &R.info, &R.sc};
+    NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)getrf_leaf_kernel<T>, dim3(G),
+                                             dim3(kLeafThreads), args, smem, R.st));
+    // The interchanges across the rest of the width.
+    int threads = 256;
+    laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(R.A, R.lda, R.n, c, w,
+                                                                             R.ipiv, c, c + w);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// X := L^-1 X, L the w x w lower block at (r, r) of A, X rows [r, r+w) cols [c0, c1) of B.
+template <typename T, bool UNIT>
+int trsm_lower(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda,
+                      int r, int w, T *B, int64_t ldb, int c0, int c1) {
+    if (w <= 0 || c1 <= c0) return 0;
+    if (w <= kTrsmLeaf) {
+        int threads = 128;
+        trsm_lower_leaf_kernel<T, UNIT>
+            <<<(unsigned)ceil_div(c1 - c0, threads), threads, 0, st>>>(A, lda, r, w, B, ldb, c0, c1);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+    int hw = (w / 2 + kTrsmLeaf - 1) / kTrsmLeaf * kTrsmLeaf;
+    int rc = trsm_lower<T, UNIT>(ctx, h, st, A, lda, r, hw, B, ldb, c0, c1);
+    if (rc) return rc;
+    NMX_CUBLAS_TRY(gemm_sub(h, w - hw, c1 - c0, hw, A + (int64_t)(r + hw) * lda + r, lda,
+                            B + (int64_t)r * ldb + c0, ldb, B + (int64_t)(r + hw) * ldb + c0, ldb));
+    return trsm_lower<T, UNIT>(ctx, h, st, A, lda, r + hw, w - hw, B, ldb, c0, c1);
+}
+
+// X := U^-1 X (TRANS: X := L^-T X with L the lower block stored at (r, r)).
+template <typename T, bool TRANS>
+int trsm_upper(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda,
+                      int r, int w, T *B, int64_t ldb, int c0, int c1) {
+    if (w <= 0 || c1 <= c0) return 0;
+    if (w <= kTrsmLeaf) {
+        int threads = 128;
+        trsm_upper_leaf_kernel<T, TRANS>
+            <<<(unsigned)ceil_div(c1 - c0, threads), threads, 0, st>>>(A, lda, r, w, B, ldb, c0, c1);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+    int hw = (w / 2 + kTrsmLeaf - 1) / kTrsmLeaf * kTrsmLeaf;
+    int rc = trsm_upper<T, TRANS>(ctx, h, st, A, lda, r + hw, w - hw, B, ldb, c0, c1);
+    if (rc) return rc;
+    // B_top -= U_top,bot X_bot   (TRANS: U_top,bot = (L_bot,top)^T)
+    if (TRANS) {
+        const T minus = T(-1), one = T(1);
+        // row-major C[hw x nc] -= (L[bot x top])^T X[bot x nc]; column-major: C^T -= X^T L
+        cublasStatus_t s;
+        if (sizeof(T) == 8)
+            s = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, c1 - c0, hw, w - hw, (const double *)&minus,
+                            (const double *)(B + (int64_t)(r + hw) * ldb + c0), (int)ldb,
+                            (const double *)(A + (int64_t)(r + hw) * lda + r), (int)lda,
+                            (const double *)&one, (double *)(B + (int64_t)r * ldb + c0), (int)ldb);
+        else
+            s = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, c1 - c0, hw, w - hw, (const float *)&minus,
+                            (const float *)(B + (int64_t)(r + hw) * ldb + c0), (int)ldb,
+                            (const float *)(A + (int64_t)(r + hw) * lda + r), (int)lda,
+                            (const float *)&one, (float *)(B + (int64_t)r * ldb + c0), (int)ldb);
+        NMX_CUBLAS_TRY(s);
+    } else {
+        NMX_CUBLAS_TRY(gemm_sub(h, hw, c1 - c0, w - hw, A + (int64_t)r * lda + r + hw, lda,
+                                B + (int64_t)(r + hw) * ldb + c0, ldb, B + (int64_t)r * ldb + c0, ldb));
+    }
+    return trsm_upper<T, TRANS>(ctx, h, st, A, lda, r, hw, B, ldb, c0, c1);
+}
+
+template <typename T>
+static int getrf2(LuRun<T> &R, int c, int w) {
+    if (w <= kLeafW) return leaf<T>(R, c, w);
+    int hw = (w / 2 + kLeafW - 1) / kLeafW * kLeafW;
+    int rc = getrf2<T>(R, c, hw);
+    if (rc) return rc;
+    // U12 := L11^-1 A12 over the right half's columns.
+    rc = trsm_lower<T, true>(R.ctx, R.h, R.st, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+    if (rc) return rc;
+    // A22 -= L21 U12.
+    NMX_CUBLAS_TRY(gemm_sub(R.h, R.n - c - hw, w - hw, hw, R.A + (int64_t)(c + hw) * R.lda + c,
+                            R.lda, R.A + (int64_t)c * R.lda + c + hw, R.lda,
+                            R.A + (int64_t)(c + hw) * R.lda + c + hw, R.lda));
+    return getrf2<T>(R, c + hw, w - hw);
+}
+
+template <typename T>
+static int getrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *ipiv, int32_t *info,
+                 void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 0 && n <= (1 << 20), 2, "n out of range");
+    NMX_ARG_CHECK(A != nullptr || n == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 4, "lda < max(1, n)");
+    NMX_ARG_CHECK(ipiv != nullptr || n == 0, 5, "ipiv is NULL");
+    NMX_ARG_CHECK(info != nullptr, 6, "info is NULL");
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
+    if (n == 0) return 0;
+    cublasHandle_t h;
+    int rc = ctx_cublas(ctx, st, &h);
+    if (rc) return rc;
+    const int G = ctx->sm_count;
+    size_t bytes = sizeof(T) * (2 * (size_t)G * kLeafW + 2 * kLeafW + 2 * G) + sizeof(int) * 2 * G +
+                   64;
+    rc = ctx->ensure_workspace(bytes);
+    if (rc) return rc;
+    char *ws = static_cast<char *>(ctx->workspace);
+    LeafScratch<T> sc;
+    sc.cand_rows = reinterpret_cast<T *>(ws);
+    sc.col_rows = sc.cand_rows + 2 * (size_t)G * kLeafW;
+    sc.cand_mag = sc.col_rows + 2 * kLeafW;
+    sc.cand_row = reinterpret_cast<int *>(sc.cand_mag + 2 * G);
+    sc.bar = reinterpret_cast<unsigned *>(sc.cand_row + 2 * G);
+    sc.err = reinterpret_cast<int *>(sc.bar + 1);
+    NMX_CUDA_TRY(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    // Every CTA of the cooperative leaf must be resident at once.
+    int per_sm = 0;
+    const int m = (int)n;
+    int rpc_max = (int)ceil_div(m, std::min<int64_t>(G, ceil_div(m, 32)));
+    size_t smem = sizeof(T) * ((size_t)rpc_max * (kLeafW + 1) + kLeafW);
+    NMX_CUDA_TRY(cudaFuncSetAttribute(getrf_leaf_kernel<T>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)std::min<size_t>(smem, ctx->smem_optin - 1024)));
+    NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, getrf_leaf_kernel<T>,
+                                                               kLeafThreads, smem));
+    if (per_sm < 1) {
+        set_error("matrix order %lld too large for the leaf panel", (long long)n);
+        return NMX_ERR_UNSUPPORTED;
+    }
+    LuRun<T> R{ctx, st, h, A, lda, (int)n, ipiv, info, sc, G};
+    rc = getrf2<T>(R, 0, (int)n);
+    if (rc) return rc;
+    return 0;
+}
+
+template <typename T>
+static int getrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *LU, int64_t lda,
+                 const int32_t *ipiv, T *B, int64_t ldb, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 0, 2, "n < 0");
+    NMX_ARG_CHECK(nrhs >= 0, 3, "nrhs < 0");
+    NMX_ARG_CHECK(LU != nullptr || n == 0, 4, "LU is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 5, "lda < max(1, n)");
+    NMX_ARG_CHECK(ipiv != nullptr || n == 0, 6, "ipiv is NULL");
+    NMX_ARG_CHECK(B != nullptr || n == 0 || nrhs == 0, 7, "B is NULL");
+    NMX_ARG_CHECK(ldb >= std::max<int64_t>(1, nrhs), 8, "ldb < max(1, nrhs)");
+    if (n == 0 || nrhs == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cublasHandle_t h;
+    int rc = ctx_cublas(ctx, st, &h);
+    if (rc) return rc;
+    int threads = 128;
+    laswp_kernel<T><<<(unsigned)ceil_div(nrhs, threads), threads, 0, st>>>(B, ldb, (int)nrhs, 0,
+                                                                           (int)n, ipiv, 0, 0);
+    NMX_CUDA_TRY(cudaGetLastError());
+    rc = trsm_lower<T, true>(ctx, h, st, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    if (rc) return rc;
+    return trsm_upper<T, false>(ctx, h, st, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+}
+
+// Explicit instantiations used by the Cholesky and IR drivers.
+template int trsm_lower<double, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
+                                      int64_t, int, int, double *, int64_t, int, int);
+template int trsm_lower<float, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
+                                     int, int, float *, int64_t, int, int);
+template int trsm_upper<double, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
+                                       int64_t, int, int, double *, int64_t, int, int);
+template int trsm_upper<float, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
+                                      int, int, float *, int64_t, int, int);
+template int trsm_lower<double, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
+                                       int64_t, int, int, double *, int64_t, int, int);
+template int trsm_lower<float, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
+                                      int, int, float *, int64_t, int, int);
+template int trsm_upper<double, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
+                                      int64_t, int, int, double *, int64_t, int, int);
+template int trsm_upper<float, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
+                                     int, int, float *, int64_t, int, int);
+
+}  // namespace nmx
+
+extern "C" {
+
+NMX_API int nmx_getrf_f64(nmx_ctx ctx, int64_t n, double *A, int64_t lda, int32_t *ipiv,
+                          int32_t *info, void *stream) {
+    return nmx::getrf<double>(ctx, n, A, lda, ipiv, info, stream);
+}
+NMX_API int nmx_getrf_f32(nmx_ctx ctx, int64_t n, float *A, int64_t lda, int32_t *ipiv,
+                          int32_t *info, void *stream) {
+    return nmx::getrf<float>(ctx, n, A, lda, ipiv, info, stream);
+}
+NMX_API int nmx_getrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *LU, int64_t lda,
+                          const int32_t *ipiv, double *B, int64_t ldb, void *stream) {
+    return nmx::getrs<double>(ctx, n, nrhs, LU, lda, ipiv, B, ldb, stream);
+}
+NMX_API int nmx_getrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *LU, int64_t lda,
+                          const int32_t *ipiv, float *B, int64_t ldb, void *stream) {
+    return nmx::getrs<float>(ctx, n, nrhs, LU, lda, ipiv, B, ldb, stream);
+}
+
+}  // extern "C"

@@ -62,6 +62,7 @@ struct nmx_context {
     size_t smem_optin = 0;
     void *workspace = nullptr;
     size_t workspace_bytes = 0;
+    void *cublas = nullptr;  // cublasHandle_t, created on first dense call
     // Returns a device buffer of at least `bytes`, reusing the context's.
     int ensure_workspace(size_t bytes);
 };

@@ -1,0 +1,136 @@
+"""numax.linalg's dense entry points over CUDA tensors, on libnmxla.so.
+
+Mirrors numax's Tensor-tier call surface (numax/linalg/__init__.mojo:323-426):
+
+    lu_factor(a) -> LU            numax/linalg/lu.mojo:454-701
+    LU.solve(b), LU.det(), LU.slogdet()   numax/linalg/lu.mojo:181-451
+    solve(a, b)                   numax/linalg/basic.mojo:55-146
+    cholesky(a)                   numax/linalg/cholesky.mojo:233-468
+    cholesky_solve(lower, b)      numax/linalg/cholesky.mojo:471-580
+    solve_triangular(a, b, ...)   numax/linalg/triangular.mojo:228-425
+
+Operands are torch tensors on a CUDA device standing in for numax's
+`Tensor` over a `DeviceBuffer`: row-major, float64 or float32, 2-D with unit
+column stride (a leading dimension is allowed), vectors 1-D.  Like numax,
+inputs are borrowed and copied into the result's own storage, every call
+synchronizes before returning, and the raised messages are numax's.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _lib
+from .batched import _resolve_device
+
+_SUF = {torch.float64: "f64", torch.float32: "f32"}
+
+
+def _check_matrix(name, a, square=True):
+    if not isinstance(a, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if a.device.type != "cuda":
+        raise ValueError(f"{name} must be on a CUDA device (numax_b200 has no CPU path)")
+    if a.dtype not in _SUF:
+        raise TypeError(f"{name}: dtype {a.dtype} is not float32/float64")
+    if a.dim() != 2:
+        raise ValueError(f"{name} must be 2-D")
+    if square and a.shape[0] != a.shape[1]:
+        raise ValueError(f"{name} must be square, got {tuple(a.shape)}")
+
+
+def _dense_copy(a):
+    """A contiguous copy (numax copies its input into its own workspace)."""
+    return a.contiguous().clone()
+
+
+def _stream(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _ctx(dev):
+    return _lib.context(dev.index)
+
+
+def _as_rhs(b, n, dtype, device):
+    if not isinstance(b, torch.Tensor) or b.device != device or b.dtype != dtype:
+        raise TypeError("b must be a tensor with the matrix's dtype on its device")
+    if b.shape[0] != n or b.dim() not in (1, 2):
+        raise ValueError(f"b must have {n} rows")
+    x = b.reshape(n, -1).contiguous().clone()
+    return x
+
+
+class LU:
+    """A blocked LU with partial pivoting (numax's `LU`, numax/linalg/lu.mojo:75-451).
+
+    `factored` holds L below the diagonal (unit diagonal implicit) and U on
+    and above it; `pivots[j]` is the row column j interchanged with
+    (0-based, LAPACK's ipiv convention); `sign` is the swap parity.
+    """
+
+    def __init__(self, factored, pivots, sign, info):
+        self.factored = factored
+        self.pivots = pivots
+        self.sign = sign
+        self.info = info
+        self.n = factored.shape[0]
+
+    def solve(self, b):
+        """x with A x = b (vector or matrix b), reusing the factorization."""
+        a = self.factored
+        x = _as_rhs(b, self.n, a.dtype, a.device)
+        if self.n:
+            _lib.call(f"nmx_getrs_{_SUF[a.dtype]}", _ctx(a.device), self.n, x.shape[1], a.data_ptr(),
+                      a.stride(0), self.pivots.data_ptr(), x.data_ptr(), x.shape[1], _stream(a.device))
+        torch.cuda.current_stream(a.device).synchronize()
+        return x.reshape(b.shape)
+
+    def det(self):
+        """det(A) = sign * prod(diag(U)) (numax/linalg/lu.mojo:382-451)."""
+        return self.sign * torch.prod(torch.diagonal(self.factored)).item()
+
+    def slogdet(self):
+        """(sign, log|det|) like numpy.linalg.slogdet."""
+        d = torch.diagonal(self.factored)
+        if bool((d == 0).any()):
+            return 0.0, -math.inf
+        sign = self.sign * (1 if int((d < 0).sum().item()) % 2 == 0 else -1)
+        return float(sign), float(torch.log(torch.abs(d)).sum().item())
+
+
+def lu_factor(a) -> LU:
+    """Factor a (n x n) into P L U with partial pivoting, on a's device.
+
+    Rank deficiency is not an error (numax/linalg/lu.mojo:96-98): an exactly
+    zero pivot column leaves `info` = its 1-based index and the solves then
+    produce non-finite values."""
+    _check_matrix("a", a)
+    dev = _resolve_device(a.device)
+    n = a.shape[0]
+    f = _dense_copy(a)
+    piv = torch.zeros(n, dtype=torch.int32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call(f"nmx_getrf_{_SUF[a.dtype]}", _ctx(dev), n, f.data_ptr(), f.stride(0) if n else 1,
+              piv.data_ptr(), info.data_ptr(), _stream(dev))
+    host = piv.cpu()
+    torch.cuda.current_stream(dev).synchronize()
+    sign = 1
+    if n:
+        swaps = int((host != torch.arange(n, dtype=torch.int32)).sum().item())
+        sign = -1 if swaps % 2 else 1
+    return LU(f, piv, sign, int(info.item()))
+
+
+def solve(a, b):
+    """x with a x = b (numax/linalg/basic.mojo:55-146)."""
+    return lu_factor(a).solve(b)
+
+
+def det(a):
+    return lu_factor(a).det()
+
+
+def slogdet(a):
+    return lu_factor(a).slogdet()

@@ -1,0 +1,116 @@
+"""Batched uneven Jacobi eigh on the GPU vs float64 references: the oracle's
+restatement of numax's Array-tier eigh (12 cyclic sweeps, run in float64)
+and LAPACK.  Eigenvalues compared sorted (parallel ordering permutes the
+diagonal relative to numax's cyclic order); eigenvectors by residual and
+orthogonality, which are invariant to column order and sign.
+
+Tolerance (float32 data, north star): |w - w_ref| <= 1e-5 * ||A||_2 per
+eigenvalue; residual ||A v - w v|| and ||V^T V - I|| within 1e-5 * n."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def well(omega, n=24):
+    """examples/advanced/quantum_well.mojo:66-75: grid on [-4, 4]."""
+    dx = 8.0 / (n - 1)
+    h = np.zeros((n, n))
+    x = -4.0
+    for i in range(n):
+        h[i, i] = 1.0 / dx ** 2 + omega * omega * x * x / 2
+        if i + 1 < n:
+            h[i, i + 1] = h[i + 1, i] = -0.5 / dx ** 2
+        x += dx
+    return h
+
+
+def make_batch(ns, seed, wells=0):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mats = []
+    for i, n in enumerate(ns):
+        if i < wells:
+            mats.append(well(rng.uniform(0.5, 2.0), n))
+        else:
+            g = rng.standard_normal((n, n))
+            mats.append((g + g.T) / 2)
+    return mats
+
+
+def run(ns, mats, sort=True, tol=1e-7, max_sweeps=20):
+    import numax_b200 as nb
+    A = torch.from_numpy(np.concatenate([m.astype(np.float32).ravel() for m in mats])).cuda()
+    plan = nb.EighBatch(ns)
+    W, V, sweeps = plan(A, sort=sort, tol=tol, max_sweeps=max_sweeps)
+    return W.cpu().numpy(), V.cpu().numpy(), sweeps.cpu().numpy()
+
+
+def test_batched_eigh_matches_float64_references(oracle):
+    edge = [1, 2, 3, 16, 24, 31, 32, 33, 63, 64]
+    rng = np.random.Generator(np.random.PCG64(2))
+    ns = np.array([24] * 60 + edge + list(rng.integers(16, 65, size=140)), dtype=np.int32)
+    mats = make_batch(ns, seed=4, wells=60)
+    W, V, sweeps = run(ns, mats, sort=True)
+    wo, ao = oracle.ragged_offsets(ns, 1), oracle.ragged_offsets(ns)
+    worst_w = worst_res = worst_orth = 0.0
+    for i, (n, a) in enumerate(zip(ns, mats)):
+        w = W[wo[i]:wo[i] + n]
+        v = V[ao[i]:ao[i] + n * n].reshape(n, n).astype(np.float64)
+        scale = max(np.abs(np.linalg.eigvalsh(a)).max(), 1e-30)
+        ref = np.linalg.eigvalsh(a)
+        jac, _ = oracle.jacobi_eigh(a, sweeps=12)
+        assert np.all(np.diff(w) >= 0)
+        np.testing.assert_allclose(np.sort(jac), ref, atol=1e-10 * scale)
+        worst_w = max(worst_w, np.abs(w - ref).max() / scale)
+        worst_res = max(worst_res, np.abs(a @ v - v * w).max() / scale / n)
+        worst_orth = max(worst_orth, np.abs(v.T @ v - np.eye(n)).max() / n)
+    assert worst_w <= 1e-5, worst_w
+    assert worst_res <= 1e-5, worst_res
+    assert worst_orth <= 1e-5, worst_orth
+    assert sweeps.max() <= 20
+
+
+def test_batched_eigh_unsorted_is_a_permutation_of_sorted():
+    ns = np.array([5, 40, 24, 64], dtype=np.int32)
+    mats = make_batch(ns, seed=8, wells=0)
+    Ws, _, _ = run(ns, mats, sort=True)
+    Wu, Vu, _ = run(ns, mats, sort=False)
+    off = 0
+    for n, a in zip(ns, mats):
+        np.testing.assert_array_equal(np.sort(Wu[off:off + n]), Ws[off:off + n])
+        off += n
+
+
+def test_batched_eigh_invariants_from_numax_tests(oracle):
+    # tests/linalg/test_linalg.mojo:576-645: trace, diagonal input, identity.
+    spd3 = np.array([[4.0, 2.0, 1.0], [2.0, 5.0, 3.0], [1.0, 3.0, 6.0]])
+    diag = np.diag([3.0, -1.0, 7.0])
+    ident = np.eye(3)
+    ns = np.array([3, 3, 3], dtype=np.int32)
+    W, V, sweeps = run(ns, [spd3, diag, ident], sort=True)
+    assert abs(W[0:3].sum() - 15.0) < 1e-5
+    assert (W[0:3] > 0).all()
+    np.testing.assert_allclose(W[3:6], [-1.0, 3.0, 7.0], atol=1e-6)
+    np.testing.assert_allclose(W[6:9], 1.0, atol=1e-7)
+    # A diagonal input needs no sweep at all.
+    assert sweeps[1] == 0 and sweeps[2] == 0
+
+
+def test_batched_eigh_fixed_sweeps_like_numax(oracle):
+    # tol = 0 runs exactly max_sweeps sweeps, numax's fixed-trip-count mode.
+    ns = np.array([24, 40], dtype=np.int32)
+    mats = make_batch(ns, seed=6, wells=1)
+    W, V, sweeps = run(ns, mats, sort=True, tol=0.0, max_sweeps=12)
+    assert list(sweeps) == [12, 12]
+    for (n, a), off in zip(zip(ns, mats), (0, 24)):
+        jac, _ = oracle.jacobi_eigh(a, sweeps=12)
+        scale = np.abs(jac).max()
+        np.testing.assert_allclose(W[off:off + n], np.sort(jac), atol=1e-5 * scale)
+
+
+def test_batched_eigh_rejects_bad_sizes():
+    import numax_b200 as nb
+    with pytest.raises(nb._lib.NmxError):
+        nb.EighBatch(np.array([65], dtype=np.int32))
