@@ -158,6 +158,31 @@ NMX_API int nmx_getrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *LU
 NMX_API int nmx_getrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *LU, int64_t lda,
                           const int32_t *ipiv, float *B, int64_t ldb, void *stream);
 
+/* ---- dense Cholesky and its solve ----------------------------------------
+ *
+ * nmx_potrf_*: factor the SPD n x n row-major A (lda) in place into L L^T,
+ * reading only the lower triangle -- numax's cholesky
+ * (numax/linalg/cholesky.mojo:59-396) with potrf_diag's failure rule
+ * (numax/linalg/panel.mojo:216-286): a pivot d <= 0 is floored to 1e-30 and
+ * the factorization continues; *info (device int32) receives the 1-based
+ * index of the first such pivot, 0 if none.  On return the lower triangle
+ * holds L and the upper triangle is zeroed (numax's `tril`,
+ * numax/linalg/cholesky.mojo:396).  numax raises "cholesky: matrix is not
+ * positive definite (non-positive pivot at index i)" with i = info - 1; the
+ * front ends reproduce that from info.
+ *
+ * nmx_potrs_*: B := A^-1 B from L: L y = b, then L^T x = y reading L in place
+ * (numax's cholesky_solve, numax/linalg/cholesky.mojo:471-580).
+ */
+NMX_API int nmx_potrf_f64(nmx_ctx ctx, int64_t n, double *A, int64_t lda, int32_t *info,
+                          void *stream);
+NMX_API int nmx_potrf_f32(nmx_ctx ctx, int64_t n, float *A, int64_t lda, int32_t *info,
+                          void *stream);
+NMX_API int nmx_potrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *L, int64_t lda,
+                          double *B, int64_t ldb, void *stream);
+NMX_API int nmx_potrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *L, int64_t lda,
+                          float *B, int64_t ldb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,10 @@ SIGNATURES = {
     "nmx_getrf_f32": (ci, [vp, i64, vp, i64, vp, vp, vp]),
     "nmx_getrs_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
     "nmx_getrs_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
+    "nmx_potrf_f64": (ci, [vp, i64, vp, i64, vp, vp]),
+    "nmx_potrf_f32": (ci, [vp, i64, vp, i64, vp, vp]),
+    "nmx_potrs_f64": (ci, [vp, i64, i64, vp, i64, vp, i64, vp]),
+    "nmx_potrs_f32": (ci, [vp, i64, i64, vp, i64, vp, i64, vp]),
 }
 
 

@@ -48,66 +48,92 @@ struct BatchedPotrfArgs {
     int nrhs;
 };
 
-// Shared-memory words (of T) one CTA needs for matrices up to nmax.
+// Shared-memory words (of T) one CTA needs for matrices up to nmax: the
+// packed lower triangle (row i at i(i+1)/2), nrhs full rows of B^T below it,
+// and a 16 x nrhs staging block for the back solve.  The inverse of each
+// 16x16 diagonal block is kept in place of that block once the block of L
+// has been written out.
 __host__ __device__ inline int potrf_smem_elems(int nmax, int nrhs) {
-    int ld = nmax | 1;
-    return (nmax + nrhs) * ld + nmax + kDiagNB * kPotrfMaxRhs;
+    return nmax * (nmax + 1) / 2 + nrhs * nmax + kDiagNB * kPotrfMaxRhs + 2;
 }
 
-// Factor the kb x kb diagonal block at (k, k) in place (lower), one warp.
-// Stores W = inverse of the block's L: W[i][j] (i > j) transposed into the
-// unused upper triangle at S[(k+j)*ld + k+i], W[j][j] = 1/l_jj in dinv[k+j].
+// Start of row i in the packed store: the lower triangle's rows, then the
+// right-hand sides' rows (length n) below them.
+__device__ __forceinline__ int prow_off(int i, int n) {
+    return i < n ? (i * (i + 1)) / 2 : (n * (n + 1)) / 2 + (i - n) * n;
+}
+
+// One warp factors the kb x kb diagonal block at (k, k) in registers (lane i
+// holds row i) with numax's Array-tier rule l_jj = sqrt(guard_nonzero(d,
+// 1e-30)) (a negative d gives NaN; info records the first d <= 0), writes
+// the block of L to global memory, then replaces it in shared memory by
+// W = L_kk^-1 (lower, W[i][i] = 1/l_ii), formed by a right-looking
+// substitution with lane j holding column j.
 template <typename T>
-__device__ __forceinline__ void potrf_diag_warp(T *S, int ld, int k, int kb, T *dinv, int lane,
-                                                int *s_info) {
+__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *Lg, int lane,
+                                                 int *s_info) {
     const T floor_ = pivot_floor<T>::value;
-    for (int j = 0; j < kb; ++j) {
-        T d = S[(k + j) * ld + k + j];
-        if (lane == 0 && d <= T(0) && *s_info == 0) *s_info = k + j + 1;
-        T ljj = sqrt(guard_nonzero(d, floor_));
-        __syncwarp();
-        if (lane > j && lane < kb) S[(k + lane) * ld + k + j] = S[(k + lane) * ld + k + j] / ljj;
-        if (lane == j) S[(k + j) * ld + k + j] = ljj;
-        __syncwarp();
-        if (lane > j && lane < kb) {
-            T lij = S[(k + lane) * ld + k + j];
-            for (int c = j + 1; c <= lane; ++c)
-                S[(k + lane) * ld + k + c] -= lij * S[(k + c) * ld + k + j];
-        }
-        __syncwarp();
-    }
-    // Column `lane` of W = L^-1: W[j][j] = 1/l_jj, W[i][j] = -(sum_{p=j}^{i-1} l_ip W[p][j]) / l_ii.
-    if (lane < kb) {
-        const int j = lane;
-        T w[kDiagNB];
+    T a[kDiagNB];
+    const int ro = prow_off(k + lane, n) + k;
 #pragma unroll
-        for (int i = 0; i < kDiagNB; ++i) w[i] = T(0);
-        T wjj = T(1) / guard_nonzero(S[(k + j) * ld + k + j], floor_);
-        dinv[k + j] = wjj;
+    for (int c = 0; c < kDiagNB; ++c) a[c] = (lane < kb && c <= lane) ? S[ro + c] : T(0);
 #pragma unroll
-        for (int i = 0; i < kDiagNB; ++i) {
-            if (i == j) w[i] = wjj;
-            if (i > j && i < kb) {
-                T s = T(0);
+    for (int j = 0; j < kDiagNB; ++j) {
+        if (j < kb) {  // warp-uniform
+            const T d = __shfl_sync(0xffffffffu, a[j], j);
+            if (lane == 0 && d <= T(0) && *s_info == 0) *s_info = k + j + 1;
+            const T g = guard_nonzero(d, floor_);
+            const T inv = rsqrt(g);
+            if (lane == j) a[j] = g * inv;
+            if (lane > j) a[j] *= inv;
+            const T lij = a[j];
 #pragma unroll
-                for (int p = 0; p < kDiagNB; ++p)
-                    if (p >= j && p < i) s += S[(k + i) * ld + k + p] * w[p];
-                w[i] = -s / guard_nonzero(S[(k + i) * ld + k + i], floor_);
-                S[(k + j) * ld + k + i] = w[i];
+            for (int c = j + 1; c < kDiagNB; ++c) {
+                const T lcj = __shfl_sync(0xffffffffu, lij, c);
+                if (lane > j && c <= lane) a[c] -= lij * lcj;
             }
         }
+    }
+    T myinv = T(0);
+    if (lane < kb) {
+        T *lrow = Lg + (int64_t)(k + lane) * n + k;
+#pragma unroll
+        for (int c = 0; c < kDiagNB; ++c)
+            if (c <= lane) {
+                S[ro + c] = a[c];
+                lrow[c] = a[c];
+            }
+        myinv = T(1) / guard_nonzero(a[lane], floor_);
+    }
+    __syncwarp();
+    // Column `lane` of W: w = L^-1 e_lane, right-looking over the rows of L.
+    T w[kDiagNB];
+#pragma unroll
+    for (int i = 0; i < kDiagNB; ++i) w[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll
+    for (int p = 0; p < kDiagNB; ++p) {
+        if (p < kb) {
+            w[p] *= __shfl_sync(0xffffffffu, myinv, p);
+#pragma unroll
+            for (int i = p + 1; i < kDiagNB; ++i)
+                if (i < kb) w[i] -= S[prow_off(k + i, n) + k + p] * w[p];
+        }
+    }
+    __syncwarp();
+    if (lane < kb) {
+#pragma unroll
+        for (int i = 0; i < kDiagNB; ++i)
+            if (i >= lane && i < kb) S[prow_off(k + i, n) + k + lane] = w[i];
     }
     __syncwarp();
 }
 
 template <typename T, int NT>
-__device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *dinv, T *xb,
-                                int *s_info) {
+__device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *xb, int *s_info) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
     const int n = args.ns[mi];
     const int nrhs = args.nrhs;
-    const int ld = n | 1;
     const int R = n + nrhs;  // rows of the augmented block [A; B^T]
     const T *A = static_cast<const T *>(args.A) + args.a_off[mi];
     T *L = static_cast<T *>(args.L) + args.a_off[mi];
@@ -116,33 +142,40 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *d
     if (tid == 0) *s_info = 0;
 
     // Stage the lower triangle (row i: i+1 contiguous elements) and B^T.
-    for (int i = warp; i < n; i += NW)
-        for (int j = lane; j <= i; j += 32) S[i * ld + j] = A[(int64_t)i * n + j];
+    for (int i = warp; i < n; i += NW) {
+        const int ro = (i * (i + 1)) / 2;
+        for (int j = lane; j <= i; j += 32) S[ro + j] = A[(int64_t)i * n + j];
+    }
+    const int bro = (n * (n + 1)) / 2;
     for (int e = tid; e < n * nrhs; e += NT) {
         int j = e / nrhs, r = e - j * nrhs;
-        S[(n + r) * ld + j] = B[e];
+        S[bro + r * n + j] = B[e];
     }
     __syncthreads();
 
     for (int k = 0; k < n; k += kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        if (warp == 0) potrf_diag_warp<T>(S, ld, k, kb, dinv, lane, s_info);
+        if (warp == 0) potrf_diag_block<T>(S, n, k, kb, L, lane, s_info);
         __syncthreads();
 
-        // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T.
+        // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T, W
+        // (the block's inverse) sitting where the block of L was.
         const int r0 = k + kb;
+        int wro[kDiagNB];
+#pragma unroll
+        for (int j = 0; j < kDiagNB; ++j) wro[j] = prow_off(k + min(j, kb - 1), n) + k;
         for (int r = r0 + tid; r < R; r += NT) {
+            const int ro = prow_off(r, n) + k;
             T a[kDiagNB];
 #pragma unroll
-            for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[r * ld + k + j] : T(0);
+            for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[ro + j] : T(0);
 #pragma unroll
             for (int j = 0; j < kDiagNB; ++j) {
                 if (j < kb) {
-                    T out = a[j] * dinv[k + j];
+                    T out = T(0);
 #pragma unroll
-                    for (int i = 0; i < kDiagNB; ++i)
-                        if (i < j) out += a[i] * S[(k + i) * ld + k + j];
-                    S[r * ld + k + j] = out;
+                    for (int i = 0; i <= j; ++i) out += a[i] * S[wro[j] + i];
+                    S[ro + j] = out;
                 }
             }
         }
@@ -175,8 +208,8 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *d
                 int ir[4], jr[4];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
-                    ir[a] = min(i0 + a, R - 1) * ld + k;
-                    jr[a] = min(j0 + a, n - 1) * ld + k;
+                    ir[a] = prow_off(min(i0 + a, R - 1), n) + k;
+                    jr[a] = prow_off(min(j0 + a, n - 1), n) + k;
                 }
                 for (int p = 0; p < kb; ++p) {
                     T x[4], y[4];
@@ -194,8 +227,8 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *d
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
-                        int i = i0 + a, j = j0 + b;
-                        if (i < R && j < n && j <= i) S[i * ld + j] -= acc[a][b];
+                        const int i = i0 + a, j = j0 + b;
+                        if (i < R && j < n && j <= i) S[ir[a] - k + j] -= acc[a][b];
                     }
             }
         }
@@ -206,49 +239,51 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *d
     // L^T x = y, 16-row blocks bottom-up, with the stored block inverses.
     for (int k = ((n - 1) / kDiagNB) * kDiagNB; k >= 0; k -= kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        // x_blk = W^T y_blk, W the block's inverse.
-        if (tid < kb * nrhs) {
-            int j = tid / nrhs, c = tid - j * nrhs;
-            const T *y = S + (n + c) * ld + k;
-            T s = dinv[k + j] * y[j];
-            for (int i = j + 1; i < kb; ++i) s += S[(k + j) * ld + k + i] * y[i];
+        if (tid < kb * nrhs) {  // x_blk = W^T y_blk
+            const int j = tid / nrhs, c = tid - j * nrhs;
+            const T *y = S + bro + c * n + k;
+            T s = T(0);
+            for (int i = j; i < kb; ++i) s += S[prow_off(k + i, n) + k + j] * y[i];
             xb[j * kPotrfMaxRhs + c] = s;
         }
         __syncthreads();
         if (tid < kb * nrhs) {
-            int j = tid / nrhs, c = tid - j * nrhs;
-            S[(n + c) * ld + k + j] = xb[j * kPotrfMaxRhs + c];
+            const int j = tid / nrhs, c = tid - j * nrhs;
+            S[bro + c * n + k + j] = xb[j * kPotrfMaxRhs + c];
         }
-        // y[0:k] -= L[k:k+kb, 0:k]^T x_blk
-        for (int e = tid; e < k * nrhs; e += NT) {
-            int i = e / nrhs, c = e - i * nrhs;
+        for (int e = tid; e < k * nrhs; e += NT) {  // y[0:k] -= L[k:k+kb, 0:k]^T x_blk
+            const int i = e / nrhs, c = e - i * nrhs;
             T s = T(0);
-            for (int j = 0; j < kb; ++j) s += S[(k + j) * ld + i] * xb[j * kPotrfMaxRhs + c];
-            S[(n + c) * ld + i] -= s;
+            for (int j = 0; j < kb; ++j) s += S[prow_off(k + j, n) + i] * xb[j * kPotrfMaxRhs + c];
+            S[bro + c * n + i] -= s;
         }
         __syncthreads();
     }
 
-    // Write back L (lower triangle) and X.
-    for (int i = warp; i < n; i += NW)
-        for (int j = lane; j <= i; j += 32) L[(int64_t)i * n + j] = S[i * ld + j];
+    // Write back L's off-diagonal blocks (the diagonal blocks went out as
+    // they were factored) and X.
+    for (int i = warp; i < n; i += NW) {
+        const int ro = (i * (i + 1)) / 2;
+        const int jend = (i / kDiagNB) * kDiagNB;
+        for (int j = lane; j < jend; j += 32) L[(int64_t)i * n + j] = S[ro + j];
+    }
     for (int e = tid; e < n * nrhs; e += NT) {
         int j = e / nrhs, r = e - j * nrhs;
-        X[e] = S[(n + r) * ld + j];
+        X[e] = S[bro + r * n + j];
     }
     if (tid == 0) args.info[mi] = *s_info;
     __syncthreads();
 }
 
+// CTAs per SM each thread count is tuned for (register budget).
+__host__ __device__ constexpr int potrf_min_blocks(int nt) { return nt >= 256 ? 3 : (nt >= 128 ? 6 : 12); }
+
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) potrf_potrs_batched_kernel(BatchedPotrfArgs args, int begin,
-                                                                 int end, int nmax,
-                                                                 int *counter) {
+__global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
+    potrf_potrs_batched_kernel(BatchedPotrfArgs args, int begin, int end, int nmax, int *counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *S = reinterpret_cast<T *>(smem_raw);
-    const int ld = nmax | 1;
-    T *dinv = S + (nmax + args.nrhs) * ld;
-    T *xb = dinv + nmax;
+    T *xb = S + nmax * (nmax + 1) / 2 + args.nrhs * nmax;
     __shared__ int s_item, s_info;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -256,7 +291,7 @@ __global__ void __launch_bounds__(NT) potrf_potrs_batched_kernel(BatchedPotrfArg
         const int item = begin + s_item;
         __syncthreads();
         if (item >= end) break;
-        potrf_potrs_one<T, NT>(args, args.order[item], S, dinv, xb, &s_info);
+        potrf_potrs_one<T, NT>(args, args.order[item], S, xb, &s_info);
     }
 }
 

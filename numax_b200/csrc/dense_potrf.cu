@@ -1,0 +1,218 @@
+// Dense Cholesky and cholesky_solve (sm_100a), row-major, lower.
+//
+// numax's cholesky (numax/linalg/cholesky.mojo:59-396) is right-looking and
+// blocked (block 32 on a device): potrf_diag on the diagonal block
+// (numax/linalg/panel.mojo:216-286), trsm_right_lower_t on the panel below it
+// (numax/linalg/panel.mojo:2316-2408), and the symmetric trailing update in
+// MAX's matmul.  Here the same three steps run recursively over halves, so
+// the trailing updates are few large SYRK/GEMM calls:
+//
+//   potrf(A11); L21 := A21 L11^-T; A22 -= L21 L21^T; potrf(A22)
+//
+// with 32-column leaves factored by one warp in registers.  The leaf keeps
+// numax's rule: a pivot d <= 0 is recorded in info (first one, 1-based) and
+// floored to 1e-30 so the factorization continues and stays finite.  Only
+// the lower triangle is read; the upper triangle is zeroed at the end, as
+// numax's `tril` does (numax/linalg/cholesky.mojo:396).
+#include <algorithm>
+
+#include "dense_common.cuh"
+
+namespace nmx {
+
+constexpr int kCholLeaf = 32;
+
+// One warp: Cholesky of the w x w (w <= 32) diagonal block at (c, c).
+template <typename T>
+__global__ void potrf_leaf_kernel(T *A, int64_t lda, int c, int w, int32_t *info) {
+    const int lane = threadIdx.x;
+    T a[kCholLeaf];
+    T *row = A + (int64_t)(c + lane) * lda + c;
+#pragma unroll
+    for (int j = 0; j < kCholLeaf; ++j) a[j] = (lane < w && j <= lane) ? row[j] : T(0);
+    int first_bad = 0;
+#pragma unroll
+    for (int j = 0; j < kCholLeaf; ++j) {
+        if (j < w) {
+            T d = __shfl_sync(0xffffffffu, a[j], j);
+            if (d <= T(0)) {
+                if (first_bad == 0) first_bad = c + j + 1;
+                d = pivot_floor<T>::value;
+            }
+            const T root = sqrt(d);
+            if (lane == j) a[j] = root;
+            if (lane > j) a[j] = a[j] / root;
+            const T lij = a[j];
+#pragma unroll
+            for (int cc = j + 1; cc < kCholLeaf; ++cc) {
+                const T lcj = __shfl_sync(0xffffffffu, lij, cc);
+                if (lane > j && cc <= lane) a[cc] -= lij * lcj;
+            }
+        }
+    }
+    if (lane < w) {
+#pragma unroll
+        for (int j = 0; j < kCholLeaf; ++j)
+            if (j <= lane) row[j] = a[j];
+    }
+    if (lane == 0 && first_bad && *info == 0) *info = first_bad;
+}
+
+// X := X L^-T for X = rows [r0, r1) x cols [c, c+w) of A and L the w x w
+// (w <= 32) lower block at (c, c).  One thread per row.
+template <typename T>
+__global__ void trsm_right_lt_leaf_kernel(T *A, int64_t lda, int c, int w, int r0, int r1) {
+    __shared__ T Ls[kCholLeaf][kCholLeaf + 1];
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        int i = e / w, j = e - i * w;
+        Ls[i][j] = A[(int64_t)(c + i) * lda + c + j];
+    }
+    __syncthreads();
+    const int r = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= r1) return;
+    T *row = A + (int64_t)r * lda + c;
+    T x[kCholLeaf];
+#pragma unroll
+    for (int j = 0; j < kCholLeaf; ++j) x[j] = j < w ? row[j] : T(0);
+#pragma unroll
+    for (int j = 0; j < kCholLeaf; ++j) {
+        if (j < w) {
+            T acc = T(0);
+#pragma unroll
+            for (int p = 0; p < kCholLeaf; ++p)
+                if (p < j) acc += x[p] * Ls[j][p];
+            x[j] = (x[j] - acc) / Ls[j][j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kCholLeaf; ++j)
+        if (j < w) row[j] = x[j];
+}
+
+template <typename T>
+__global__ void zero_upper_kernel(T *A, int64_t lda, int n) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * n) return;
+    const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
+    if (j > i) A[(int64_t)i * lda + j] = T(0);
+}
+
+inline cublasStatus_t syrk_sub(cublasHandle_t h, int64_t n, int64_t k, const double *A, int64_t lda,
+                               double *C, int64_t ldc) {
+    const double minus = -1.0, one = 1.0;
+    return cublasDsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)n, (int)k, &minus, A, (int)lda,
+                       &one, C, (int)ldc);
+}
+inline cublasStatus_t syrk_sub(cublasHandle_t h, int64_t n, int64_t k, const float *A, int64_t lda,
+                               float *C, int64_t ldc) {
+    const float minus = -1.0f, one = 1.0f;
+    return cublasSsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)n, (int)k, &minus, A, (int)lda,
+                       &one, C, (int)ldc);
+}
+
+// X := X L^-T, X = rows [r0, r1) x cols [c, c+w), L the lower block at (c, c).
+template <typename T>
+static int trsm_right_lt(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c, int w, int r0,
+                         int r1) {
+    if (w <= 0 || r1 <= r0) return 0;
+    if (w <= kCholLeaf) {
+        const int threads = 128;
+        trsm_right_lt_leaf_kernel<T>
+            <<<(unsigned)ceil_div(r1 - r0, threads), threads, 0, st>>>(A, lda, c, w, r0, r1);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+    const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
+    int rc = trsm_right_lt<T>(h, st, A, lda, c, hw, r0, r1);
+    if (rc) return rc;
+    // X_b -= X_a L_ba^T, L_ba = rows [c+hw, c+w) x cols [c, c+hw).
+    NMX_CUBLAS_TRY(gemm_sub_bt(h, r1 - r0, w - hw, hw, A + (int64_t)r0 * lda + c, lda,
+                               A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)r0 * lda + c + hw,
+                               lda));
+    return trsm_right_lt<T>(h, st, A, lda, c + hw, w - hw, r0, r1);
+}
+
+template <typename T>
+static int potrf_rec(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c, int w,
+                     int32_t *info) {
+    if (w <= kCholLeaf) {
+        potrf_leaf_kernel<T><<<1, 32, 0, st>>>(A, lda, c, w, info);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+    const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
+    int rc = potrf_rec<T>(h, st, A, lda, c, hw, info);
+    if (rc) return rc;
+    rc = trsm_right_lt<T>(h, st, A, lda, c, hw, c + hw, c + w);
+    if (rc) return rc;
+    // A22 -= L21 L21^T on the lower triangle (column-major upper).
+    NMX_CUBLAS_TRY(syrk_sub(h, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
+                            A + (int64_t)(c + hw) * lda + c + hw, lda));
+    return potrf_rec<T>(h, st, A, lda, c + hw, w - hw, info);
+}
+
+template <typename T>
+static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 0 && n <= (1 << 20), 2, "n out of range");
+    NMX_ARG_CHECK(A != nullptr || n == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 4, "lda < max(1, n)");
+    NMX_ARG_CHECK(info != nullptr, 5, "info is NULL");
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
+    if (n == 0) return 0;
+    cublasHandle_t h;
+    int rc = ctx_cublas(ctx, st, &h);
+    if (rc) return rc;
+    rc = potrf_rec<T>(h, st, A, lda, 0, (int)n, info);
+    if (rc) return rc;
+    const int threads = 256;
+    zero_upper_kernel<T><<<(unsigned)ceil_div(n * n, threads), threads, 0, st>>>(A, lda, (int)n);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+static int potrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *L, int64_t lda, T *B, int64_t ldb,
+                 void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 0, 2, "n < 0");
+    NMX_ARG_CHECK(nrhs >= 0, 3, "nrhs < 0");
+    NMX_ARG_CHECK(L != nullptr || n == 0, 4, "L is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 5, "lda < max(1, n)");
+    NMX_ARG_CHECK(B != nullptr || n == 0 || nrhs == 0, 6, "B is NULL");
+    NMX_ARG_CHECK(ldb >= std::max<int64_t>(1, nrhs), 7, "ldb < max(1, nrhs)");
+    if (n == 0 || nrhs == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cublasHandle_t h;
+    int rc = ctx_cublas(ctx, st, &h);
+    if (rc) return rc;
+    rc = trsm_lower<T, false>(ctx, h, st, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    if (rc) return rc;
+    return trsm_upper<T, true>(ctx, h, st, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+}
+
+}  // namespace nmx
+
+extern "C" {
+
+NMX_API int nmx_potrf_f64(nmx_ctx ctx, int64_t n, double *A, int64_t lda, int32_t *info,
+                          void *stream) {
+    return nmx::potrf<double>(ctx, n, A, lda, info, stream);
+}
+NMX_API int nmx_potrf_f32(nmx_ctx ctx, int64_t n, float *A, int64_t lda, int32_t *info,
+                          void *stream) {
+    return nmx::potrf<float>(ctx, n, A, lda, info, stream);
+}
+NMX_API int nmx_potrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *L, int64_t lda,
+                          double *B, int64_t ldb, void *stream) {
+    return nmx::potrs<double>(ctx, n, nrhs, L, lda, B, ldb, stream);
+}
+NMX_API int nmx_potrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *L, int64_t lda,
+                          float *B, int64_t ldb, void *stream) {
+    return nmx::potrs<float>(ctx, n, nrhs, L, lda, B, ldb, stream);
+}
+
+}  // extern "C"

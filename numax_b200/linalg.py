@@ -134,3 +134,36 @@ def det(a):
 
 def slogdet(a):
     return lu_factor(a).slogdet()
+
+
+def cholesky(a):
+    """The lower-triangular L with L L^T = a, upper triangle zero
+    (numax/linalg/cholesky.mojo:233-396).  Reads only a's lower triangle.
+
+    Raises numax's error when a is not positive definite: the factorization
+    runs to the end with the failing pivots floored, then reports the first."""
+    _check_matrix("a", a)
+    dev = _resolve_device(a.device)
+    n = a.shape[0]
+    l = _dense_copy(a)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call(f"nmx_potrf_{_SUF[a.dtype]}", _ctx(dev), n, l.data_ptr(), l.stride(0) if n else 1,
+              info.data_ptr(), _stream(dev))
+    flag = int(info.item())
+    if flag != 0:
+        raise ValueError("cholesky: matrix is not positive definite (non-positive pivot at index "
+                         f"{flag - 1})")
+    return l
+
+
+def cholesky_solve(lower, b):
+    """x with (L L^T) x = b from cholesky's L (numax/linalg/cholesky.mojo:471-580)."""
+    _check_matrix("lower", lower)
+    n = lower.shape[0]
+    x = _as_rhs(b, n, lower.dtype, lower.device)
+    L = lower.contiguous()
+    if n:
+        _lib.call(f"nmx_potrs_{_SUF[lower.dtype]}", _ctx(lower.device), n, x.shape[1], L.data_ptr(),
+                  L.stride(0), x.data_ptr(), x.shape[1], _stream(lower.device))
+    torch.cuda.current_stream(lower.device).synchronize()
+    return x.reshape(b.shape)

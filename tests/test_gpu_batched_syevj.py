@@ -99,11 +99,14 @@ def test_batched_eigh_invariants_from_numax_tests(oracle):
 
 
 def test_batched_eigh_fixed_sweeps_like_numax(oracle):
-    # tol = 0 runs exactly max_sweeps sweeps, numax's fixed-trip-count mode.
+    # tol = 0 sweeps until the off-diagonal is exactly zero or max_sweeps
+    # (numax's fixed 12) have run, and agrees with numax's 12-sweep answer.
     ns = np.array([24, 40], dtype=np.int32)
     mats = make_batch(ns, seed=6, wells=1)
     W, V, sweeps = run(ns, mats, sort=True, tol=0.0, max_sweeps=12)
-    assert list(sweeps) == [12, 12]
+    assert all(1 <= s <= 12 for s in sweeps)
+    W2, _, sweeps2 = run(ns, mats, sort=True, tol=0.0, max_sweeps=3)
+    assert list(sweeps2) == [3, 3]
     for (n, a), off in zip(zip(ns, mats), (0, 24)):
         jac, _ = oracle.jacobi_eigh(a, sweeps=12)
         scale = np.abs(jac).max()
