@@ -104,6 +104,27 @@ NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, cons
                                         float *L, const float *B, float *X, int32_t *info,
                                         void *stream);
 
+/* Allocation-free form of nmx_potrf_potrs_batched_f64, with no counterpart
+ * in the reference (numax allocates per call).  For callers that cannot
+ * allocate device memory -- a host runtime whose allocator already owns the
+ * GPU's memory, or code running inside another framework's memory pool --
+ * the batch's schedule (sizes, size-sorted order, offsets, work counter) is
+ * kept in a fixed device array built into the library instead of a plan's
+ * cudaMalloc'd buffer.  The call itself allocates nothing on the device or
+ * through any library.  Same layout and results as the plan path; n_host is
+ * on the host and is copied into that array on `stream`.
+ * Limit: count <= 65536 matrices (a larger count is rejected with -2).
+ * The array (about 1.5 MB) stays resident on every GPU that loads the
+ * library until exit.  The first call on a device performs that device's
+ * set-up (resolving the array's address), so make it before any stream
+ * capture.  All calls share the one array: calls that may overlap on the GPU
+ * (different streams, or several host threads) race and must be serialized
+ * by the caller. */
+NMX_API int nmx_potrf_potrs_batched_noalloc_f64(nmx_ctx ctx, int64_t count, const int32_t *n_host,
+                                                int nrhs, const double *A, double *L,
+                                                const double *B, double *X, int32_t *info,
+                                                void *stream);
+
 /* ---- batched uneven-size symmetric eigensolver (Jacobi) -----------------
  *
  * Replaces numax's Array-tier `eigh[T, n, sweeps=12]` run one matrix per GPU

@@ -24,6 +24,7 @@
 // the small ones fill the tail.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -518,3 +519,189 @@ int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, const float 
 }
 
 }  // extern "C"
+
+// ---- allocation-free entry point --------------------------------------------
+//
+// For callers that cannot allocate device memory (a host runtime whose
+// allocator owns all of HBM, code running inside another framework's memory
+// pool or a CUDA-graph-only region): the same kernel as the plan path, with
+// its schedule -- matrix sizes, size-sorted order, element offsets and the
+// work counter -- held in a fixed file-scope device array instead of a plan's
+// cudaMalloc'd buffer.  The array is sized for kNoAllocMaxCount matrices
+// (about 1.5 MB) and lives on every GPU that loads the library until exit.
+
+namespace nmx {
+
+constexpr int64_t kNoAllocMaxCount = 65536;
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxCount * (4 + 4 + 8 + 8) + 256;
+
+// Layout: int32 n[max] | int32 order[max] | int64 a_off[max] | int64 b_off[max] | int32 counter.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocViews {
+    int32_t *n, *order;
+    int64_t *a_off, *b_off;
+    int32_t *counter;
+};
+
+__host__ __device__ inline NoAllocViews noalloc_views(unsigned char *base) {
+    NoAllocViews v;
+    v.n = reinterpret_cast<int32_t *>(base);
+    v.order = v.n + kNoAllocMaxCount;
+    v.a_off = reinterpret_cast<int64_t *>(v.order + kNoAllocMaxCount);
+    v.b_off = v.a_off + kNoAllocMaxCount;
+    v.counter = reinterpret_cast<int32_t *>(v.b_off + kNoAllocMaxCount);
+    return v;
+}
+
+// One CTA: element offsets (exclusive prefix sums of n^2 and n*nrhs), the
+// order sorted by n descending (counting sort), and a zeroed work counter.
+constexpr int kSchedThreads = 1024;
+__global__ void __launch_bounds__(kSchedThreads) noalloc_schedule_kernel(unsigned char *scratch,
+                                                                         int count, int nrhs) {
+    NoAllocViews v = noalloc_views(scratch);
+    __shared__ int64_t part_a[kSchedThreads], part_b[kSchedThreads];
+    __shared__ int hist[kPotrfMaxN + 1], start[kPotrfMaxN + 1];
+    const int t = threadIdx.x;
+    const int per = (count + kSchedThreads - 1) / kSchedThreads;
+    const int lo = min(count, t * per), hi = min(count, lo + per);
+    int64_t sa = 0, sb = 0;
+    for (int i = lo; i < hi; ++i) {
+        int64_t n = v.n[i];
+        sa += n * n;
+        sb += n * nrhs;
+    }
+    part_a[t] = sa;
+    part_b[t] = sb;
+    for (int i = t; i <= kPotrfMaxN; i += kSchedThreads) hist[i] = 0;
+    __syncthreads();
+    if (t == 0) {
+        int64_t ra = 0, rb = 0;
+        for (int i = 0; i < kSchedThreads; ++i) {
+            int64_t a = part_a[i], b = part_b[i];
+            part_a[i] = ra;
+            part_b[i] = rb;
+            ra += a;
+            rb += b;
+        }
+    }
+    __syncthreads();
+    sa = part_a[t];
+    sb = part_b[t];
+    for (int i = lo; i < hi; ++i) {
+        int64_t n = v.n[i];
+        v.a_off[i] = sa;
+        v.b_off[i] = sb;
+        sa += n * n;
+        sb += n * nrhs;
+        atomicAdd(&hist[n], 1);
+    }
+    __syncthreads();
+    if (t == 0) {
+        int pos = 0;
+        for (int n = kPotrfMaxN; n >= 1; --n) {
+            start[n] = pos;
+            pos += hist[n];
+        }
+        *v.counter = 0;
+    }
+    __syncthreads();
+    for (int i = lo; i < hi; ++i) v.order[atomicAdd(&start[v.n[i]], 1)] = i;
+}
+
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
+    int sm_count = 0;
+    int per_sm[2] = {0, 0};  // potrf_potrs_batched_kernel<T, 256> at nmax=128, nrhs=8
+};
+static NoAllocDevice g_noalloc_dev[64];
+static std::mutex g_noalloc_mu;
+
+// Per-device set-up, run by the first call on each device with that device
+// current: resolve the array's device address (host code cannot use the
+// symbol itself) and configure the kernel.
+template <typename T>
+static int noalloc_setup(nmx_ctx ctx, NoAllocDevice **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (ctx->device < 0 || ctx->device >= 64) {
+        set_error("device ordinal %d out of range", ctx->device);
+        return NMX_ERR_UNSUPPORTED;
+    }
+    NoAllocDevice &d = g_noalloc_dev[ctx->device];
+    const int ti = sizeof(T) == 8 ? 0 : 1;
+    if (!d.ready) {
+        void *ptr = nullptr;
+        NMX_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        d.scratch = static_cast<unsigned char *>(ptr);
+        d.sm_count = ctx->sm_count;
+        d.ready = true;
+    }
+    if (d.per_sm[ti] == 0) {
+        auto kern = potrf_potrs_batched_kernel<T, 256>;
+        NMX_CUDA_TRY(set_max_dynamic_smem(kern, ctx));
+        size_t smem = sizeof(T) * (size_t)potrf_smem_elems(kPotrfMaxN, kPotrfMaxRhs);
+        int per_sm = 0;
+        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+        if (per_sm < 1) {
+            set_error("allocation-free kernel does not fit an SM");
+            return NMX_ERR_UNSUPPORTED;
+        }
+        d.per_sm[ti] = per_sm;
+    }
+    *out = &d;
+    return 0;
+}
+
+template <typename T>
+static int run_noalloc(nmx_ctx ctx, int64_t count, const int32_t *n_host, int nrhs, const T *A,
+                       T *L, const T *B, T *X, int32_t *info, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(count >= 0, 2, "count < 0");
+    if (count > kNoAllocMaxCount) {
+        set_error("argument 2: count %lld exceeds the allocation-free limit of %lld matrices "
+                  "(use the plan entry points for larger batches)",
+                  (long long)count, (long long)kNoAllocMaxCount);
+        return -2;
+    }
+    NMX_ARG_CHECK(n_host != nullptr || count == 0, 3, "n_host is NULL");
+    NMX_ARG_CHECK(nrhs >= 0 && nrhs <= kPotrfMaxRhs, 4, "nrhs must be in 0..8");
+    NMX_ARG_CHECK(A != nullptr || count == 0, 5, "A is NULL");
+    NMX_ARG_CHECK(L != nullptr || count == 0, 6, "L is NULL");
+    NMX_ARG_CHECK(B != nullptr || nrhs == 0 || count == 0, 7, "B is NULL");
+    NMX_ARG_CHECK(X != nullptr || nrhs == 0 || count == 0, 8, "X is NULL");
+    NMX_ARG_CHECK(info != nullptr || count == 0, 9, "info is NULL");
+    int nmax = 1;
+    for (int64_t i = 0; i < count; ++i) {
+        NMX_ARG_CHECK(n_host[i] >= 1 && n_host[i] <= kPotrfMaxN, 3, "every n_i must be in 1..128");
+        nmax = std::max(nmax, (int)n_host[i]);
+    }
+    if (count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    NoAllocDevice *d = nullptr;
+    int rc = noalloc_setup<T>(ctx, &d);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NoAllocViews v = noalloc_views(d->scratch);
+    NMX_CUDA_TRY(cudaMemcpyAsync(v.n, n_host, sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
+    noalloc_schedule_kernel<<<1, kSchedThreads, 0, st>>>(d->scratch, (int)count, nrhs);
+    NMX_CUDA_TRY(cudaGetLastError());
+    BatchedPotrfArgs args{v.order, v.n, v.a_off, v.b_off, A, L, B, X, info, nrhs};
+    const size_t smem = sizeof(T) * (size_t)potrf_smem_elems(nmax, nrhs);
+    const int grid = (int)std::min<int64_t>(count, (int64_t)d->per_sm[sizeof(T) == 8 ? 0 : 1] *
+                                                       d->sm_count);
+    potrf_potrs_batched_kernel<T, 256><<<grid, 256, smem, st>>>(args, 0, (int)count, nmax,
+                                                                v.counter);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace nmx
+
+extern "C" NMX_API int nmx_potrf_potrs_batched_noalloc_f64(nmx_ctx ctx, int64_t count,
+                                                           const int32_t *n_host, int nrhs,
+                                                           const double *A, double *L,
+                                                           const double *B, double *X,
+                                                           int32_t *info, void *stream) {
+    return nmx::run_noalloc<double>(ctx, count, n_host, nrhs, A, L, B, X, info, stream);
+}
