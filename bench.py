@@ -215,6 +215,91 @@ def run_reference(args):
     return 0
 
 
+def haar_torch(n, gen, dev):
+    """Haar-distributed orthogonal matrix: Q of a Gaussian's QR with the
+    sign fix (data generation only; torch/cuSOLVER)."""
+    import torch
+    g = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+    q, r = torch.linalg.qr(g)
+    q *= torch.sign(torch.diagonal(r))[None, :]
+    del g, r
+    return q
+
+
+def run_lu_ir(n, kappas, dev, seed=SEED):
+    """FP64 LU solve vs the BF16-factor IR solve at order n, A = U diag(s) V^T
+    (U, V Haar, s geometric 1..1/kappa), b = A x_true.  Both timed on the
+    device (CUDA events), inputs resident; returns a dict per kappa."""
+    import ctypes as C
+    import torch
+    from numax_b200 import _lib
+    ctx = _lib.context(dev.index)
+    stream = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 77)
+    u = haar_torch(n, gen, dev)
+    v = haar_torch(n, gen, dev)
+    xt = torch.randn(n, generator=gen, dtype=torch.float64, device=dev)
+    out = {}
+    for kappa in kappas:
+        s = torch.logspace(0.0, -np.log10(kappa), n, dtype=torch.float64, device=dev)
+        a = (u * s[None, :]) @ v.T
+        b = a @ xt
+        norm_a = float(a.abs().sum(1).max())
+
+        def berr(x):
+            r = b - a @ x
+            return float(r.abs().max() / (norm_a * x.abs().max() + b.abs().max()))
+
+        # FP64: nmx_getrf_f64 + nmx_getrs_f64 on a copy.
+        lu = torch.empty_like(a)
+        piv = torch.empty(n, dtype=torch.int32, device=dev)
+        info = torch.empty(1, dtype=torch.int32, device=dev)
+        x64 = torch.empty_like(b)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lu.copy_(a)
+        x64.copy_(b)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(),
+                  stream.cuda_stream)
+        _lib.call("nmx_getrs_f64", ctx, n, 1, lu.data_ptr(), n, piv.data_ptr(), x64.data_ptr(), 1,
+                  stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        t64 = e0.elapsed_time(e1)
+        be64 = berr(x64)
+        del lu
+        # BF16 factors + FP64 refinement (GMRES-IR when plain IR stalls).
+        res = {"fp64_lu_solve_ms": t64, "fp64_backward_error": be64}
+        for prec, mode in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO),):
+            x = torch.empty_like(b)
+            st = _lib.IrStats()
+            e0.record(stream)
+            rc = _lib.load().nmx_gesv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
+                                             C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                             mode, 1e-14, 100, C.byref(st),
+                                             C.c_void_p(stream.cuda_stream))
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if rc != 0:
+                res[f"{prec}_ir_error"] = _lib.last_error()
+                continue
+            tir = e0.elapsed_time(e1)
+            fe = float((x - x64).abs().max() / x64.abs().max())
+            res.update({f"{prec}_ir_solve_ms": tir, f"{prec}_ir_backward_error": berr(x),
+                        f"{prec}_ir_iterations": st.iterations,
+                        f"{prec}_gmres_iterations": st.gmres_iterations,
+                        f"{prec}_used_gmres": bool(st.used_gmres),
+                        f"{prec}_factor_ms": st.factor_ms, f"{prec}_refine_ms": st.refine_ms,
+                        f"{prec}_forward_diff_vs_fp64": fe,
+                        f"speedup_fp64_over_{prec}_ir": t64 / tir})
+        out[f"{kappa:.0e}"] = res
+        del a, b, s
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -326,6 +411,15 @@ def run_ours(args):
     achieved = abytes / launch_s / 1e9
     traffic = read_traffic()
 
+    lu_ir = None
+    if world == 1 and args.lu_n > 0:
+        try:
+            kappas = [float(k) for k in args.lu_kappas.split(",") if k]
+            lu_ir = {"n": args.lu_n, "timing": "device events, inputs resident, one solve each",
+                     "results": run_lu_ir(args.lu_n, kappas, dev)}
+        except Exception as exc:  # report, keep the batched line
+            lu_ir = {"n": args.lu_n, "error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         from oracle import build as obuild
@@ -352,6 +446,7 @@ def run_ours(args):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "lu_ir": lu_ir,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -366,9 +461,22 @@ def main():
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lu-n", type=int, default=32768,
+                    help="order of the FP64-LU vs BF16-IR comparison (0 skips it)")
+    ap.add_argument("--lu-kappas", default="1e2",
+                    help="comma-separated condition numbers for the comparison")
+    ap.add_argument("--only-lu", action="store_true", help="run only the LU/IR comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_lu:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        kappas = [float(k) for k in args.lu_kappas.split(",") if k]
+        print(json.dumps({"lu_ir": {"n": args.lu_n, "results": run_lu_ir(args.lu_n, kappas, dev)}}),
+              flush=True)
+        return 0
     return run_ours(args)
 
 

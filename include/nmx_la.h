@@ -204,6 +204,72 @@ NMX_API int nmx_potrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *L,
 NMX_API int nmx_potrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *L, int64_t lda,
                           float *B, int64_t ldb, void *stream);
 
+/* ---- Householder QR (m >= n) and the thin Q --------------------------------
+ *
+ * nmx_geqrf_*: factor the m x n row-major A (lda) in place into LAPACK's
+ * packed form -- R on and above the diagonal of the first n rows, each
+ * reflector's v below the diagonal with an implicit unit leading entry, its
+ * scale in tau[j] -- numax's qr_factor (numax/linalg/qr.mojo:615-743) with
+ * geqr2_panel's convention (numax/linalg/panel.mojo:1975-2073):
+ * beta = -sign(alpha)*||x|| (+||x|| when alpha <= 0), tau = (beta-alpha)/beta,
+ * v = x/(alpha-beta), tau = 0 for an exactly zero sub-column.  Panels are 16
+ * columns, numax's default block.
+ *
+ * nmx_orgqr_*: the thin Q (m x n, row-major ldq) from geqrf's output F and
+ * tau, the reflectors replayed last panel first on the identity -- numax's
+ * QR.q() (numax/linalg/qr.mojo:405-468).
+ */
+NMX_API int nmx_geqrf_f32(nmx_ctx ctx, int64_t m, int64_t n, float *A, int64_t lda, float *tau,
+                          void *stream);
+NMX_API int nmx_geqrf_f64(nmx_ctx ctx, int64_t m, int64_t n, double *A, int64_t lda, double *tau,
+                          void *stream);
+NMX_API int nmx_orgqr_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int64_t ldf,
+                          const float *tau, float *Q, int64_t ldq, void *stream);
+NMX_API int nmx_orgqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
+                          const double *tau, double *Q, int64_t ldq, void *stream);
+
+/* ---- mixed-precision LU solve with iterative refinement -------------------
+ *
+ * No numax counterpart (numax's GPU path is FP32-only, without refinement);
+ * the north star's large solve.  x := A^-1 b for the FP64 n x n row-major A
+ * (lda) and FP64 vectors b, x (device):
+ *   - A is scaled by powers of two (rows, then columns; exact) when the
+ *     factors are FP16, rounded to FP32 and factored by the recursive LU of
+ *     nmx_getrf_f32 with its trailing updates in BF16/FP16 on the tcgen05
+ *     tensor cores (FP32 accumulate), or FP32 CUDA cores (NMX_IR_FP32);
+ *   - refinement in FP64: r = b - A x over the original A, correction from
+ *     the low-precision factors; with NMX_IR_GMRES the correction is solved by
+ *     restarted GMRES preconditioned by those factors (GMRES-IR); with
+ *     NMX_IR_AUTO plain refinement hands over to GMRES-IR when it stops
+ *     contracting.
+ * Stops when ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol or
+ * after max_iter refinement steps.  Synchronizes `stream` (the refinement
+ * loop decides on the host).  stats (host pointer, may be NULL) receives the
+ * iteration counts, the final normwise backward error and the device time of
+ * the factorization and of the refinement.
+ */
+#define NMX_IR_BF16 1
+#define NMX_IR_FP16 2
+#define NMX_IR_FP32 3
+#define NMX_IR_GMRES 0x10
+#define NMX_IR_AUTO 0x20
+
+typedef struct {
+    int32_t iterations;       /* refinement steps taken */
+    int32_t gmres_iterations; /* total inner GMRES iterations */
+    int32_t converged;        /* 1 if the backward error reached tol */
+    int32_t info;             /* info of the low-precision LU (first zero pivot) */
+    int32_t used_gmres;       /* 1 if GMRES-IR ran */
+    int32_t reserved;
+    double backward_error;    /* final normwise backward error */
+    double factor_ms;         /* device time: scaling + low-precision LU */
+    double refine_ms;         /* device time: the refinement loop */
+} nmx_ir_stats;
+
+NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, const double *b,
+                            double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
+                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

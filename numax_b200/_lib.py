@@ -52,7 +52,26 @@ SIGNATURES = {
     "nmx_potrf_f32": (ci, [vp, i64, vp, i64, vp, vp]),
     "nmx_potrs_f64": (ci, [vp, i64, i64, vp, i64, vp, i64, vp]),
     "nmx_potrs_f32": (ci, [vp, i64, i64, vp, i64, vp, i64, vp]),
+    "nmx_geqrf_f32": (ci, [vp, i64, i64, vp, i64, vp, vp]),
+    "nmx_geqrf_f64": (ci, [vp, i64, i64, vp, i64, vp, vp]),
+    "nmx_orgqr_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
+    "nmx_orgqr_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
+    "nmx_gesv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
 }
+
+NMX_IR_BF16 = 1
+NMX_IR_FP16 = 2
+NMX_IR_FP32 = 3
+NMX_IR_GMRES = 0x10
+NMX_IR_AUTO = 0x20
+
+
+class IrStats(C.Structure):
+    """nmx_ir_stats (include/nmx_la.h)."""
+    _fields_ = [("iterations", C.c_int32), ("gmres_iterations", C.c_int32),
+                ("converged", C.c_int32), ("info", C.c_int32), ("used_gmres", C.c_int32),
+                ("reserved", C.c_int32), ("backward_error", C.c_double),
+                ("factor_ms", C.c_double), ("refine_ms", C.c_double)]
 
 
 class NmxError(RuntimeError):

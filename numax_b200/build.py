@@ -29,6 +29,19 @@ NVCC_FLAGS = ARCH + [
 ]
 
 
+def cutlass_include() -> str:
+    """CUTLASS/CuTe headers (vendored by the flashinfer wheel in this image)."""
+    import importlib.util
+    spec = importlib.util.find_spec("flashinfer")
+    cands = []
+    if spec and spec.submodule_search_locations:
+        cands.append(os.path.join(spec.submodule_search_locations[0], "data", "cutlass", "include"))
+    for c in cands:
+        if os.path.exists(os.path.join(c, "cutlass", "cutlass.h")):
+            return c
+    raise RuntimeError("CUTLASS headers not found (flashinfer/data/cutlass/include)")
+
+
 def nvcc() -> str:
     path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(path):
@@ -46,7 +59,8 @@ def _compile(src: str, extra: list[str]) -> str:
     deps = [src] + _headers()
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj
-    cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
+    inc = ["-I", cutlass_include()] if os.path.basename(src) == "gemm_tc.cu" else []
+    cmd = [nvcc()] + NVCC_FLAGS + inc + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

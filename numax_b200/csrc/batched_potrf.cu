@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <numeric>
 #include <vector>
 
@@ -129,6 +130,182 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
     __syncwarp();
 }
 
+// ---- panel solve and trailing update, CUDA-core form (float32) ----------
+
+template <typename T, int NT>
+__device__ __forceinline__ void panel_simt(T *S, int n, int R, int k, int kb) {
+    const int tid = threadIdx.x;
+    const int r0 = k + kb;
+    int wro[kDiagNB];
+#pragma unroll
+    for (int j = 0; j < kDiagNB; ++j) wro[j] = prow_off(k + min(j, kb - 1), n) + k;
+    for (int r = r0 + tid; r < R; r += NT) {
+        const int ro = prow_off(r, n) + k;
+        T a[kDiagNB];
+#pragma unroll
+        for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[ro + j] : T(0);
+#pragma unroll
+        for (int j = 0; j < kDiagNB; ++j) {
+            if (j < kb) {
+                T out = T(0);
+#pragma unroll
+                for (int i = 0; i <= j; ++i) out += a[i] * S[wro[j] + i];
+                S[ro + j] = out;
+            }
+        }
+    }
+}
+
+// Flat index of a tile of the augmented trapezoid -> (tile row, tile col):
+// the first TN tile rows are triangular, the rest are full TN-wide.
+__device__ __forceinline__ void trap_tile(int e, int TN, int &ti, int &tj) {
+    const int tri = TN * (TN + 1) / 2;
+    if (e < tri) {
+        ti = (int)((sqrtf(8.f * e + 1.f) - 1.f) * 0.5f);
+        while (ti * (ti + 1) / 2 > e) --ti;
+        while ((ti + 1) * (ti + 2) / 2 <= e) ++ti;
+        tj = e - ti * (ti + 1) / 2;
+    } else {
+        const int e2 = e - tri;
+        ti = TN + e2 / TN;
+        tj = e2 - (ti - TN) * TN;
+    }
+}
+
+// S[i][j] -= sum_p S[i][k+p] S[j][k+p] over rows [r0, R), cols [r0, min(i+1, n)),
+// 4x4 register tiles.
+template <typename T, int NT>
+__device__ __forceinline__ void trailing_simt(T *S, int n, int R, int k, int kb) {
+    const int tid = threadIdx.x;
+    const int r0 = k + kb;
+    const int TR = (int)ceil_div(R - r0, 4), TN = (int)ceil_div(n - r0, 4);
+    if (TN <= 0) return;
+    const int tiles = TN * (TN + 1) / 2 + (TR - TN) * TN;
+    for (int e = tid; e < tiles; e += NT) {
+        int ti, tj;
+        trap_tile(e, TN, ti, tj);
+        const int i0 = r0 + 4 * ti, j0 = r0 + 4 * tj;
+        T acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+        int ir[4], jr[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            ir[a] = prow_off(min(i0 + a, R - 1), n) + k;
+            jr[a] = prow_off(min(j0 + a, n - 1), n) + k;
+        }
+        for (int p = 0; p < kb; ++p) {
+            T x[4], y[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                x[a] = S[ir[a] + p];
+                y[a] = S[jr[a] + p];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int i = i0 + a, j = j0 + b;
+                if (i < R && j < n && j <= i) S[ir[a] - k + j] -= acc[a][b];
+            }
+    }
+}
+
+// ---- panel solve and trailing update on the FP64 tensor cores ------------
+// mma.sync m8n8k4 f64 (DMMA): lane l holds A[l/4][l%4], B[k=l%4][n=l/4] and
+// C[l/4][2*(l%4) + {0,1}].  Rows of a fragment come from packed rows of S.
+
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Panel rows in 8-row blocks, one warp per block: rows x 16 times W^T (16 x 16).
+template <int NT>
+__device__ __forceinline__ void panel_dmma(double *S, int n, int R, int k, int kb) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    const int r0 = k + kb;
+    const int g = lane >> 2, t = lane & 3;
+    // B fragments: W^T, B[i][j] = W[j][i] (zero above W's diagonal / past kb).
+    double bw[2][4];
+#pragma unroll
+    for (int jb = 0; jb < 2; ++jb)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int j = jb * 8 + g, i = kk * 4 + t;
+            bw[jb][kk] = (j < kb && i <= j) ? S[prow_off(k + j, n) + k + i] : 0.0;
+        }
+    const int blocks = (R - r0 + 7) >> 3;
+    for (int b = warp; b < blocks; b += NW) {
+        const int row = r0 + 8 * b + g;
+        const int ro = prow_off(min(row, R - 1), n) + k;
+        double a[4];
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int i = kk * 4 + t;
+            a[kk] = i < kb ? S[ro + i] : 0.0;
+        }
+        double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int jb = 0; jb < 2; ++jb)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) dmma_8x8x4(c[jb][0], c[jb][1], a[kk], bw[jb][kk]);
+        __syncwarp();
+        if (row < R) {
+#pragma unroll
+            for (int jb = 0; jb < 2; ++jb)
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const int j = jb * 8 + 2 * t + v;
+                    if (j < kb) S[ro + j] = c[jb][v];
+                }
+        }
+    }
+}
+
+// Trailing update in 8x8 blocks of the augmented trapezoid, one warp each.
+template <int NT>
+__device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, int kb) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    const int r0 = k + kb;
+    const int g = lane >> 2, t = lane & 3;
+    const int TR = (R - r0 + 7) >> 3, TN = (n - r0 + 7) >> 3;
+    if (TN <= 0) return;
+    const int tiles = TN * (TN + 1) / 2 + (TR - TN) * TN;
+    for (int e = warp; e < tiles; e += NW) {
+        int ti, tj;
+        trap_tile(e, TN, ti, tj);
+        const int i0 = r0 + 8 * ti, j0 = r0 + 8 * tj;
+        const int arow = prow_off(min(i0 + g, R - 1), n) + k;
+        const int brow = prow_off(min(j0 + g, n - 1), n) + k;
+        double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int p = kk * 4 + t;
+            const double a = p < kb ? S[arow + p] : 0.0;
+            const double b = p < kb ? S[brow + p] : 0.0;
+            dmma_8x8x4(c0, c1, a, b);
+        }
+        const int i = i0 + g;
+        if (i < R) {
+            const int ro = prow_off(i, n);
+            const int j = j0 + 2 * t;
+            if (j < n && j <= i) S[ro + j] -= c0;
+            if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c1;
+        }
+    }
+}
+
 template <typename T, int NT>
 __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *xb, int *s_info) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -160,78 +337,17 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
         __syncthreads();
 
         // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T, W
-        // (the block's inverse) sitting where the block of L was.
+        // (the block's inverse) sitting where the block of L was; then the
+        // trailing update of the augmented trapezoid.
         const int r0 = k + kb;
-        int wro[kDiagNB];
-#pragma unroll
-        for (int j = 0; j < kDiagNB; ++j) wro[j] = prow_off(k + min(j, kb - 1), n) + k;
-        for (int r = r0 + tid; r < R; r += NT) {
-            const int ro = prow_off(r, n) + k;
-            T a[kDiagNB];
-#pragma unroll
-            for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[ro + j] : T(0);
-#pragma unroll
-            for (int j = 0; j < kDiagNB; ++j) {
-                if (j < kb) {
-                    T out = T(0);
-#pragma unroll
-                    for (int i = 0; i <= j; ++i) out += a[i] * S[wro[j] + i];
-                    S[ro + j] = out;
-                }
-            }
-        }
-        __syncthreads();
-
-        // Trailing update of the augmented trapezoid: rows [r0, R), cols
-        // [r0, min(i+1, n)), S[i][j] -= sum_p S[i][k+p] S[j][k+p], 4x4 tiles.
-        const int TR = (int)ceil_div(R - r0, 4), TN = (int)ceil_div(n - r0, 4);
-        if (TN > 0) {
-            const int tri = TN * (TN + 1) / 2;
-            const int tiles = tri + (TR - TN) * TN;
-            for (int e = tid; e < tiles; e += NT) {
-                int ti, tj;
-                if (e < tri) {
-                    ti = (int)((sqrtf(8.f * e + 1.f) - 1.f) * 0.5f);
-                    while (ti * (ti + 1) / 2 > e) --ti;
-                    while ((ti + 1) * (ti + 2) / 2 <= e) ++ti;
-                    tj = e - ti * (ti + 1) / 2;
-                } else {
-                    int e2 = e - tri;
-                    ti = TN + e2 / TN;
-                    tj = e2 - (ti - TN) * TN;
-                }
-                const int i0 = r0 + 4 * ti, j0 = r0 + 4 * tj;
-                T acc[4][4];
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-                int ir[4], jr[4];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    ir[a] = prow_off(min(i0 + a, R - 1), n) + k;
-                    jr[a] = prow_off(min(j0 + a, n - 1), n) + k;
-                }
-                for (int p = 0; p < kb; ++p) {
-                    T x[4], y[4];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        x[a] = S[ir[a] + p];
-                        y[a] = S[jr[a] + p];
-                    }
-#pragma unroll
-                    for (int a = 0; a < 4; ++a)
-#pragma unroll
-                        for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
-                }
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int i = i0 + a, j = j0 + b;
-                        if (i < R && j < n && j <= i) S[ir[a] - k + j] -= acc[a][b];
-                    }
-            }
+        if constexpr (std::is_same<T, double>::value) {
+            panel_dmma<NT>(S, n, R, k, kb);
+            __syncthreads();
+            trailing_dmma<NT>(S, n, R, k, kb);
+        } else {
+            panel_simt<T, NT>(S, n, R, k, kb);
+            __syncthreads();
+            trailing_simt<T, NT>(S, n, R, k, kb);
         }
         __syncthreads();
     }

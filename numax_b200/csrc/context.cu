@@ -57,6 +57,28 @@ int nmx_context::ensure_workspace(size_t bytes) {
     return 0;
 }
 
+int nmx_context::ensure_slot(int slot, size_t bytes, void **out) {
+    if (slot < 0 || slot >= kSlots) {
+        nmx::set_error("bad workspace slot %d", slot);
+        return NMX_ERR_INTERNAL;
+    }
+    if (bytes > slot_bytes[slot]) {
+        if (slot_ptr[slot]) cudaFree(slot_ptr[slot]);
+        slot_ptr[slot] = nullptr;
+        slot_bytes[slot] = 0;
+        size_t rounded = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
+        cudaError_t e = cudaMalloc(&slot_ptr[slot], rounded);
+        if (e != cudaSuccess) {
+            nmx::set_error("workspace slot %d cudaMalloc(%zu): %s", slot, rounded,
+                           cudaGetErrorString(e));
+            return NMX_ERR_ALLOC;
+        }
+        slot_bytes[slot] = rounded;
+    }
+    *out = slot_ptr[slot];
+    return 0;
+}
+
 extern "C" {
 
 const char *nmx_last_error_string(void) { return nmx::g_last_error; }
@@ -94,6 +116,8 @@ int nmx_destroy(nmx_ctx ctx) {
     {
         nmx::DeviceGuard g(ctx->device);
         if (ctx->workspace) cudaFree(ctx->workspace);
+        for (int i = 0; i < nmx_context::kSlots; ++i)
+            if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
         if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
     }
     delete ctx;

@@ -83,6 +83,23 @@ inline cublasStatus_t gemm_sub_bt(cublasHandle_t h, int64_t m, int64_t n, int64_
                        (int)lda, &one, C, (int)ldc);
 }
 
+// General row-major GEMM: C[m x n] = alpha op(A)[m x k] op(B)[k x n] + beta C,
+// op(X) = X or X^T (X stored row-major with its leading dimension).
+inline cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                              double alpha, const double *A, int64_t lda, const double *B,
+                              int64_t ldb, double beta, double *C, int64_t ldc) {
+    if (m <= 0 || n <= 0) return CUBLAS_STATUS_SUCCESS;
+    return cublasDgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n,
+                       (int)m, (int)k, &alpha, B, (int)ldb, A, (int)lda, &beta, C, (int)ldc);
+}
+inline cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                              float alpha, const float *A, int64_t lda, const float *B, int64_t ldb,
+                              float beta, float *C, int64_t ldc) {
+    if (m <= 0 || n <= 0) return CUBLAS_STATUS_SUCCESS;
+    return cublasSgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n,
+                       (int)m, (int)k, &alpha, B, (int)ldb, A, (int)lda, &beta, C, (int)ldc);
+}
+
 #define NMX_CUBLAS_TRY(expr)                                                                 \
     do {                                                                                     \
         cublasStatus_t _s = (expr);                                                          \
@@ -96,16 +113,60 @@ inline cublasStatus_t gemm_sub_bt(cublasHandle_t h, int64_t m, int64_t n, int64_
 // The context's cuBLAS handle bound to `st` (created on first use).
 int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
 
+// Tensor-core update (gemm_tc.cu): C -= round16(A) round16(B), fp32 operands.
+int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
+                    int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
+                    size_t ws_bytes);
+size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K);
+
+// The trailing-update product of the recursive factorizations and solves:
+// C[m x n] -= A[m x k] B[k x n], row-major.  precision 0 keeps the operands'
+// own precision (cuBLAS FP64/FP32 GEMM); NMX_PREC_BF16 / NMX_PREC_FP16 (fp32
+// data only) round the operands to 16 bits and run the tcgen05 kernel.
+struct GemmSub {
+    cublasHandle_t h = nullptr;
+    cudaStream_t st = nullptr;
+    int precision = 0;
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+    int operator()(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
+                   int64_t ldb, double *C, int64_t ldc) const {
+        cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
+        if (s != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasDgemm failed (%d)", (int)s);
+            return NMX_ERR_CUDA;
+        }
+        return 0;
+    }
+    int operator()(int64_t m, int64_t n, int64_t k, const float *A, int64_t lda, const float *B,
+                   int64_t ldb, float *C, int64_t ldc) const {
+        if (precision)
+            return tc_gemm_sub_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes);
+        cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
+        if (s != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasSgemm failed (%d)", (int)s);
+            return NMX_ERR_CUDA;
+        }
+        return 0;
+    }
+};
+
 // Blocked triangular solves, row-major (dense_lu.cu):
 //   trsm_lower<T, UNIT>:  X := L^-1 X, L the w x w lower block at (r, r) of A
 //   trsm_upper<T, TRANS>: X := U^-1 X, U the upper block at (r, r) of A, or
 //                         with TRANS X := L^-T X reading the lower block
 // X = rows [r, r+w) x cols [c0, c1) of B.
 template <typename T, bool UNIT>
-int trsm_lower(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda, int r,
-               int w, T *B, int64_t ldb, int c0, int c1);
+int trsm_lower(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
+               int c1);
 template <typename T, bool TRANS>
-int trsm_upper(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda, int r,
-               int w, T *B, int64_t ldb, int c0, int c1);
+int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
+               int c1);
+
+// Recursive LU with partial pivoting of the n x n row-major A (dense_lu.cu),
+// trailing updates through `gs`.  ipiv/info as nmx_getrf_*.
+template <typename T>
+int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
+              int32_t *info);
 
 }  // namespace nmx

@@ -278,7 +278,7 @@ template <typename T>
 struct LuRun {
     nmx_ctx ctx;
     cudaStream_t st;
-    cublasHandle_t h;
+    GemmSub gs;
     T *A;
     int64_t lda;
     int n;
@@ -314,8 +314,9 @@ static int leaf(LuRun<T> &R, int c, int w) {
 
 // X := L^-1 X, L the w x w lower block at (r, r) of A, X rows [r, r+w) cols [c0, c1) of B.
 template <typename T, bool UNIT>
-int trsm_lower(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda,
-                      int r, int w, T *B, int64_t ldb, int c0, int c1) {
+int trsm_lower(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
+               int c1) {
+    cudaStream_t st = gs.st;
     if (w <= 0 || c1 <= c0) return 0;
     if (w <= kTrsmLeaf) {
         int threads = 128;
@@ -325,17 +326,20 @@ int trsm_lower(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64
         return 0;
     }
     int hw = (w / 2 + kTrsmLeaf - 1) / kTrsmLeaf * kTrsmLeaf;
-    int rc = trsm_lower<T, UNIT>(ctx, h, st, A, lda, r, hw, B, ldb, c0, c1);
+    int rc = trsm_lower<T, UNIT>(gs, A, lda, r, hw, B, ldb, c0, c1);
     if (rc) return rc;
-    NMX_CUBLAS_TRY(gemm_sub(h, w - hw, c1 - c0, hw, A + (int64_t)(r + hw) * lda + r, lda,
-                            B + (int64_t)r * ldb + c0, ldb, B + (int64_t)(r + hw) * ldb + c0, ldb));
-    return trsm_lower<T, UNIT>(ctx, h, st, A, lda, r + hw, w - hw, B, ldb, c0, c1);
+    rc = gs(w - hw, c1 - c0, hw, A + (int64_t)(r + hw) * lda + r, lda, B + (int64_t)r * ldb + c0, ldb,
+            B + (int64_t)(r + hw) * ldb + c0, ldb);
+    if (rc) return rc;
+    return trsm_lower<T, UNIT>(gs, A, lda, r + hw, w - hw, B, ldb, c0, c1);
 }
 
 // X := U^-1 X (TRANS: X := L^-T X with L the lower block stored at (r, r)).
 template <typename T, bool TRANS>
-int trsm_upper(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64_t lda,
-                      int r, int w, T *B, int64_t ldb, int c0, int c1) {
+int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
+               int c1) {
+    cudaStream_t st = gs.st;
+    cublasHandle_t h = gs.h;
     if (w <= 0 || c1 <= c0) return 0;
     if (w <= kTrsmLeaf) {
         int threads = 128;
@@ -345,7 +349,7 @@ int trsm_upper(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64
         return 0;
     }
     int hw = (w / 2 + kTrsmLeaf - 1) / kTrsmLeaf * kTrsmLeaf;
-    int rc = trsm_upper<T, TRANS>(ctx, h, st, A, lda, r + hw, w - hw, B, ldb, c0, c1);
+    int rc = trsm_upper<T, TRANS>(gs, A, lda, r + hw, w - hw, B, ldb, c0, c1);
     if (rc) return rc;
     // B_top -= U_top,bot X_bot   (TRANS: U_top,bot = (L_bot,top)^T)
     if (TRANS) {
@@ -364,10 +368,11 @@ int trsm_upper(nmx_ctx ctx, cublasHandle_t h, cudaStream_t st, const T *A, int64
                             (const float *)&one, (float *)(B + (int64_t)r * ldb + c0), (int)ldb);
         NMX_CUBLAS_TRY(s);
     } else {
-        NMX_CUBLAS_TRY(gemm_sub(h, hw, c1 - c0, w - hw, A + (int64_t)r * lda + r + hw, lda,
-                                B + (int64_t)(r + hw) * ldb + c0, ldb, B + (int64_t)r * ldb + c0, ldb));
+        rc = gs(hw, c1 - c0, w - hw, A + (int64_t)r * lda + r + hw, lda,
+                B + (int64_t)(r + hw) * ldb + c0, ldb, B + (int64_t)r * ldb + c0, ldb);
+        if (rc) return rc;
     }
-    return trsm_upper<T, TRANS>(ctx, h, st, A, lda, r, hw, B, ldb, c0, c1);
+    return trsm_upper<T, TRANS>(gs, A, lda, r, hw, B, ldb, c0, c1);
 }
 
 template <typename T>
@@ -377,37 +382,29 @@ static int getrf2(LuRun<T> &R, int c, int w) {
     int rc = getrf2<T>(R, c, hw);
     if (rc) return rc;
     // U12 := L11^-1 A12 over the right half's columns.
-    rc = trsm_lower<T, true>(R.ctx, R.h, R.st, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+    rc = trsm_lower<T, true>(R.gs, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
     if (rc) return rc;
     // A22 -= L21 U12.
-    NMX_CUBLAS_TRY(gemm_sub(R.h, R.n - c - hw, w - hw, hw, R.A + (int64_t)(c + hw) * R.lda + c,
-                            R.lda, R.A + (int64_t)c * R.lda + c + hw, R.lda,
-                            R.A + (int64_t)(c + hw) * R.lda + c + hw, R.lda));
+    rc = R.gs(R.n - c - hw, w - hw, hw, R.A + (int64_t)(c + hw) * R.lda + c, R.lda,
+              R.A + (int64_t)c * R.lda + c + hw, R.lda, R.A + (int64_t)(c + hw) * R.lda + c + hw,
+              R.lda);
+    if (rc) return rc;
     return getrf2<T>(R, c + hw, w - hw);
 }
 
 template <typename T>
-static int getrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *ipiv, int32_t *info,
-                 void *stream) {
-    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
-    NMX_ARG_CHECK(n >= 0 && n <= (1 << 20), 2, "n out of range");
-    NMX_ARG_CHECK(A != nullptr || n == 0, 3, "A is NULL");
-    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 4, "lda < max(1, n)");
-    NMX_ARG_CHECK(ipiv != nullptr || n == 0, 5, "ipiv is NULL");
-    NMX_ARG_CHECK(info != nullptr, 6, "info is NULL");
-    DeviceGuard g(ctx->device);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
+              int32_t *info) {
+    cudaStream_t st = gs.st;
     NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     if (n == 0) return 0;
-    cublasHandle_t h;
-    int rc = ctx_cublas(ctx, st, &h);
-    if (rc) return rc;
     const int G = ctx->sm_count;
     size_t bytes = sizeof(T) * (2 * (size_t)G * kLeafW + 2 * kLeafW + 2 * G) + sizeof(int) * 2 * G +
                    64;
-    rc = ctx->ensure_workspace(bytes);
+    void *wsv = nullptr;
+    int rc = ctx->ensure_slot(kWsLeaf, bytes, &wsv);
     if (rc) return rc;
-    char *ws = static_cast<char *>(ctx->workspace);
+    char *ws = static_cast<char *>(wsv);
     LeafScratch<T> sc;
     sc.cand_rows = reinterpret_cast<T *>(ws);
     sc.col_rows = sc.cand_rows + 2 * (size_t)G * kLeafW;
@@ -430,10 +427,30 @@ static int getrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *ipiv, int32
         set_error("matrix order %lld too large for the leaf panel", (long long)n);
         return NMX_ERR_UNSUPPORTED;
     }
-    LuRun<T> R{ctx, st, h, A, lda, (int)n, ipiv, info, sc, G};
-    rc = getrf2<T>(R, 0, (int)n);
+    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, G};
+    return getrf2<T>(R, 0, (int)n);
+}
+
+template int getrf_run<double>(nmx_ctx, const GemmSub &, int64_t, double *, int64_t, int32_t *,
+                               int32_t *);
+template int getrf_run<float>(nmx_ctx, const GemmSub &, int64_t, float *, int64_t, int32_t *,
+                              int32_t *);
+
+template <typename T>
+static int getrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *ipiv, int32_t *info,
+                 void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 0 && n <= (1 << 20), 2, "n out of range");
+    NMX_ARG_CHECK(A != nullptr || n == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, n), 4, "lda < max(1, n)");
+    NMX_ARG_CHECK(ipiv != nullptr || n == 0, 5, "ipiv is NULL");
+    NMX_ARG_CHECK(info != nullptr, 6, "info is NULL");
+    DeviceGuard g(ctx->device);
+    GemmSub gs;
+    gs.st = static_cast<cudaStream_t>(stream);
+    int rc = ctx_cublas(ctx, gs.st, &gs.h);
     if (rc) return rc;
-    return 0;
+    return getrf_run<T>(ctx, gs, n, A, lda, ipiv, info);
 }
 
 template <typename T>
@@ -450,35 +467,36 @@ static int getrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *LU, int64_t lda,
     if (n == 0 || nrhs == 0) return 0;
     DeviceGuard g(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cublasHandle_t h;
-    int rc = ctx_cublas(ctx, st, &h);
+    GemmSub gs;
+    gs.st = st;
+    int rc = ctx_cublas(ctx, st, &gs.h);
     if (rc) return rc;
     int threads = 128;
     laswp_kernel<T><<<(unsigned)ceil_div(nrhs, threads), threads, 0, st>>>(B, ldb, (int)nrhs, 0,
                                                                            (int)n, ipiv, 0, 0);
     NMX_CUDA_TRY(cudaGetLastError());
-    rc = trsm_lower<T, true>(ctx, h, st, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    rc = trsm_lower<T, true>(gs, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
     if (rc) return rc;
-    return trsm_upper<T, false>(ctx, h, st, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    return trsm_upper<T, false>(gs, LU, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
 }
 
 // Explicit instantiations used by the Cholesky and IR drivers.
-template int trsm_lower<double, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
-                                      int64_t, int, int, double *, int64_t, int, int);
-template int trsm_lower<float, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
-                                     int, int, float *, int64_t, int, int);
-template int trsm_upper<double, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
-                                       int64_t, int, int, double *, int64_t, int, int);
-template int trsm_upper<float, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
-                                      int, int, float *, int64_t, int, int);
-template int trsm_lower<double, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
-                                       int64_t, int, int, double *, int64_t, int, int);
-template int trsm_lower<float, false>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
-                                      int, int, float *, int64_t, int, int);
-template int trsm_upper<double, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const double *,
-                                      int64_t, int, int, double *, int64_t, int, int);
-template int trsm_upper<float, true>(nmx_ctx, cublasHandle_t, cudaStream_t, const float *, int64_t,
-                                     int, int, float *, int64_t, int, int);
+template int trsm_lower<double, true>(const GemmSub &, const double *, int64_t, int, int, double *,
+                                    int64_t, int, int);
+template int trsm_lower<float, true>(const GemmSub &, const float *, int64_t, int, int, float *,
+                                    int64_t, int, int);
+template int trsm_lower<double, false>(const GemmSub &, const double *, int64_t, int, int, double *,
+                                    int64_t, int, int);
+template int trsm_lower<float, false>(const GemmSub &, const float *, int64_t, int, int, float *,
+                                    int64_t, int, int);
+template int trsm_upper<double, true>(const GemmSub &, const double *, int64_t, int, int, double *,
+                                    int64_t, int, int);
+template int trsm_upper<float, true>(const GemmSub &, const float *, int64_t, int, int, float *,
+                                    int64_t, int, int);
+template int trsm_upper<double, false>(const GemmSub &, const double *, int64_t, int, int, double *,
+                                    int64_t, int, int);
+template int trsm_upper<float, false>(const GemmSub &, const float *, int64_t, int, int, float *,
+                                    int64_t, int, int);
 
 }  // namespace nmx
 

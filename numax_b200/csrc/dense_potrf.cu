@@ -186,12 +186,13 @@ static int potrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *L, int64_t lda, 
     if (n == 0 || nrhs == 0) return 0;
     DeviceGuard g(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cublasHandle_t h;
-    int rc = ctx_cublas(ctx, st, &h);
+    GemmSub gs;
+    gs.st = st;
+    int rc = ctx_cublas(ctx, st, &gs.h);
     if (rc) return rc;
-    rc = trsm_lower<T, false>(ctx, h, st, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    rc = trsm_lower<T, false>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
     if (rc) return rc;
-    return trsm_upper<T, true>(ctx, h, st, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    return trsm_upper<T, true>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
 }
 
 }  // namespace nmx

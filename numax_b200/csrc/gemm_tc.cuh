@@ -1,0 +1,22 @@
+// Tensor-core (tcgen05, BF16/FP16 in, FP32 accumulate) trailing update used
+// by the mixed-precision factorizations.  Implemented in gemm_tc.cu.
+#pragma once
+
+#include "nmx_common.cuh"
+
+#define NMX_PREC_BF16 1
+#define NMX_PREC_FP16 2
+
+namespace nmx {
+
+// C[M x N] -= round(A)[M x K] * round(B)[K x N], fp32 row-major operands,
+// rounded to BF16 (precision = NMX_PREC_BF16) or FP16 into `ws` first.
+// C must be 16-byte aligned with ldc % 4 == 0.
+int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
+                    int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
+                    size_t ws_bytes);
+
+// Workspace tc_gemm_sub_f32 needs for an M x N x K update.
+size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K);
+
+}  // namespace nmx

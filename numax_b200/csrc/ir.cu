@@ -1,0 +1,561 @@
+// Mixed-precision LU solve with iterative refinement (sm_100a).
+//
+// Not in numax (its GPU path is FP32-only and has no refinement); the
+// north-star addition for the large solve.  A (FP64, row-major) is factored
+// once in low precision and the solution is refined in FP64:
+//
+//   W = (float) R A C        R, C power-of-two row/column scalings (exact)
+//   P W = L U                the recursive LU of dense_lu.cu with its trailing
+//                            updates on the tensor cores (BF16 or FP16 in,
+//                            FP32 accumulate) or FP32 CUDA cores
+//   x = 0, r = b
+//   repeat: d = C U^-1 L^-1 P R r   (triangular solves read the FP32 factors,
+//                                    arithmetic in FP64)
+//           x += d; r = b - A x (FP64 GEMV over the original A)
+//   until ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol
+//
+// GMRES-IR (Carson & Higham) replaces the correction solve by restarted
+// GMRES on the left-preconditioned system (U^-1 L^-1 P R A C) y = U^-1 L^-1 P R r,
+// all Krylov arithmetic in FP64 with A applied in FP64, for conditioning
+// beyond what plain refinement with 16-bit factors converges on.
+//
+// The single-right-hand-side triangular solves are one persistent kernel
+// each: CTAs take 64-row blocks in order from an atomic counter, stream the
+// block's row segments left of the diagonal as the solution blocks they need
+// become ready (a release/acquire counter of finished blocks), then solve the
+// 64 x 64 diagonal block.  Every wait is bounded.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dense_common.cuh"
+#include "gemm_tc.cuh"
+
+namespace nmx {
+
+constexpr int kTrsvRB = 64;
+constexpr int kTrsvThreads = 256;
+constexpr long long kTrsvSpin = 1ll << 25;
+
+__device__ __forceinline__ int ld_acquire_i32(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_i32(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Solve with the unit-lower (UPPER = false) or upper (UPPER = true) triangle
+// of the FP32 factor F (n x n, ldf) in place on the FP64 vector x.
+// counter[0]: block ticket, counter[1]: blocks finished, counter[2]: error.
+template <bool UPPER>
+__global__ void __launch_bounds__(kTrsvThreads)
+    trsv_f32f64_kernel(const float *F, int64_t ldf, int n, double *x, int *counter) {
+    __shared__ float Dg[kTrsvRB][kTrsvRB + 1];
+    __shared__ double acc_s[kTrsvRB];
+    __shared__ int s_blk, s_avail, s_fail;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int NB = (n + kTrsvRB - 1) / kTrsvRB;
+    for (;;) {
+        if (tid == 0) s_blk = atomicAdd(&counter[0], 1);
+        __syncthreads();
+        const int ticket = s_blk;
+        __syncthreads();
+        if (ticket >= NB) return;
+        const int b = UPPER ? NB - 1 - ticket : ticket;  // row block
+        const int r0 = b * kTrsvRB, rows = min(kTrsvRB, n - r0);
+        // Diagonal block into shared memory while earlier blocks finish.
+        for (int e = tid; e < rows * rows; e += kTrsvThreads) {
+            const int i = e / rows, j = e - i * rows;
+            Dg[i][j] = F[(int64_t)(r0 + i) * ldf + r0 + j];
+        }
+        // Each warp owns rows r0 + 8*warp .. +8; lanes stride the columns.
+        double acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+        int done = 0;  // column blocks consumed
+        while (done < ticket) {
+            if (tid == 0) {
+                long long spins = 0;
+                int avail;
+                while ((avail = ld_acquire_i32(&counter[1])) <= done) {
+                    if (++spins > kTrsvSpin) {
+                        atomicExch(&counter[2], 1);
+                        avail = -1;
+                        break;
+                    }
+                    if (spins > 32) __nanosleep(100);
+                }
+                s_avail = avail;
+            }
+            __syncthreads();
+            const int avail = s_avail;
+            __syncthreads();
+            if (avail < 0) return;
+            // Columns of the newly finished blocks (for the upper solve, the
+            // blocks finished so far are the last ones: block NB-1 first).
+            const int nd = min(avail, ticket);
+            int c0, c1;
+            if (!UPPER) {
+                c0 = done * kTrsvRB;
+                c1 = nd * kTrsvRB;
+            } else {
+                c1 = done == 0 ? n : (NB - done) * kTrsvRB;
+                c0 = (NB - nd) * kTrsvRB;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int i = 8 * warp + q;
+                if (i < rows) {
+                    const float *row = F + (int64_t)(r0 + i) * ldf;
+                    double s = 0.0;
+                    for (int c = c0 + lane; c < c1; c += 32) s += (double)row[c] * __ldcg(&x[c]);
+                    acc[q] += s;
+                }
+            }
+            done = nd;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            double s = acc[q];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0 && 8 * warp + q < rows) acc_s[8 * warp + q] = s;
+        }
+        __syncthreads();
+        // The diagonal block, one warp: lane l owns rows l and l + 32.
+        if (warp == 0) {
+            double y0 = 0.0, y1 = 0.0;
+            if (lane < rows) y0 = x[r0 + lane] - acc_s[lane];
+            if (lane + 32 < rows) y1 = x[r0 + lane + 32] - acc_s[lane + 32];
+            if (!UPPER) {
+                for (int j = 0; j < rows; ++j) {
+                    const double xj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
+                    if (lane > j && lane < rows) y0 -= (double)Dg[lane][j] * xj;
+                    if (lane + 32 > j && lane + 32 < rows) y1 -= (double)Dg[lane + 32][j] * xj;
+                }
+            } else {
+                for (int j = rows - 1; j >= 0; --j) {
+                    const double d = (double)Dg[j][j];
+                    if (j < 32 && lane == j) y0 /= d;
+                    if (j >= 32 && lane + 32 == j) y1 /= d;
+                    const double xj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
+                    if (lane < j) y0 -= (double)Dg[lane][j] * xj;
+                    if (lane + 32 < j) y1 -= (double)Dg[lane + 32][j] * xj;
+                }
+            }
+            if (lane < rows) x[r0 + lane] = y0;
+            if (lane + 32 < rows) x[r0 + lane + 32] = y1;
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) st_release_i32(&counter[1], ticket + 1);
+        }
+        __syncthreads();
+    }
+}
+
+// r = b - A x (FP64), one warp per row; rmax <- max |r_i| (as ordered bits).
+__global__ void residual_kernel(const double *A, int64_t lda, int n, const double *x,
+                                const double *b, double *r, unsigned long long *rmax) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double *row = A + (int64_t)warp * lda;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int c = lane;
+    for (; c + 96 < n; c += 128) {
+        s0 += row[c] * x[c];
+        s1 += row[c + 32] * x[c + 32];
+        s2 += row[c + 64] * x[c + 64];
+        s3 += row[c + 96] * x[c + 96];
+    }
+    for (; c < n; c += 32) s0 += row[c] * x[c];
+    double s = (s0 + s1) + (s2 + s3);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const double v = b[warp] - s;
+        r[warp] = v;
+        atomicMax(rmax, (unsigned long long)__double_as_longlong(fabs(v)));
+    }
+}
+
+// max_i sum_j |A_ij| (||A||_inf) and optional per-row max |A_ij|.
+__global__ void row_norms_kernel(const double *A, int64_t lda, int n, unsigned long long *norm_inf,
+                                 double *rowmax) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double *row = A + (int64_t)warp * lda;
+    double s = 0.0, m = 0.0;
+    for (int c = lane; c < n; c += 32) {
+        const double v = fabs(row[c]);
+        s += v;
+        m = fmax(m, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if (lane == 0) {
+        atomicMax(norm_inf, (unsigned long long)__double_as_longlong(s));
+        if (rowmax) rowmax[warp] = m;
+    }
+}
+
+__global__ void absmax_kernel(const double *v, int n, unsigned long long *out) {
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmax(m, fabs(v[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// Power of two nearest 1/m (1 for m == 0 or non-finite m).
+__device__ __forceinline__ double pow2_inv(double m) {
+    if (!(m > 0.0) || !isfinite(m)) return 1.0;
+    return exp2(-rint(log2(m)));
+}
+
+// Row scales from the row maxima.
+__global__ void row_scale_kernel(const double *rowmax, int n, double *rs, int enabled) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rs[i] = enabled ? pow2_inv(rowmax[i]) : 1.0;
+}
+
+// Column maxima of R A (one thread per column, coalesced across threads).
+__global__ void col_scale_kernel(const double *A, int64_t lda, int n, const double *rs, double *cs,
+                                 int enabled) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    if (!enabled) {
+        cs[j] = 1.0;
+        return;
+    }
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) m = fmax(m, fabs(A[(int64_t)i * lda + j] * rs[i]));
+    cs[j] = pow2_inv(m);
+}
+
+// W = (float)(R A C).
+__global__ void scale_to_f32_kernel(const double *A, int64_t lda, int n, const double *rs,
+                                    const double *cs, float *W, int64_t ldw) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * n) return;
+    const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
+    W[(int64_t)i * ldw + j] = (float)(A[(int64_t)i * lda + j] * rs[i] * cs[j]);
+}
+
+// v[i] = s[perm[i]] * rs[perm[i]]  (apply P R to a vector).
+__global__ void permute_scale_kernel(const double *s, const int *perm, const double *rs, int n,
+                                     double *v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = s[perm[i]] * rs[perm[i]];
+}
+
+// x += C v  (or x = C v when assign).
+__global__ void axpy_scale_kernel(const double *v, const double *cs, int n, double *x, int assign) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = assign ? cs[i] * v[i] : x[i] + cs[i] * v[i];
+}
+
+__global__ void add_kernel(const double *v, int n, double *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += v[i];
+}
+
+__global__ void scale_vec_kernel(const double *v, const double *cs, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = cs[i] * v[i];
+}
+
+// ---- host side ----------------------------------------------------------
+
+struct IrRun {
+    nmx_ctx ctx;
+    cudaStream_t st;
+    cublasHandle_t h;
+    int n;
+    const double *A;
+    int64_t lda;
+    float *W;
+    int64_t ldw;
+    int *perm;
+    double *rs, *cs, *v, *r, *tmp, *rowmax;
+    int *counters;  // 3 per triangular solve
+    unsigned long long *norms;  // [0] ||A||_inf, [1] ||r||, [2] ||x||, [3] ||b||, [4] scratch
+};
+
+static double bits_to_double(unsigned long long u) {
+    double d;
+    std::memcpy(&d, &u, sizeof d);
+    return d;
+}
+
+// v := U^-1 L^-1 v (the FP32 factors in W, arithmetic in FP64).
+static int lu_solve_inplace(IrRun &R, double *v) {
+    const int NB = (R.n + kTrsvRB - 1) / kTrsvRB;
+    const int grid = std::min(NB, 2 * R.ctx->sm_count);
+    NMX_CUDA_TRY(cudaMemsetAsync(R.counters, 0, 6 * sizeof(int), R.st));
+    trsv_f32f64_kernel<false><<<grid, kTrsvThreads, 0, R.st>>>(R.W, R.ldw, R.n, v, R.counters);
+    trsv_f32f64_kernel<true><<<grid, kTrsvThreads, 0, R.st>>>(R.W, R.ldw, R.n, v, R.counters + 3);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// out = C U^-1 L^-1 P R in   (the preconditioned correction of one residual).
+static int precond_apply(IrRun &R, const double *in, double *out) {
+    const int threads = 256, blocks = (int)ceil_div(R.n, threads);
+    permute_scale_kernel<<<blocks, threads, 0, R.st>>>(in, R.perm, R.rs, R.n, R.tmp);
+    int rc = lu_solve_inplace(R, R.tmp);
+    if (rc) return rc;
+    scale_vec_kernel<<<blocks, threads, 0, R.st>>>(R.tmp, R.cs, R.n, out);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// out = A in (FP64) via the residual kernel with b = 0 (out = -A in).
+static int apply_A(IrRun &R, const double *in, double *out, const double *zero) {
+    const int threads = 256, blocks = (int)ceil_div((int64_t)R.n * 32, threads);
+    residual_kernel<<<blocks, threads, 0, R.st>>>(R.A, R.lda, R.n, in, zero, out, R.norms + 4);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const double *b,
+                   double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
+                   void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n64 >= 1 && n64 <= (1 << 17), 2, "n must be in 1..131072");
+    NMX_ARG_CHECK(A != nullptr, 3, "A is NULL");
+    NMX_ARG_CHECK(lda >= n64, 4, "lda < n");
+    NMX_ARG_CHECK(b != nullptr, 5, "b is NULL");
+    NMX_ARG_CHECK(x != nullptr, 6, "x is NULL");
+    const int prec = mode & 0xF;
+    const bool gmres = (mode & NMX_IR_GMRES) != 0;
+    NMX_ARG_CHECK(prec == NMX_IR_BF16 || prec == NMX_IR_FP16 || prec == NMX_IR_FP32, 7,
+                  "mode must be NMX_IR_BF16/FP16/FP32, optionally | NMX_IR_GMRES");
+    NMX_ARG_CHECK(tol >= 0.0, 8, "tol < 0");
+    NMX_ARG_CHECK(max_iter >= 1 && max_iter <= 10000, 9, "max_iter must be in 1..10000");
+    const int n = (int)n64;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    IrRun R;
+    R.ctx = ctx;
+    R.st = st;
+    R.n = n;
+    R.A = A;
+    R.lda = lda;
+    int rc = ctx_cublas(ctx, st, &R.h);
+    if (rc) return rc;
+    // Workspace: FP32 factor, vectors, 16-bit GEMM operands.
+    R.ldw = (n + 7) / 8 * 8;
+    void *wv = nullptr;
+    rc = ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * R.ldw + 256, &wv);
+    if (rc) return rc;
+    R.W = static_cast<float *>(wv);
+    const int restart = 60;
+    size_t vec_bytes = sizeof(double) * (size_t)n * 8 + sizeof(int) * (size_t)n * 2 + 4096;
+    void *vv = nullptr;
+    rc = ctx->ensure_slot(kWsVec, vec_bytes, &vv);
+    if (rc) return rc;
+    char *vp = static_cast<char *>(vv);
+    R.norms = reinterpret_cast<unsigned long long *>(vp);
+    R.counters = reinterpret_cast<int *>(vp + 256);
+    double *dv = reinterpret_cast<double *>(vp + 1024);
+    R.rs = dv;
+    R.cs = dv + n;
+    R.v = dv + 2 * (size_t)n;
+    R.r = dv + 3 * (size_t)n;
+    R.tmp = dv + 4 * (size_t)n;
+    R.rowmax = dv + 5 * (size_t)n;
+    double *zero = dv + 6 * (size_t)n;
+    double *aux = dv + 7 * (size_t)n;
+    R.perm = reinterpret_cast<int *>(dv + 8 * (size_t)n);
+    int32_t *ipiv = R.perm + n;
+    int32_t *info_d = reinterpret_cast<int32_t *>(R.counters + 16);
+    GemmSub gs;
+    gs.h = R.h;
+    gs.st = st;
+    gs.precision = prec == NMX_IR_FP32 ? 0 : (prec == NMX_IR_FP16 ? NMX_PREC_FP16 : NMX_PREC_BF16);
+    if (gs.precision) {
+        const int64_t half = (n / 2 + 31) / 32 * 32;
+        gs.ws_bytes = tc_gemm_workspace_bytes(n - half, n - half, half) + 4096;
+        rc = ctx->ensure_slot(kWsGemm16, gs.ws_bytes, &gs.ws);
+        if (rc) return rc;
+    }
+    const int threads = 256;
+    const int vb = (int)ceil_div(n, threads);
+    const int wb = (int)ceil_div((int64_t)n * 32, threads);
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    NMX_CUDA_TRY(cudaEventRecord(e0, st));
+    // ||A||_inf, equilibration (power-of-two scalings; FP16 factors need the range).
+    NMX_CUDA_TRY(cudaMemsetAsync(R.norms, 0, 8 * sizeof(unsigned long long), st));
+    NMX_CUDA_TRY(cudaMemsetAsync(zero, 0, sizeof(double) * n, st));
+    row_norms_kernel<<<wb, threads, 0, st>>>(A, lda, n, R.norms, R.rowmax);
+    const int equil = prec == NMX_IR_FP16 ? 1 : 0;
+    row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
+    col_scale_kernel<<<vb, threads, 0, st>>>(A, lda, n, R.rs, R.cs, equil);
+    scale_to_f32_kernel<<<(unsigned)ceil_div((int64_t)n * n, threads), threads, 0, st>>>(
+        A, lda, n, R.rs, R.cs, R.W, R.ldw);
+    NMX_CUDA_TRY(cudaGetLastError());
+    rc = getrf_run<float>(ctx, gs, n, R.W, R.ldw, ipiv, info_d);
+    if (rc) return rc;
+    NMX_CUDA_TRY(cudaEventRecord(e1, st));
+    // Pivots -> permutation on the host (the interchanges compose in order).
+    std::vector<int32_t> hp(n), perm(n);
+    int32_t hinfo = 0;
+    NMX_CUDA_TRY(cudaMemcpyAsync(hp.data(), ipiv, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaMemcpyAsync(&hinfo, info_d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    unsigned long long hnorm[8];
+    NMX_CUDA_TRY(cudaMemcpyAsync(hnorm, R.norms, sizeof hnorm, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int j = 0; j < n; ++j)
+        if (hp[j] != j) std::swap(perm[j], perm[hp[j]]);
+    NMX_CUDA_TRY(cudaMemcpyAsync(R.perm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    const double normA = bits_to_double(hnorm[0]);
+    // ||b||_inf
+    absmax_kernel<<<std::min(vb, 1024), threads, 0, st>>>(b, n, R.norms + 3);
+    // x = 0, r = b
+    NMX_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    NMX_CUDA_TRY(cudaMemcpyAsync(R.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    int it = 0, inner_total = 0;
+    double berr = INFINITY, prev = INFINITY;
+    bool use_gmres = gmres;
+    std::vector<double> H((size_t)(restart + 1) * restart), cs_g(restart), sn_g(restart),
+        gvec(restart + 1), y(restart);
+    void *kv = nullptr;
+    for (it = 1; it <= max_iter; ++it) {
+        if (!use_gmres) {
+            rc = precond_apply(R, R.r, R.v);  // d = M^-1 r
+            if (rc) return rc;
+            add_kernel<<<vb, threads, 0, st>>>(R.v, n, x);
+            NMX_CUDA_TRY(cudaGetLastError());
+        } else {
+            // Restarted GMRES on M^-1 A d = M^-1 r, M^-1 = C U^-1 L^-1 P R.
+            rc = ctx->ensure_slot(kWsKrylov, sizeof(double) * ((size_t)n * (restart + 1) + 2 * 64), &kv);
+            if (rc) return rc;
+            double *Vk = static_cast<double *>(kv);
+            double *hdev = Vk + (size_t)n * (restart + 1);
+            std::vector<double> hh(restart + 1);
+            rc = precond_apply(R, R.r, Vk);  // z0 = M^-1 r
+            if (rc) return rc;
+            double beta = 0.0;
+            NMX_CUBLAS_TRY(cublasDnrm2(R.h, n, Vk, 1, &beta));
+            NMX_CUDA_TRY(cudaStreamSynchronize(st));
+            if (!(beta > 0.0)) break;
+            const double inv = 1.0 / beta;
+            NMX_CUBLAS_TRY(cublasDscal(R.h, n, &inv, Vk, 1));
+            std::fill(gvec.begin(), gvec.end(), 0.0);
+            gvec[0] = beta;
+            int k = 0;
+            for (; k < restart; ++k) {
+                double *vk = Vk + (size_t)k * n, *w = Vk + (size_t)(k + 1) * n;
+                rc = apply_A(R, vk, aux, zero);  // aux = -A vk
+                if (rc) return rc;
+                const double minus = -1.0;
+                NMX_CUBLAS_TRY(cublasDscal(R.h, n, &minus, aux, 1));
+                rc = precond_apply(R, aux, w);
+                if (rc) return rc;
+                // Classical Gram-Schmidt, twice (CGS2): h = V^T w, w -= V h.
+                const double one = 1.0, zero_d = 0.0, mone = -1.0;
+                for (int pass = 0; pass < 2; ++pass) {
+                    NMX_CUBLAS_TRY(cublasDgemv(R.h, CUBLAS_OP_T, n, k + 1, &one, Vk, n, w, 1,
+                                               &zero_d, hdev, 1));
+                    NMX_CUBLAS_TRY(cublasDgemv(R.h, CUBLAS_OP_N, n, k + 1, &mone, Vk, n, hdev, 1,
+                                               &one, w, 1));
+                    NMX_CUDA_TRY(cudaMemcpyAsync(hh.data(), hdev, sizeof(double) * (k + 1),
+                                                 cudaMemcpyDeviceToHost, st));
+                    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+                    for (int j = 0; j <= k; ++j)
+                        H[(size_t)j * restart + k] = (pass == 0 ? 0.0 : H[(size_t)j * restart + k]) + hh[j];
+                }
+                double hn = 0.0;
+                NMX_CUBLAS_TRY(cublasDnrm2(R.h, n, w, 1, &hn));
+                NMX_CUDA_TRY(cudaStreamSynchronize(st));
+                H[(size_t)(k + 1) * restart + k] = hn;
+                if (hn > 0.0) {
+                    const double ih = 1.0 / hn;
+                    NMX_CUBLAS_TRY(cublasDscal(R.h, n, &ih, w, 1));
+                }
+                // Givens rotations on column k of H.
+                for (int j = 0; j < k; ++j) {
+                    const double a = H[(size_t)j * restart + k], bb = H[(size_t)(j + 1) * restart + k];
+                    H[(size_t)j * restart + k] = cs_g[j] * a + sn_g[j] * bb;
+                    H[(size_t)(j + 1) * restart + k] = -sn_g[j] * a + cs_g[j] * bb;
+                }
+                const double a = H[(size_t)k * restart + k], bb = H[(size_t)(k + 1) * restart + k];
+                const double rr = std::hypot(a, bb);
+                cs_g[k] = rr > 0 ? a / rr : 1.0;
+                sn_g[k] = rr > 0 ? bb / rr : 0.0;
+                H[(size_t)k * restart + k] = rr;
+                H[(size_t)(k + 1) * restart + k] = 0.0;
+                gvec[k + 1] = -sn_g[k] * gvec[k];
+                gvec[k] = cs_g[k] * gvec[k];
+                ++inner_total;
+                if (std::fabs(gvec[k + 1]) <= 1e-6 * beta || hn == 0.0) {
+                    ++k;
+                    break;
+                }
+            }
+            // y = H^-1 g (upper triangular k x k), d = V y, x += d.
+            for (int i = k - 1; i >= 0; --i) {
+                double s = gvec[i];
+                for (int j = i + 1; j < k; ++j) s -= H[(size_t)i * restart + j] * y[j];
+                y[i] = s / H[(size_t)i * restart + i];
+            }
+            for (int j = 0; j < k; ++j)
+                NMX_CUBLAS_TRY(cublasDaxpy(R.h, n, &y[j], Vk + (size_t)j * n, 1, x, 1));
+        }
+        // r = b - A x; norms.
+        NMX_CUDA_TRY(cudaMemsetAsync(R.norms + 1, 0, 2 * sizeof(unsigned long long), st));
+        residual_kernel<<<wb, threads, 0, st>>>(A, lda, n, x, b, R.r, R.norms + 1);
+        absmax_kernel<<<std::min(vb, 1024), threads, 0, st>>>(x, n, R.norms + 2);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_CUDA_TRY(cudaMemcpyAsync(hnorm, R.norms, sizeof hnorm, cudaMemcpyDeviceToHost, st));
+        NMX_CUDA_TRY(cudaStreamSynchronize(st));
+        const double rn = bits_to_double(hnorm[1]), xn = bits_to_double(hnorm[2]),
+                     bn = bits_to_double(hnorm[3]);
+        berr = rn / (normA * xn + bn);
+        int terr[6] = {0, 0, 0, 0, 0, 0};
+        NMX_CUDA_TRY(cudaMemcpy(terr, R.counters, sizeof terr, cudaMemcpyDeviceToHost));
+        if (terr[2] || terr[5]) {
+            set_error("triangular solve: a bounded wait expired");
+            return NMX_ERR_INTERNAL;
+        }
+        if (berr <= tol || !std::isfinite(berr)) break;
+        // Plain refinement that stops contracting hands over to GMRES-IR when allowed.
+        if (!use_gmres && (mode & NMX_IR_AUTO) && berr > 0.5 * prev) use_gmres = true;
+        prev = berr;
+    }
+    NMX_CUDA_TRY(cudaEventRecord(e2, st));
+    NMX_CUDA_TRY(cudaEventSynchronize(e2));
+    if (stats) {
+        float f_ms = 0, r_ms = 0;
+        cudaEventElapsedTime(&f_ms, e0, e1);
+        cudaEventElapsedTime(&r_ms, e1, e2);
+        stats->iterations = std::min(it, max_iter);
+        stats->gmres_iterations = inner_total;
+        stats->converged = berr <= tol ? 1 : 0;
+        stats->info = hinfo;
+        stats->backward_error = berr;
+        stats->factor_ms = f_ms;
+        stats->refine_ms = r_ms;
+        stats->used_gmres = use_gmres ? 1 : 0;
+        stats->reserved = 0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    return 0;
+}
+
+}  // namespace nmx
+
+extern "C" NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda,
+                                       const double *b, double *x, int mode, double tol,
+                                       int max_iter, nmx_ir_stats *stats, void *stream) {
+    return nmx::gesv_ir(ctx, n, A, lda, b, x, mode, tol, max_iter, stats, stream);
+}

@@ -63,9 +63,19 @@ struct nmx_context {
     void *workspace = nullptr;
     size_t workspace_bytes = 0;
     void *cublas = nullptr;  // cublasHandle_t, created on first dense call
+    // Grow-only named device buffers, one per use, kept for the context's life.
+    static constexpr int kSlots = 8;
+    void *slot_ptr[kSlots] = {};
+    size_t slot_bytes[kSlots] = {};
     // Returns a device buffer of at least `bytes`, reusing the context's.
     int ensure_workspace(size_t bytes);
+    // Same for slot `slot` (see nmx::WsSlot); *out receives the buffer.
+    int ensure_slot(int slot, size_t bytes, void **out);
 };
+
+namespace nmx {
+enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4 };
+}
 
 namespace nmx {
 

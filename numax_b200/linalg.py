@@ -167,3 +167,75 @@ def cholesky_solve(lower, b):
                   L.stride(0), x.data_ptr(), x.shape[1], _stream(lower.device))
     torch.cuda.current_stream(lower.device).synchronize()
     return x.reshape(b.shape)
+
+
+class QR:
+    """A blocked Householder QR (numax's `QR`, numax/linalg/qr.mojo:330-612):
+    `factored` in LAPACK's packed form plus `taus`."""
+
+    def __init__(self, factored, taus):
+        self.factored = factored
+        self.taus = taus
+        self.m, self.n = factored.shape
+
+    def r(self):
+        """The n x n upper-triangular R (numax/linalg/qr.mojo:371-403)."""
+        return torch.triu(self.factored[: self.n, : self.n]).contiguous()
+
+    def q(self):
+        """The thin m x n Q with orthonormal columns (numax/linalg/qr.mojo:405-468)."""
+        f = self.factored
+        q = torch.empty((self.m, self.n), dtype=f.dtype, device=f.device)
+        if self.n:
+            _lib.call(f"nmx_orgqr_{_SUF[f.dtype]}", _ctx(f.device), self.m, self.n, f.data_ptr(),
+                      f.stride(0), self.taus.data_ptr(), q.data_ptr(), q.stride(0), _stream(f.device))
+        torch.cuda.current_stream(f.device).synchronize()
+        return q
+
+
+def qr_factor(a) -> QR:
+    """Householder QR of an m x n matrix with m >= n (numax/linalg/qr.mojo:615-743)."""
+    _check_matrix("a", a, square=False)
+    m, n = a.shape
+    if m < n:
+        raise ValueError(f"qr_factor needs m >= n, got {m} x {n}")
+    dev = _resolve_device(a.device)
+    f = _dense_copy(a)
+    tau = torch.zeros(n, dtype=a.dtype, device=dev)
+    if n:
+        _lib.call(f"nmx_geqrf_{_SUF[a.dtype]}", _ctx(dev), m, n, f.data_ptr(), f.stride(0),
+                  tau.data_ptr(), _stream(dev))
+    torch.cuda.current_stream(dev).synchronize()
+    return QR(f, tau)
+
+
+_IR_MODES = {"bf16": _lib.NMX_IR_BF16, "fp16": _lib.NMX_IR_FP16, "fp32": _lib.NMX_IR_FP32}
+
+
+def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: float = 1e-14,
+             max_iter: int = 50):
+    """x with a x = b for float64 a, b: low-precision LU (BF16/FP16 tensor-core
+    trailing updates, or FP32) refined in FP64 to backward error <= tol, with
+    GMRES-IR when `gmres` is True (or "auto": when plain refinement stalls).
+
+    Returns (x, stats) with stats a dict: iterations, gmres_iterations,
+    converged, info, used_gmres, backward_error, factor_ms, refine_ms."""
+    _check_matrix("a", a)
+    if a.dtype != torch.float64:
+        raise TypeError("solve_ir needs float64 a and b")
+    dev = _resolve_device(a.device)
+    n = a.shape[0]
+    A = a.contiguous()
+    bb = _as_rhs(b, n, torch.float64, a.device).reshape(n)
+    x = torch.empty(n, dtype=torch.float64, device=dev)
+    mode = _IR_MODES[precision]
+    if gmres is True:
+        mode |= _lib.NMX_IR_GMRES
+    elif gmres == "auto":
+        mode |= _lib.NMX_IR_AUTO
+    st = _lib.IrStats()
+    import ctypes as _C
+    _lib.call("nmx_gesv_ir_f64", _ctx(dev), n, A.data_ptr(), A.stride(0), bb.data_ptr(),
+              x.data_ptr(), mode, float(tol), int(max_iter), _C.byref(st), _stream(dev))
+    stats = {f: getattr(st, f) for f, _ in _lib.IrStats._fields_ if f != "reserved"}
+    return x.reshape(b.shape), stats
