@@ -300,6 +300,84 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
     return out
 
 
+def make_eigh_batch(count, dev, seed=SEED):
+    """Half harmonic-well Hamiltonians (n = 24 on [-4, 4], omega ~ U[0.5, 2];
+    diagonal 1/dx^2 + omega^2 x^2 / 2, off-diagonal -1/(2 dx^2)) and half
+    dense (G + G^T)/2 with n ~ U{16..64}; float32, ragged row-major."""
+    import torch
+    from numax_b200.batched import ragged_offsets
+    rng = np.random.Generator(np.random.PCG64(seed + 5))
+    half = count // 2
+    ns = np.concatenate([np.full(half, 24), rng.integers(16, 65, size=count - half)]).astype(np.int32)
+    a_off = ragged_offsets(ns)
+    A = torch.empty(int((ns.astype(np.int64) ** 2).sum()), dtype=torch.float32, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 9)
+    n, dx = 24, 8.0 / 23
+    omega = torch.rand(half, generator=gen, dtype=torch.float64, device=dev) * 1.5 + 0.5
+    xg = -4.0 + dx * torch.arange(n, dtype=torch.float64, device=dev)
+    H = torch.zeros((half, n, n), dtype=torch.float64, device=dev)
+    idx = torch.arange(n, device=dev)
+    H[:, idx, idx] = 1.0 / dx ** 2 + (omega[:, None] ** 2) * xg[None, :] ** 2 / 2
+    H[:, idx[:-1], idx[1:]] = -0.5 / dx ** 2
+    H[:, idx[1:], idx[:-1]] = -0.5 / dx ** 2
+    A[: half * n * n] = H.reshape(-1).to(torch.float32)
+    ns_t = torch.from_numpy(ns).to(dev)
+    a_off_t = torch.from_numpy(a_off).to(dev)
+    for m in range(16, 65):
+        sel = torch.nonzero(ns_t[half:] == m).flatten() + half
+        if sel.numel() == 0:
+            continue
+        g = torch.randn((sel.numel(), m, m), generator=gen, dtype=torch.float64, device=dev)
+        sym = (g + g.transpose(1, 2)) / 2
+        pos = a_off_t[sel][:, None] + torch.arange(m * m, device=dev)[None, :]
+        A[pos.flatten()] = sym.reshape(-1).to(torch.float32)
+    return ns, A
+
+
+def run_eigh(count, dev, steps=3, tol=1e-7, max_sweeps=20):
+    """Batched Jacobi eigh throughput (matrices/s) and float32 eigenvalue
+    error against float64 LAPACK (cuSOLVER) on a sample."""
+    import torch
+    import numax_b200 as nb
+    from numax_b200.batched import ragged_offsets
+    ns, A = make_eigh_batch(count, dev)
+    plan = nb.EighBatch(ns, device=dev)
+    W = torch.empty(plan.w_elems, dtype=torch.float32, device=dev)
+    V = torch.empty(plan.a_elems, dtype=torch.float32, device=dev)
+    sw = torch.empty(len(ns), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(2):
+        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    sweeps = sw.double()
+    # Error on a sample: 256 wells + 256 dense.
+    ao, wo = ragged_offsets(ns), ragged_offsets(ns, 1)
+    worst = 0.0
+    half = count // 2
+    for i in list(range(0, 256)) + list(range(half, half + 256)):
+        n = int(ns[i])
+        a = A[ao[i]:ao[i] + n * n].double().reshape(n, n)
+        ref = torch.linalg.eigvalsh(a)
+        got = W[wo[i]:wo[i] + n].double()
+        worst = max(worst, float((got - ref).abs().max() / ref.abs().max()))
+    n64 = ns.astype(np.float64)
+    swp = sweeps.cpu().numpy()
+    flops = float((9.0 * n64 ** 2 * (n64 - 1) * swp).sum())
+    bytes_ = float((4 * (2 * n64 ** 2 + n64)).sum())
+    return {"count": count, "ms": ms, "matrices_per_s": count / (ms / 1e3),
+            "mean_sweeps": float(swp.mean()), "max_sweeps": int(swp.max()),
+            "max_rel_eig_err_vs_fp64": worst, "flop_rate_tflops": flops / (ms / 1e3) / 1e12,
+            "hbm_gbs": bytes_ / (ms / 1e3) / 1e9}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -411,6 +489,14 @@ def run_ours(args):
     achieved = abytes / launch_s / 1e9
     traffic = read_traffic()
 
+    eigh = None
+    if world == 1 and args.eigh_count > 0:
+        try:
+            eigh = run_eigh(args.eigh_count, dev)
+            eigh["hbm_frac"] = eigh["hbm_gbs"] / float(peaks.get("hbm_gbs", 6650.0))
+        except Exception as exc:
+            eigh = {"error": f"{type(exc).__name__}: {exc}"}
+
     lu_ir = None
     if world == 1 and args.lu_n > 0:
         try:
@@ -446,6 +532,7 @@ def run_ours(args):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "eigh": eigh,
         "lu_ir": lu_ir,
     }
     print(json.dumps(line), flush=True)
@@ -466,6 +553,8 @@ def main():
     ap.add_argument("--lu-kappas", default="1e2",
                     help="comma-separated condition numbers for the comparison")
     ap.add_argument("--only-lu", action="store_true", help="run only the LU/IR comparison")
+    ap.add_argument("--eigh-count", type=int, default=65536,
+                    help="matrices in the batched Jacobi eigh leg (0 skips it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -266,6 +266,20 @@ typedef struct {
     double refine_ms;         /* device time: the refinement loop */
 } nmx_ir_stats;
 
+/* The trailing-update primitive of the mixed-precision factorizations on its
+ * own: C[M x N] -= round(A)[M x K] * round(B)[K x N] for fp32 row-major
+ * operands, A and B rounded to BF16 (precision 1) or FP16 (precision 2) and
+ * the products accumulated in FP32 on the tcgen05 tensor cores.  C must be
+ * 16-byte aligned with ldc a multiple of 4 and ldc >= N rounded up to 8: the
+ * update runs on N (and K) rounded up to 8 with zero padding, so C's columns
+ * N .. round8(N)-1 are read and written back unchanged.  No numax
+ * counterpart (the role MAX's matmul plays in numax/linalg/lu.mojo:646-673). */
+#define NMX_PREC_BF16 1
+#define NMX_PREC_FP16 2
+NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64_t K, const float *A,
+                             int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc,
+                             int precision, void *stream);
+
 NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, const double *b,
                             double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
                             void *stream);

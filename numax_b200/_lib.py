@@ -57,6 +57,7 @@ SIGNATURES = {
     "nmx_orgqr_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
     "nmx_orgqr_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
     "nmx_gesv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
+    "nmx_gemm_sub_f32": (ci, [vp, i64, i64, i64, vp, i64, vp, i64, vp, i64, ci, vp]),
 }
 
 NMX_IR_BF16 = 1

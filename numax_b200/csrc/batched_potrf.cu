@@ -75,18 +75,28 @@ template <typename T>
 __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *Lg, int lane,
                                                  int *s_info) {
     const T floor_ = pivot_floor<T>::value;
+    // Every index into a[] and w[] below is a compile-time constant (the
+    // loops are unrolled), so both stay in registers.
     T a[kDiagNB];
-    const int ro = prow_off(k + lane, n) + k;
+    int ro[kDiagNB];
 #pragma unroll
-    for (int c = 0; c < kDiagNB; ++c) a[c] = (lane < kb && c <= lane) ? S[ro + c] : T(0);
+    for (int i = 0; i < kDiagNB; ++i) ro[i] = prow_off(k + min(i, kb - 1), n) + k;
+    const int myro = prow_off(k + min(lane, kb - 1), n) + k;
+#pragma unroll
+    for (int c = 0; c < kDiagNB; ++c) a[c] = (lane < kb && c <= lane) ? S[myro + c] : T(0);
+    T myinv = T(0);
+    int bad = 0;
 #pragma unroll
     for (int j = 0; j < kDiagNB; ++j) {
         if (j < kb) {  // warp-uniform
             const T d = __shfl_sync(0xffffffffu, a[j], j);
-            if (lane == 0 && d <= T(0) && *s_info == 0) *s_info = k + j + 1;
+            if (!bad && d <= T(0)) bad = k + j + 1;
             const T g = guard_nonzero(d, floor_);
             const T inv = rsqrt(g);
-            if (lane == j) a[j] = g * inv;
+            if (lane == j) {
+                a[j] = g * inv;
+                myinv = T(1) / guard_nonzero(a[j], floor_);
+            }
             if (lane > j) a[j] *= inv;
             const T lij = a[j];
 #pragma unroll
@@ -96,16 +106,15 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
             }
         }
     }
-    T myinv = T(0);
+    if (lane == 0 && bad && *s_info == 0) *s_info = bad;
     if (lane < kb) {
         T *lrow = Lg + (int64_t)(k + lane) * n + k;
 #pragma unroll
         for (int c = 0; c < kDiagNB; ++c)
             if (c <= lane) {
-                S[ro + c] = a[c];
+                S[myro + c] = a[c];
                 lrow[c] = a[c];
             }
-        myinv = T(1) / guard_nonzero(a[lane], floor_);
     }
     __syncwarp();
     // Column `lane` of W: w = L^-1 e_lane, right-looking over the rows of L.
@@ -118,14 +127,14 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
             w[p] *= __shfl_sync(0xffffffffu, myinv, p);
 #pragma unroll
             for (int i = p + 1; i < kDiagNB; ++i)
-                if (i < kb) w[i] -= S[prow_off(k + i, n) + k + p] * w[p];
+                if (i < kb) w[i] -= S[ro[i] + p] * w[p];
         }
     }
     __syncwarp();
     if (lane < kb) {
 #pragma unroll
         for (int i = 0; i < kDiagNB; ++i)
-            if (i >= lane && i < kb) S[prow_off(k + i, n) + k + lane] = w[i];
+            if (i >= lane && i < kb) S[ro[i] + lane] = w[i];
     }
     __syncwarp();
 }

@@ -19,6 +19,8 @@
 #include <cutlass/gemm/dispatch_policy.hpp>
 #include <cutlass/gemm/kernel/gemm_universal.hpp>
 
+#include <algorithm>
+
 #include "gemm_tc.cuh"
 
 #pragma nv_diag_suppress 20012
@@ -82,51 +84,61 @@ NMX_TC_GEMM(fp16, cutlass::half_t)
 
 }  // namespace tc
 
-// fp32 block (rows x cols, ld) -> 16-bit dense block (ld_out), row-major.
+// fp32 block (rows x cols, ld) -> 16-bit block (rows_p x cols_p, ld_out),
+// zero-filled past rows x cols so padded products contribute exactly 0.
 template <typename Elem>
-__global__ void round_block_kernel(const float *src, int64_t lds, int rows, int cols, Elem *dst,
-                                   int64_t ldd) {
+__global__ void round_block_kernel(const float *src, int64_t lds, int rows, int cols, int rows_p,
+                                   int cols_p, Elem *dst, int64_t ldd) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)rows * cols) return;
-    const int r = (int)(e / cols), c = (int)(e - (int64_t)r * cols);
-    dst[(int64_t)r * ldd + c] = Elem(src[(int64_t)r * lds + c]);
+    if (e >= (int64_t)rows_p * cols_p) return;
+    const int r = (int)(e / cols_p), c = (int)(e - (int64_t)r * cols_p);
+    const float v = (r < rows && c < cols) ? src[(int64_t)r * lds + c] : 0.0f;
+    dst[(int64_t)r * ldd + c] = Elem(v);
 }
+
+// The GEMM runs on K and N rounded up to multiples of 8 (the 16-byte TMA and
+// epilogue granularity): the padded rows/columns of the 16-bit operands are
+// zero, so the extra columns of C (up to N rounded to 8) get C - 0 and are
+// left bit-for-bit unchanged.
+static inline int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
 
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
                     int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
                     size_t ws_bytes) {
     if (M <= 0 || N <= 0 || K <= 0) return 0;
-    const int64_t ldk = (K + 7) / 8 * 8, ldn = (N + 7) / 8 * 8;
-    const size_t need = 2 * (size_t)(M * ldk + K * ldn) + 256;
+    const int64_t Kp = up8(K), Np = up8(N);
+    const size_t need = tc_gemm_workspace_bytes(M, N, K);
     if (need > ws_bytes) {
         set_error("tensor-core update needs %zu B of workspace, have %zu", need, ws_bytes);
         return NMX_ERR_INTERNAL;
     }
-    if ((ldc % 4) != 0 || (reinterpret_cast<uintptr_t>(C) % 16) != 0) {
-        set_error("tensor-core update: C must be 16-byte aligned with ldc % 4 == 0");
+    if ((ldc % 4) != 0 || (reinterpret_cast<uintptr_t>(C) % 16) != 0 || ldc < Np) {
+        set_error("tensor-core update: C must be 16-byte aligned, ldc %% 4 == 0, ldc >= N rounded to 8");
         return NMX_ERR_INTERNAL;
     }
     auto *a16 = static_cast<unsigned char *>(ws);
-    auto *b16 = a16 + ((2 * (size_t)M * ldk + 255) & ~size_t(255));
+    auto *b16 = a16 + ((2 * (size_t)M * Kp + 255) & ~size_t(255));
     const int threads = 256;
+    const unsigned ga = (unsigned)ceil_div(M * Kp, threads), gb = (unsigned)ceil_div(Kp * Np, threads);
     int rc;
     if (precision == NMX_PREC_FP16) {
-        round_block_kernel<cutlass::half_t><<<(unsigned)ceil_div(M * K, threads), threads, 0, st>>>(
-            A, lda, (int)M, (int)K, reinterpret_cast<cutlass::half_t *>(a16), ldk);
-        round_block_kernel<cutlass::half_t><<<(unsigned)ceil_div(K * N, threads), threads, 0, st>>>(
-            B, ldb, (int)K, (int)N, reinterpret_cast<cutlass::half_t *>(b16), ldn);
+        auto *a = reinterpret_cast<cutlass::half_t *>(a16);
+        auto *b = reinterpret_cast<cutlass::half_t *>(b16);
+        round_block_kernel<cutlass::half_t><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                    (int)Kp, a, Kp);
+        round_block_kernel<cutlass::half_t><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N, (int)Kp,
+                                                                    (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
-        rc = tc::fp16::run((int)M, (int)N, (int)K, a16, ldk, b16, ldn, C, ldc, st);
+        rc = tc::fp16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st);
     } else {
-        round_block_kernel<cutlass::bfloat16_t>
-            <<<(unsigned)ceil_div(M * K, threads), threads, 0, st>>>(
-                A, lda, (int)M, (int)K, reinterpret_cast<cutlass::bfloat16_t *>(a16), ldk);
-        round_block_kernel<cutlass::bfloat16_t>
-            <<<(unsigned)ceil_div(K * N, threads), threads, 0, st>>>(
-                B, ldb, (int)K, (int)N, reinterpret_cast<cutlass::bfloat16_t *>(b16), ldn);
+        auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
+        auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
+        round_block_kernel<cutlass::bfloat16_t><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K,
+                                                                        (int)M, (int)Kp, a, Kp);
+        round_block_kernel<cutlass::bfloat16_t><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N,
+                                                                        (int)Kp, (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
-        rc = tc::bf16::run((int)M, (int)N, (int)K, a16, ldk, b16, ldn, C, ldc,
-                                                   st);
+        rc = tc::bf16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st);
     }
     if (rc) {
         set_error("tensor-core GEMM %lldx%lldx%lld failed at step %d", (long long)M, (long long)N,
@@ -138,8 +150,33 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
 }
 
 size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K) {
-    const int64_t ldk = (K + 7) / 8 * 8, ldn = (N + 7) / 8 * 8;
-    return 2 * (size_t)(M * ldk + K * ldn) + 512;
+    const int64_t Kp = up8(K), Np = up8(N);
+    return ((2 * (size_t)M * Kp + 255) & ~size_t(255)) + 2 * (size_t)Kp * Np + 512;
 }
 
 }  // namespace nmx
+
+// ---- C ABI: the trailing-update primitive on its own ------------------------
+extern "C" NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64_t K,
+                                        const float *A, int64_t lda, const float *B, int64_t ldb,
+                                        float *C, int64_t ldc, int precision, void *stream) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(M >= 0 && N >= 0 && K >= 0, 2, "negative size");
+    NMX_ARG_CHECK(A != nullptr || M * K == 0, 5, "A is NULL");
+    NMX_ARG_CHECK(lda >= std::max<int64_t>(1, K), 6, "lda < K");
+    NMX_ARG_CHECK(B != nullptr || K * N == 0, 7, "B is NULL");
+    NMX_ARG_CHECK(ldb >= std::max<int64_t>(1, N), 8, "ldb < N");
+    NMX_ARG_CHECK(C != nullptr || M * N == 0, 9, "C is NULL");
+    NMX_ARG_CHECK(ldc >= std::max<int64_t>(1, N), 10, "ldc < N");
+    NMX_ARG_CHECK(precision == NMX_PREC_BF16 || precision == NMX_PREC_FP16, 11,
+                  "precision must be NMX_PREC_BF16 or NMX_PREC_FP16");
+    if (M == 0 || N == 0 || K == 0) return 0;
+    DeviceGuard g(ctx->device);
+    void *ws = nullptr;
+    const size_t bytes = tc_gemm_workspace_bytes(M, N, K);
+    int rc = ctx->ensure_slot(kWsGemm16, bytes, &ws);
+    if (rc) return rc;
+    return tc_gemm_sub_f32(static_cast<cudaStream_t>(stream), precision, M, N, K, A, lda, B, ldb, C,
+                           ldc, ws, bytes);
+}

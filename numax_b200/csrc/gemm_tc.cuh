@@ -4,8 +4,10 @@
 
 #include "nmx_common.cuh"
 
+#ifndef NMX_PREC_BF16
 #define NMX_PREC_BF16 1
 #define NMX_PREC_FP16 2
+#endif
 
 namespace nmx {
 

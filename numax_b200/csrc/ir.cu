@@ -352,7 +352,7 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     rc = ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * R.ldw + 256, &wv);
     if (rc) return rc;
     R.W = static_cast<float *>(wv);
-    const int restart = 60;
+    const int restart = 200;
     size_t vec_bytes = sizeof(double) * (size_t)n * 8 + sizeof(int) * (size_t)n * 2 + 4096;
     void *vv = nullptr;
     rc = ctx->ensure_slot(kWsVec, vec_bytes, &vv);

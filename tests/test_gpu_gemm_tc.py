@@ -1,0 +1,31 @@
+"""The tensor-core trailing update (tcgen05, BF16/FP16 inputs, FP32
+accumulate) against an FP64 product of the same rounded inputs: normwise
+relative error within 1e-5 (FP32 accumulation), on ragged shapes and
+strided operands."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("m,n,k", [(128, 256, 64), (300, 200, 96), (1000, 513, 257), (37, 64, 16)])
+def test_gemm_sub_tc(prec, m, n, k):
+    from numax_b200 import _lib
+    g = torch.Generator(device="cuda")
+    g.manual_seed(m * 31 + n * 7 + k)
+    lda, ldb, ldc = k + 5, n + 3, (n + 7) // 8 * 8 + 8
+    A = torch.randn((m, lda), generator=g, device="cuda", dtype=torch.float32)
+    B = torch.randn((k, ldb), generator=g, device="cuda", dtype=torch.float32)
+    C = torch.randn((m, ldc), generator=g, device="cuda", dtype=torch.float32)
+    dt = torch.bfloat16 if prec == 1 else torch.float16
+    want = C[:, :n].double() - A[:, :k].to(dt).double() @ B[:, :n].to(dt).double()
+    rc = _lib.load().nmx_gemm_sub_f32(_lib.context(0), m, n, k, A.data_ptr(), lda, B.data_ptr(),
+                                       ldb, C.data_ptr(), ldc, prec,
+                                       torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    err = float((C[:, :n].double() - want).norm() / want.norm())
+    assert err <= 1e-5, err
