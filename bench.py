@@ -272,13 +272,14 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
         del lu
         # BF16 factors + FP64 refinement (GMRES-IR when plain IR stalls).
         res = {"fp64_lu_solve_ms": t64, "fp64_backward_error": be64}
-        for prec, mode in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO),):
+        for prec, mode in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO),
+                           ("fp16", _lib.NMX_IR_FP16 | _lib.NMX_IR_AUTO)):
             x = torch.empty_like(b)
             st = _lib.IrStats()
             e0.record(stream)
             rc = _lib.load().nmx_gesv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
                                              C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
-                                             mode, 1e-14, 100, C.byref(st),
+                                             mode, 1e-14, 30, C.byref(st),
                                              C.c_void_p(stream.cuda_stream))
             e1.record(stream)
             torch.cuda.synchronize(dev)

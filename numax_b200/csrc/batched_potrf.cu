@@ -59,6 +59,14 @@ __host__ __device__ inline int potrf_smem_elems(int nmax, int nrhs) {
     return nmax * (nmax + 1) / 2 + nrhs * nmax + kDiagNB * kPotrfMaxRhs + 2;
 }
 
+// Row of packed lower-triangle index e (e = i(i+1)/2 + j, 0 <= j <= i).
+__device__ __forceinline__ int tri_row(int e) {
+    int i = (int)((sqrtf(8.f * (float)e + 1.f) - 1.f) * 0.5f);
+    i -= (i * (i + 1)) / 2 > e;
+    i += ((i + 1) * (i + 2)) / 2 <= e;
+    return i;
+}
+
 // Start of row i in the packed store: the lower triangle's rows, then the
 // right-hand sides' rows (length n) below them.
 __device__ __forceinline__ int prow_off(int i, int n) {
@@ -291,26 +299,47 @@ __device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, in
     const int TR = (R - r0 + 7) >> 3, TN = (n - r0 + 7) >> 3;
     if (TN <= 0) return;
     const int tiles = TN * (TN + 1) / 2 + (TR - TN) * TN;
-    for (int e = warp; e < tiles; e += NW) {
-        int ti, tj;
+    // Two tiles per pass: independent accumulator chains for the DMMA pipe.
+    for (int e = warp; e < tiles; e += 2 * NW) {
+        const int e2 = e + NW;
+        const bool two = e2 < tiles;
+        int ti, tj, ti2 = 0, tj2 = 0;
         trap_tile(e, TN, ti, tj);
+        if (two) trap_tile(e2, TN, ti2, tj2);
         const int i0 = r0 + 8 * ti, j0 = r0 + 8 * tj;
+        const int i02 = r0 + 8 * ti2, j02 = r0 + 8 * tj2;
         const int arow = prow_off(min(i0 + g, R - 1), n) + k;
         const int brow = prow_off(min(j0 + g, n - 1), n) + k;
-        double c0 = 0.0, c1 = 0.0;
+        const int arow2 = prow_off(min(i02 + g, R - 1), n) + k;
+        const int brow2 = prow_off(min(j02 + g, n - 1), n) + k;
+        double a[4], b[4], a2[4], b2[4];
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
             const int p = kk * 4 + t;
-            const double a = p < kb ? S[arow + p] : 0.0;
-            const double b = p < kb ? S[brow + p] : 0.0;
-            dmma_8x8x4(c0, c1, a, b);
+            a[kk] = p < kb ? S[arow + p] : 0.0;
+            b[kk] = p < kb ? S[brow + p] : 0.0;
+            a2[kk] = (two && p < kb) ? S[arow2 + p] : 0.0;
+            b2[kk] = (two && p < kb) ? S[brow2 + p] : 0.0;
         }
-        const int i = i0 + g;
+        double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            dmma_8x8x4(c0, c1, a[kk], b[kk]);
+            dmma_8x8x4(d0, d1, a2[kk], b2[kk]);
+        }
+        int i = i0 + g;
         if (i < R) {
             const int ro = prow_off(i, n);
             const int j = j0 + 2 * t;
             if (j < n && j <= i) S[ro + j] -= c0;
             if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c1;
+        }
+        i = i02 + g;
+        if (two && i < R) {
+            const int ro = prow_off(i, n);
+            const int j = j02 + 2 * t;
+            if (j < n && j <= i) S[ro + j] -= d0;
+            if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= d1;
         }
     }
 }
@@ -328,12 +357,14 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
     T *X = static_cast<T *>(args.X) + args.b_off[mi];
     if (tid == 0) *s_info = 0;
 
-    // Stage the lower triangle (row i: i+1 contiguous elements) and B^T.
-    for (int i = warp; i < n; i += NW) {
-        const int ro = (i * (i + 1)) / 2;
-        for (int j = lane; j <= i; j += 32) S[ro + j] = A[(int64_t)i * n + j];
-    }
+    // Stage the lower triangle and B^T.  The packed index e of (i, j) is
+    // i(i+1)/2 + j, so the copy is one flat, independent-load loop.
     const int bro = (n * (n + 1)) / 2;
+#pragma unroll 4
+    for (int e = tid; e < bro; e += NT) {
+        int i = tri_row(e);
+        S[e] = A[(int64_t)i * n + (e - (i * (i + 1)) / 2)];
+    }
     for (int e = tid; e < n * nrhs; e += NT) {
         int j = e / nrhs, r = e - j * nrhs;
         S[bro + r * n + j] = B[e];
@@ -388,10 +419,10 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
 
     // Write back L's off-diagonal blocks (the diagonal blocks went out as
     // they were factored) and X.
-    for (int i = warp; i < n; i += NW) {
-        const int ro = (i * (i + 1)) / 2;
-        const int jend = (i / kDiagNB) * kDiagNB;
-        for (int j = lane; j < jend; j += 32) L[(int64_t)i * n + j] = S[ro + j];
+#pragma unroll 4
+    for (int e = tid; e < bro; e += NT) {
+        const int i = tri_row(e), j = e - (i * (i + 1)) / 2;
+        if (j < (i / kDiagNB) * kDiagNB) L[(int64_t)i * n + j] = S[e];
     }
     for (int e = tid; e < n * nrhs; e += NT) {
         int j = e / nrhs, r = e - j * nrhs;

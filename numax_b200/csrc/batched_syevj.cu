@@ -131,40 +131,41 @@ __device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float
                 pq[2 * k + 1] = q;
             }
             group_sync<G>();
-            // 2x2 blocks: rows of pair kr, columns of pair kc.
+            // 2x2 blocks: rows of pair kr, columns of pair kc.  The rotations
+            // were formed in float64; they are applied to the float32 data in
+            // float32.
             for (int e = gt; e < half * half; e += G) {
                 const int kr = e / half, kc = e - kr * half;
                 const int p = pq[2 * kr], q = pq[2 * kr + 1];
                 const int u = pq[2 * kc], v = pq[2 * kc + 1];
                 if (q >= n && v >= n) continue;
-                const double cr = cs[2 * kr], sr = cs[2 * kr + 1];
-                const double cc = cs[2 * kc], sc = cs[2 * kc + 1];
+                const float cr = (float)cs[2 * kr], sr = (float)cs[2 * kr + 1];
+                const float cc = (float)cs[2 * kc], sc = (float)cs[2 * kc + 1];
                 if (q < n && v < n) {
-                    double b00 = As[p * ld + u], b01 = As[p * ld + v];
-                    double b10 = As[q * ld + u], b11 = As[q * ld + v];
+                    const float b00 = As[p * ld + u], b01 = As[p * ld + v];
+                    const float b10 = As[q * ld + u], b11 = As[q * ld + v];
                     // rows: [c -s; s c] applied from the left
-                    double r00 = cr * b00 - sr * b10, r01 = cr * b01 - sr * b11;
-                    double r10 = sr * b00 + cr * b10, r11 = sr * b01 + cr * b11;
+                    const float r00 = cr * b00 - sr * b10, r01 = cr * b01 - sr * b11;
+                    const float r10 = sr * b00 + cr * b10, r11 = sr * b01 + cr * b11;
                     // columns: [c s; -s c] applied from the right
-                    double o00 = cc * r00 - sc * r01, o01 = sc * r00 + cc * r01;
-                    double o10 = cc * r10 - sc * r11, o11 = sc * r10 + cc * r11;
+                    float o00 = cc * r00 - sc * r01, o01 = sc * r00 + cc * r01;
+                    float o10 = cc * r10 - sc * r11, o11 = sc * r10 + cc * r11;
                     if (kr == kc) {
-                        o01 = 0.0;  // the annihilated pair
-                        o10 = 0.0;
+                        o01 = 0.f;  // the annihilated pair
+                        o10 = 0.f;
                     }
-                    As[p * ld + u] = (float)o00;
-                    As[p * ld + v] = (float)o01;
-                    As[q * ld + u] = (float)o10;
-                    As[q * ld + v] = (float)o11;
+                    As[p * ld + u] = o00;
+                    As[p * ld + v] = o01;
+                    As[q * ld + u] = o10;
+                    As[q * ld + v] = o11;
                 } else if (q < n) {  // column pair has the dummy index: only column u exists
-                    double b0 = As[p * ld + u], b1 = As[q * ld + u];
-                    double r0 = cr * b0 - sr * b1, r1 = sr * b0 + cr * b1;
-                    As[p * ld + u] = (float)(cc * r0);
-                    As[q * ld + u] = (float)(cc * r1);
+                    const float b0 = As[p * ld + u], b1 = As[q * ld + u];
+                    As[p * ld + u] = cr * b0 - sr * b1;
+                    As[q * ld + u] = sr * b0 + cr * b1;
                 } else {  // row pair has the dummy index: only row p exists
-                    double b0 = As[p * ld + u], b1 = As[p * ld + v];
-                    As[p * ld + u] = (float)(cr * (cc * b0 - sc * b1));
-                    As[p * ld + v] = (float)(cr * (sc * b0 + cc * b1));
+                    const float b0 = As[p * ld + u], b1 = As[p * ld + v];
+                    As[p * ld + u] = cc * b0 - sc * b1;
+                    As[p * ld + v] = sc * b0 + cc * b1;
                 }
             }
             // V := V J, columns of every pair.
@@ -172,10 +173,10 @@ __device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float
                 const int i = e / half, k = e - i * half;
                 const int p = pq[2 * k], q = pq[2 * k + 1];
                 if (q >= n) continue;
-                const double c = cs[2 * k], s = cs[2 * k + 1];
-                double vp = Vs[i * ld + p], vq = Vs[i * ld + q];
-                Vs[i * ld + p] = (float)(c * vp - s * vq);
-                Vs[i * ld + q] = (float)(s * vp + c * vq);
+                const float c = (float)cs[2 * k], s = (float)cs[2 * k + 1];
+                const float vp = Vs[i * ld + p], vq = Vs[i * ld + q];
+                Vs[i * ld + p] = c * vp - s * vq;
+                Vs[i * ld + q] = s * vp + c * vq;
             }
             group_sync<G>();
         }

@@ -27,64 +27,86 @@
 
 namespace nmx {
 
-constexpr int kLeafW = 32;      // leaf panel width
+constexpr int kLeafW = 32;      // recursion leaf width (the panel a leaf kernel factors)
+constexpr int kLeafMax = 64;    // widest leaf the kernel supports
 constexpr int kLeafThreads = 256;
 constexpr int kTrsmLeaf = 32;
 
+// One CTA's published pivot candidate for one column: |a|, its row, and the
+// column number + 1 that marks the entry as current.
+template <typename T>
+struct LeafSlot {
+    T mag;
+    int row;
+    int seq;
+};
+
 template <typename T>
 struct LeafScratch {
-    T *cand_rows;     // [2][G][kLeafW]
-    T *col_rows;      // [2][kLeafW]
-    T *cand_mag;      // [2][G]
-    int *cand_row;    // [2][G]
-    unsigned *bar;
+    LeafSlot<T> *slots;  // [2][G]
+    T *cand_rows;        // [2][G][kLeafMax] the candidate rows' panel values
+    T *col_rows;         // [2][kLeafMax] row `col` as it was before the swap
     int *err;
 };
 
-// Cooperative leaf: factor columns [c, c+w) over rows [c, n) in place.
+__device__ __forceinline__ int ld_acquire_s32(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_s32(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Cooperative leaf: factor columns [c, c+w) (w <= kLeafMax) over rows [c, n)
+// in place.  Each column is one exchange: every CTA publishes its candidate
+// (value, row, the candidate row and, from its owner, row `col`) in its own
+// slot with a sequence number, then waits until every slot carries the
+// column's number -- the exchange is the barrier, no atomic counter.
 template <typename T>
 __global__ void __launch_bounds__(kLeafThreads)
     getrf_leaf_kernel(T *A, int64_t lda, int n, int c, int w, int rows_per_cta, int32_t *ipiv,
                       int32_t *info, LeafScratch<T> sc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int ldl = kLeafW + 1;
-    T *loc = reinterpret_cast<T *>(smem_raw);           // rows_per_cta x ldl
-    T *prow = loc + (size_t)rows_per_cta * ldl;          // pivot row (w)
+    const int ldl = w | 1;
+    T *loc = reinterpret_cast<T *>(smem_raw);            // rows_per_cta x ldl
+    T *prow = loc + (size_t)rows_per_cta * ldl;           // pivot row (w)
     __shared__ T s_mag[kLeafThreads / 32];
     __shared__ int s_row[kLeafThreads / 32];
-    __shared__ int s_flag, s_piv, s_wcta;
-    __shared__ T s_wmag;
+    __shared__ int s_piv, s_wcta, s_fail;
 
     const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int r0 = c + cta * rows_per_cta;                     // first global row owned
-    const int nloc = max(0, min(rows_per_cta, n - r0));        // rows owned
+    const int r0 = c + cta * rows_per_cta;                // first global row owned
+    const int nloc = max(0, min(rows_per_cta, n - r0));   // rows owned
 
     for (int e = tid; e < nloc * w; e += kLeafThreads) {
         int r = e / w, j = e - r * w;
         loc[r * ldl + j] = A[(int64_t)(r0 + r) * lda + c + j];
     }
+    if (tid == 0) s_fail = 0;
     __syncthreads();
 
     for (int j = 0; j < w; ++j) {
         const int col = c + j;
         const int slot = j & 1;
-        // Local argmax over owned rows with global index >= col.
+        // Local argmax over owned rows with global index >= col; zero and NaN
+        // magnitudes never pivot (numax: strict > starting from 0).
         T best = T(-1);
         int brow = INT32_MAX;
         for (int r = tid; r < nloc; r += kLeafThreads) {
-            int gr = r0 + r;
+            const int gr = r0 + r;
             if (gr < col) continue;
-            T m = fabs(loc[r * ldl + j]);
-            if (!(m > T(0))) continue;  // zero/NaN never pivots (numax: strict > from 0)
+            const T m = fabs(loc[r * ldl + j]);
+            if (!(m > T(0))) continue;
             if (m > best || (m == best && gr < brow)) {
                 best = m;
                 brow = gr;
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
-            T om = __shfl_xor_sync(0xffffffffu, best, o);
-            int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            const T om = __shfl_xor_sync(0xffffffffu, best, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
             if (om > best || (om == best && orow < brow)) {
                 best = om;
                 brow = orow;
@@ -99,72 +121,93 @@ __global__ void __launch_bounds__(kLeafThreads)
             best = lane < kLeafThreads / 32 ? s_mag[lane] : T(-1);
             brow = lane < kLeafThreads / 32 ? s_row[lane] : INT32_MAX;
             for (int o = 16; o > 0; o >>= 1) {
-                T om = __shfl_xor_sync(0xffffffffu, best, o);
-                int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                const T om = __shfl_xor_sync(0xffffffffu, best, o);
+                const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
                 if (om > best || (om == best && orow < brow)) {
                     best = om;
                     brow = orow;
                 }
             }
+            // Publish: the rows first, then the slot, then its sequence number.
+            if (brow != INT32_MAX)
+                for (int q = lane; q < w; q += 32)
+                    sc.cand_rows[((size_t)slot * G + cta) * kLeafMax + q] =
+                        loc[(brow - r0) * ldl + q];
+            if (col >= r0 && col < r0 + nloc)
+                for (int q = lane; q < w; q += 32)
+                    sc.col_rows[slot * kLeafMax + q] = loc[(col - r0) * ldl + q];
+            __threadfence();
+            __syncwarp();
             if (lane == 0) {
-                sc.cand_mag[slot * G + cta] = best;
-                sc.cand_row[slot * G + cta] = brow;
-                s_row[0] = brow;
+                LeafSlot<T> *me = &sc.slots[slot * G + cta];
+                me->mag = best;
+                me->row = brow;
+                __threadfence();
+                st_release_s32(&me->seq, col + 1);
+            }
+            // Wait until every CTA's slot carries this column (bounded).
+            long long spins = 0;
+            bool ready = false;
+            while (!ready) {
+                bool mine = true;
+                for (int g = lane; g < G; g += 32)
+                    mine &= ld_acquire_s32(&sc.slots[slot * G + g].seq) == col + 1;
+                ready = __all_sync(0xffffffffu, mine);
+                if (!ready && ++spins > kSpinLimit) {
+                    if (lane == 0) {
+                        atomicExch(sc.err, 1);
+                        s_fail = 1;
+                    }
+                    break;
+                }
+            }
+            // Every CTA reduces the same candidates in the same order.
+            if (ready) {
+                best = T(-1);
+                brow = INT32_MAX;
+                int bcta = -1;
+                for (int g = lane; g < G; g += 32) {
+                    const T m = __ldcg(&sc.slots[slot * G + g].mag);
+                    const int rr = __ldcg(&sc.slots[slot * G + g].row);
+                    if (m > best || (m == best && rr < brow)) {
+                        best = m;
+                        brow = rr;
+                        bcta = g;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const T om = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                    const int octa = __shfl_xor_sync(0xffffffffu, bcta, o);
+                    if (om > best || (om == best && orow < brow)) {
+                        best = om;
+                        brow = orow;
+                        bcta = octa;
+                    }
+                }
+                if (lane == 0) {
+                    s_piv = brow;
+                    s_wcta = bcta;
+                }
             }
         }
         __syncthreads();
-        // Publish the candidate row, and row `col` if this CTA owns it.
-        {
-            const int brow_l = s_row[0] - r0;
-            if (s_row[0] != INT32_MAX && tid < w)
-                sc.cand_rows[((size_t)slot * G + cta) * kLeafW + tid] = loc[brow_l * ldl + tid];
-            if (col >= r0 && col < r0 + nloc && tid < w)
-                sc.col_rows[slot * kLeafW + tid] = loc[(col - r0) * ldl + tid];
-        }
-        if (!grid_barrier(sc.bar, (unsigned)j, (unsigned)G, sc.err, &s_flag)) return;
-
-        // Every CTA reduces the same candidates in the same order: same winner.
-        if (warp == 0) {
-            best = T(-1);
-            brow = INT32_MAX;
-            int bcta = -1;
-            for (int g = lane; g < G; g += 32) {
-                T m = sc.cand_mag[slot * G + g];
-                int rr = sc.cand_row[slot * G + g];
-                if (m > best || (m == best && rr < brow)) {
-                    best = m;
-                    brow = rr;
-                    bcta = g;
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                T om = __shfl_xor_sync(0xffffffffu, best, o);
-                int orow = __shfl_xor_sync(0xffffffffu, brow, o);
-                int octa = __shfl_xor_sync(0xffffffffu, bcta, o);
-                if (om > best || (om == best && orow < brow)) {
-                    best = om;
-                    brow = orow;
-                    bcta = octa;
-                }
-            }
-            if (lane == 0) {
-                s_piv = brow;
-                s_wcta = bcta;
-                s_wmag = best;
-            }
-        }
-        __syncthreads();
+        if (s_fail) return;
         // No positive magnitude anywhere: numax keeps row `col` as the pivot.
         const bool none = s_piv == INT32_MAX;
         const int piv = none ? col : s_piv;
-        if (tid < w)
-            prow[tid] = none ? sc.col_rows[slot * kLeafW + tid]
-                             : sc.cand_rows[((size_t)slot * G + s_wcta) * kLeafW + tid];
+        // Published data is read through L2 (__ldcg): the same addresses held
+        // the values of two columns ago.
+        for (int q = tid; q < w; q += kLeafThreads)
+            prow[q] = none ? __ldcg(&sc.col_rows[slot * kLeafMax + q])
+                           : __ldcg(&sc.cand_rows[((size_t)slot * G + s_wcta) * kLeafMax + q]);
         __syncthreads();
         if (piv != col) {
-            if (col >= r0 && col < r0 + nloc && tid < w) loc[(col - r0) * ldl + tid] = prow[tid];
-            if (piv >= r0 && piv < r0 + nloc && tid < w)
-                loc[(piv - r0) * ldl + tid] = sc.col_rows[slot * kLeafW + tid];
+            if (col >= r0 && col < r0 + nloc)
+                for (int q = tid; q < w; q += kLeafThreads) loc[(col - r0) * ldl + q] = prow[q];
+            if (piv >= r0 && piv < r0 + nloc)
+                for (int q = tid; q < w; q += kLeafThreads)
+                    loc[(piv - r0) * ldl + q] = __ldcg(&sc.col_rows[slot * kLeafMax + q]);
         }
         if (cta == 0 && tid == 0) {
             ipiv[col] = piv;
@@ -176,7 +219,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         for (int r = tid; r < nloc; r += kLeafThreads) {
             const int gr = r0 + r;
             if (gr <= col) continue;
-            T l = loc[r * ldl + j] / p;
+            const T l = loc[r * ldl + j] / p;
             loc[r * ldl + j] = l;
             for (int jj = j + 1; jj < w; ++jj) loc[r * ldl + jj] -= l * prow[jj];
         }
@@ -295,12 +338,11 @@ static int leaf(LuRun<T> &R, int c, int w) {
     G = std::max(G, 1);
     int rpc = (int)ceil_div(m, G);
     G = (int)ceil_div(m, rpc);
-    size_t smem = sizeof(T) * ((size_t)rpc * (kLeafW + 1) + kLeafW);
+    size_t smem = sizeof(T) * ((size_t)rpc * (w | 1) + kLeafMax);
     if (smem > R.ctx->smem_optin - 1024) {
         set_error("matrix order %d too large for the leaf panel (%zu B shared)", R.n, smem);
         return NMX_ERR_UNSUPPORTED;
     }
-    NMX_CUDA_TRY(cudaMemsetAsync(R.sc.bar, 0, sizeof(unsigned), R.st));
     void *args[] = {&R.A, &R.lda, &R.n, &c, &w, &rpc, &R.ipiv, &R.info, &R.sc};
     NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)getrf_leaf_kernel<T>, dim3(G),
                                              dim3(kLeafThreads), args, smem, R.st));
@@ -399,25 +441,25 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
     NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     if (n == 0) return 0;
     const int G = ctx->sm_count;
-    size_t bytes = sizeof(T) * (2 * (size_t)G * kLeafW + 2 * kLeafW + 2 * G) + sizeof(int) * 2 * G +
-                   64;
+    const size_t slot_bytes = sizeof(LeafSlot<T>) * 2 * (size_t)G;
+    size_t bytes = slot_bytes + sizeof(T) * (2 * (size_t)G * kLeafMax + 2 * kLeafMax) + 64;
     void *wsv = nullptr;
     int rc = ctx->ensure_slot(kWsLeaf, bytes, &wsv);
     if (rc) return rc;
     char *ws = static_cast<char *>(wsv);
     LeafScratch<T> sc;
-    sc.cand_rows = reinterpret_cast<T *>(ws);
-    sc.col_rows = sc.cand_rows + 2 * (size_t)G * kLeafW;
-    sc.cand_mag = sc.col_rows + 2 * kLeafW;
-    sc.cand_row = reinterpret_cast<int *>(sc.cand_mag + 2 * G);
-    sc.bar = reinterpret_cast<unsigned *>(sc.cand_row + 2 * G);
-    sc.err = reinterpret_cast<int *>(sc.bar + 1);
+    sc.slots = reinterpret_cast<LeafSlot<T> *>(ws);
+    sc.cand_rows = reinterpret_cast<T *>(ws + slot_bytes);
+    sc.col_rows = sc.cand_rows + 2 * (size_t)G * kLeafMax;
+    sc.err = reinterpret_cast<int *>(sc.col_rows + 2 * kLeafMax);
+    // Sequence numbers start below every column's (col + 1 >= 1).
+    NMX_CUDA_TRY(cudaMemsetAsync(sc.slots, 0, slot_bytes, st));
     NMX_CUDA_TRY(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
     // Every CTA of the cooperative leaf must be resident at once.
     int per_sm = 0;
     const int m = (int)n;
     int rpc_max = (int)ceil_div(m, std::min<int64_t>(G, ceil_div(m, 32)));
-    size_t smem = sizeof(T) * ((size_t)rpc_max * (kLeafW + 1) + kLeafW);
+    size_t smem = sizeof(T) * ((size_t)rpc_max * (kLeafW | 1) + kLeafMax);
     NMX_CUDA_TRY(cudaFuncSetAttribute(getrf_leaf_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)std::min<size_t>(smem, ctx->smem_optin - 1024)));

@@ -83,8 +83,8 @@ __global__ void __launch_bounds__(kQrThreads)
         if (own_col && tid == 0) sc.alpha[slot] = loc[(col - r0) * ldl + j];
         if (!grid_barrier(sc.bar, gen++, (unsigned)G, sc.err, &s_flag)) return;
         T below = T(0);
-        for (int g = 0; g < G; ++g) below += sc.part[((size_t)slot * G + g) * (kQrW + 1)];
-        const T alpha = sc.alpha[slot];
+        for (int g = 0; g < G; ++g) below += __ldcg(&sc.part[((size_t)slot * G + g) * (kQrW + 1)]);
+        const T alpha = __ldcg(&sc.alpha[slot]);
         T this_tau = T(0), scale = T(0), beta = alpha;
         const bool reflect = below != T(0);
         if (reflect) {
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kQrThreads)
         if (!grid_barrier(sc.bar, gen++, (unsigned)G, sc.err, &s_flag)) return;
         if (tid < w && tid > j) {
             T d = T(0);
-            for (int g = 0; g < G; ++g) d += sc.part[((size_t)slot * G + g) * (kQrW + 1) + tid];
+            for (int g = 0; g < G; ++g) d += __ldcg(&sc.part[((size_t)slot * G + g) * (kQrW + 1) + tid]);
             s_fac[tid] = this_tau * d;
         }
         __syncthreads();

@@ -74,7 +74,7 @@ struct nmx_context {
 };
 
 namespace nmx {
-enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4 };
+enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5 };
 }
 
 namespace nmx {
