@@ -63,6 +63,11 @@ NMX_API int nmx_destroy(nmx_ctx ctx);
 NMX_API const char *nmx_last_error_string(void);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
 NMX_API int nmx_version(void);
+/* Per-context tuning knobs, the hook the autotuner writes (0 = automatic):
+ *   "lu.leaf_ctas"  CTAs of the cooperative LU leaf panel
+ *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop */
+NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
+NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
 
 /* ---- batched uneven-size Cholesky + cho_solve ---------------------------
  *

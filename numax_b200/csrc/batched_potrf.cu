@@ -73,6 +73,22 @@ __device__ __forceinline__ int prow_off(int i, int n) {
     return i < n ? (i * (i + 1)) / 2 : (n * (n + 1)) / 2 + (i - n) * n;
 }
 
+// 1/sqrt(g) for g > 0 in float64: a float32 hardware seed refined by two
+// Newton-Raphson steps r <- r (3 - g r^2) / 2 (the classical iteration for the
+// reciprocal square root; each step squares the relative error, so 1e-7
+// becomes < 1e-28).  Outside float32's normal range, or for g <= 0 / NaN, the
+// library rsqrt is used (and gives NaN for negative g, as numax's sqrt of a
+// guarded negative pivot does).
+__device__ __forceinline__ double rsqrt_nr(double g) {
+    if (!(g > 1e-36 && g < 1e36)) return rsqrt(g);
+    double r = (double)rsqrtf((float)g);
+    const double h = 0.5 * g;
+    r = r * (1.5 - h * r * r);
+    r = r * (1.5 - h * r * r);
+    return r;
+}
+__device__ __forceinline__ float rsqrt_nr(float g) { return rsqrtf(g); }
+
 // One warp factors the kb x kb diagonal block at (k, k) in registers (lane i
 // holds row i) with numax's Array-tier rule l_jj = sqrt(guard_nonzero(d,
 // 1e-30)) (a negative d gives NaN; info records the first d <= 0), writes
@@ -100,10 +116,10 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
             const T d = __shfl_sync(0xffffffffu, a[j], j);
             if (!bad && d <= T(0)) bad = k + j + 1;
             const T g = guard_nonzero(d, floor_);
-            const T inv = rsqrt(g);
+            const T inv = rsqrt_nr(g);  // 1 / l_jj, also W's diagonal entry
             if (lane == j) {
                 a[j] = g * inv;
-                myinv = T(1) / guard_nonzero(a[j], floor_);
+                myinv = inv;
             }
             if (lane > j) a[j] *= inv;
             const T lij = a[j];

@@ -133,50 +133,54 @@ __device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float
             group_sync<G>();
             // 2x2 blocks: rows of pair kr, columns of pair kc.  The rotations
             // were formed in float64; they are applied to the float32 data in
-            // float32.
-            for (int e = gt; e < half * half; e += G) {
-                const int kr = e / half, kc = e - kr * half;
-                const int p = pq[2 * kr], q = pq[2 * kr + 1];
-                const int u = pq[2 * kc], v = pq[2 * kc + 1];
-                if (q >= n && v >= n) continue;
-                const float cr = (float)cs[2 * kr], sr = (float)cs[2 * kr + 1];
-                const float cc = (float)cs[2 * kc], sc = (float)cs[2 * kc + 1];
-                if (q < n && v < n) {
-                    const float b00 = As[p * ld + u], b01 = As[p * ld + v];
-                    const float b10 = As[q * ld + u], b11 = As[q * ld + v];
-                    // rows: [c -s; s c] applied from the left
-                    const float r00 = cr * b00 - sr * b10, r01 = cr * b01 - sr * b11;
-                    const float r10 = sr * b00 + cr * b10, r11 = sr * b01 + cr * b11;
-                    // columns: [c s; -s c] applied from the right
-                    float o00 = cc * r00 - sc * r01, o01 = sc * r00 + cc * r01;
-                    float o10 = cc * r10 - sc * r11, o11 = sc * r10 + cc * r11;
-                    if (kr == kc) {
-                        o01 = 0.f;  // the annihilated pair
-                        o10 = 0.f;
+            // float32.  Lane = column pair (half <= 32), warp = row pairs.
+            {
+                constexpr int NWG = G / 32;
+                const int lane = gt & 31, wg = gt >> 5;
+                const int kc = lane;
+                const bool colok = kc < half;
+                const int u = colok ? pq[2 * kc] : 0, v = colok ? pq[2 * kc + 1] : 0;
+                const float cc = colok ? (float)cs[2 * kc] : 1.f;
+                const float sc = colok ? (float)cs[2 * kc + 1] : 0.f;
+                for (int kr = wg; kr < half; kr += NWG) {
+                    if (!colok) continue;
+                    const int p = pq[2 * kr], q = pq[2 * kr + 1];
+                    if (q >= n && v >= n) continue;
+                    const float cr = (float)cs[2 * kr], sr = (float)cs[2 * kr + 1];
+                    if (q < n && v < n) {
+                        const float b00 = As[p * ld + u], b01 = As[p * ld + v];
+                        const float b10 = As[q * ld + u], b11 = As[q * ld + v];
+                        // rows: [c -s; s c] applied from the left
+                        const float r00 = cr * b00 - sr * b10, r01 = cr * b01 - sr * b11;
+                        const float r10 = sr * b00 + cr * b10, r11 = sr * b01 + cr * b11;
+                        // columns: [c s; -s c] applied from the right
+                        float o00 = cc * r00 - sc * r01, o01 = sc * r00 + cc * r01;
+                        float o10 = cc * r10 - sc * r11, o11 = sc * r10 + cc * r11;
+                        if (kr == kc) {
+                            o01 = 0.f;  // the annihilated pair
+                            o10 = 0.f;
+                        }
+                        As[p * ld + u] = o00;
+                        As[p * ld + v] = o01;
+                        As[q * ld + u] = o10;
+                        As[q * ld + v] = o11;
+                    } else if (q < n) {  // column pair has the dummy index
+                        const float b0 = As[p * ld + u], b1 = As[q * ld + u];
+                        As[p * ld + u] = cr * b0 - sr * b1;
+                        As[q * ld + u] = sr * b0 + cr * b1;
+                    } else {  // row pair has the dummy index
+                        const float b0 = As[p * ld + u], b1 = As[p * ld + v];
+                        As[p * ld + u] = cc * b0 - sc * b1;
+                        As[p * ld + v] = sc * b0 + cc * b1;
                     }
-                    As[p * ld + u] = o00;
-                    As[p * ld + v] = o01;
-                    As[q * ld + u] = o10;
-                    As[q * ld + v] = o11;
-                } else if (q < n) {  // column pair has the dummy index: only column u exists
-                    const float b0 = As[p * ld + u], b1 = As[q * ld + u];
-                    As[p * ld + u] = cr * b0 - sr * b1;
-                    As[q * ld + u] = sr * b0 + cr * b1;
-                } else {  // row pair has the dummy index: only row p exists
-                    const float b0 = As[p * ld + u], b1 = As[p * ld + v];
-                    As[p * ld + u] = cc * b0 - sc * b1;
-                    As[p * ld + v] = sc * b0 + cc * b1;
                 }
-            }
-            // V := V J, columns of every pair.
-            for (int e = gt; e < n * half; e += G) {
-                const int i = e / half, k = e - i * half;
-                const int p = pq[2 * k], q = pq[2 * k + 1];
-                if (q >= n) continue;
-                const float c = (float)cs[2 * k], s = (float)cs[2 * k + 1];
-                const float vp = Vs[i * ld + p], vq = Vs[i * ld + q];
-                Vs[i * ld + p] = c * vp - s * vq;
-                Vs[i * ld + q] = s * vp + c * vq;
+                // V := V J: warp = rows of V, lane = column pair.
+                if (colok && v < n)
+                    for (int i = wg; i < n; i += NWG) {
+                        const float vp = Vs[i * ld + u], vq = Vs[i * ld + v];
+                        Vs[i * ld + u] = cc * vp - sc * vq;
+                        Vs[i * ld + v] = sc * vp + cc * vq;
+                    }
             }
             group_sync<G>();
         }

@@ -111,6 +111,32 @@ int nmx_create(int device, nmx_ctx *out) {
     return 0;
 }
 
+// Tuning knobs.  Keys: "lu.leaf_ctas", "ir.trsv_ctas" (0 = automatic).
+static int64_t *tune_slot(nmx_ctx ctx, const char *key) {
+    if (!key) return nullptr;
+    if (!std::strcmp(key, "lu.leaf_ctas")) return &ctx->tune_lu_leaf_ctas;
+    if (!std::strcmp(key, "ir.trsv_ctas")) return &ctx->tune_ir_trsv_ctas;
+    return nullptr;
+}
+
+int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    int64_t *slot = tune_slot(ctx, key);
+    NMX_ARG_CHECK(slot != nullptr, 2, "unknown tuning key");
+    NMX_ARG_CHECK(value >= 0, 3, "value must be >= 0");
+    *slot = value;
+    return 0;
+}
+
+int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    int64_t *slot = tune_slot(ctx, key);
+    NMX_ARG_CHECK(slot != nullptr, 2, "unknown tuning key");
+    NMX_ARG_CHECK(value != nullptr, 3, "value is NULL");
+    *value = *slot;
+    return 0;
+}
+
 int nmx_destroy(nmx_ctx ctx) {
     if (!ctx) return 0;
     {

@@ -455,10 +455,13 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
     // Sequence numbers start below every column's (col + 1 >= 1).
     NMX_CUDA_TRY(cudaMemsetAsync(sc.slots, 0, slot_bytes, st));
     NMX_CUDA_TRY(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    const int leaf_ctas = ctx->tune_lu_leaf_ctas > 0
+                              ? (int)std::min<int64_t>(ctx->tune_lu_leaf_ctas, G)
+                              : G;
     // Every CTA of the cooperative leaf must be resident at once.
     int per_sm = 0;
     const int m = (int)n;
-    int rpc_max = (int)ceil_div(m, std::min<int64_t>(G, ceil_div(m, 32)));
+    int rpc_max = (int)ceil_div(m, std::min<int64_t>(leaf_ctas, ceil_div(m, 32)));
     size_t smem = sizeof(T) * ((size_t)rpc_max * (kLeafW | 1) + kLeafMax);
     NMX_CUDA_TRY(cudaFuncSetAttribute(getrf_leaf_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -469,7 +472,7 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
         set_error("matrix order %lld too large for the leaf panel", (long long)n);
         return NMX_ERR_UNSUPPORTED;
     }
-    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, G};
+    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas};
     return getrf2<T>(R, 0, (int)n);
 }
 

@@ -330,7 +330,9 @@ static double bits_to_double(unsigned long long u) {
 // v := U^-1 L^-1 v (the FP32 factors in W, arithmetic in FP64).
 static int lu_solve_inplace(IrRun &R, double *v) {
     const int NB = (R.n + kTrsvRB - 1) / kTrsvRB;
-    const int grid = std::min(NB, 2 * R.ctx->sm_count);
+    const int want = R.ctx->tune_ir_trsv_ctas > 0 ? (int)R.ctx->tune_ir_trsv_ctas
+                                                  : 2 * R.ctx->sm_count;
+    const int grid = std::max(1, std::min(NB, want));
     NMX_CUDA_TRY(cudaMemsetAsync(R.counters, 0, 6 * sizeof(int), R.st));
     trsv_f32f64_kernel<false><<<grid, kTrsvThreads, 0, R.st>>>(R.W, R.ldw, R.n, R.invL, v,
                                                                R.counters);

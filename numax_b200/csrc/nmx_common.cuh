@@ -63,6 +63,9 @@ struct nmx_context {
     void *workspace = nullptr;
     size_t workspace_bytes = 0;
     void *cublas = nullptr;  // cublasHandle_t, created on first dense call
+    // Tuning knobs (nmx_tune_set / nmx_tune_get); 0 means "automatic".
+    int64_t tune_lu_leaf_ctas = 0;    // CTAs of the cooperative LU leaf panel
+    int64_t tune_ir_trsv_ctas = 0;    // CTAs of the persistent triangular solves
     // Grow-only named device buffers, one per use, kept for the context's life.
     static constexpr int kSlots = 8;
     void *slot_ptr[kSlots] = {};
