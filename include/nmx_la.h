@@ -65,6 +65,8 @@ NMX_API const char *nmx_last_error_string(void);
 NMX_API int nmx_version(void);
 /* Per-context tuning knobs, the hook the autotuner writes (0 = automatic):
  *   "lu.leaf_ctas"  CTAs of the cooperative LU leaf panel
+ *   "lu.cluster"    cap on the CTAs of the cluster LU leaf (-1 = no cap,
+ *                   0 = never use the cluster leaf)
  *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
 NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);

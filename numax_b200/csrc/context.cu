@@ -116,6 +116,7 @@ static int64_t *tune_slot(nmx_ctx ctx, const char *key) {
     if (!key) return nullptr;
     if (!std::strcmp(key, "lu.leaf_ctas")) return &ctx->tune_lu_leaf_ctas;
     if (!std::strcmp(key, "ir.trsv_ctas")) return &ctx->tune_ir_trsv_ctas;
+    if (!std::strcmp(key, "lu.cluster")) return &ctx->tune_lu_cluster;
     return nullptr;
 }
 
@@ -123,7 +124,7 @@ int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value) {
     NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
     int64_t *slot = tune_slot(ctx, key);
     NMX_ARG_CHECK(slot != nullptr, 2, "unknown tuning key");
-    NMX_ARG_CHECK(value >= 0, 3, "value must be >= 0");
+    NMX_ARG_CHECK(value >= -1, 3, "value must be >= -1");
     *slot = value;
     return 0;
 }

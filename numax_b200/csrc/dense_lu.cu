@@ -231,6 +231,168 @@ __global__ void __launch_bounds__(kLeafThreads)
     }
 }
 
+// Cluster leaf: the same panel factorization on one thread-block cluster
+// (up to 16 CTAs, one per SM) whose shared memories together hold the whole
+// panel.  The per-column exchange runs over distributed shared memory: each
+// CTA leaves its candidate (|a|, row, the row's panel values) and, from the
+// owner, row `col` in its own shared memory, one hardware cluster barrier,
+// then every CTA reads the others' candidates and the winning row directly
+// from their shared memory.  No global-memory round trip per column.
+constexpr int kClusterLeafThreads = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(kClusterLeafThreads)
+    getrf_cluster_leaf_kernel(T *A, int64_t lda, int n, int c, int w, int rows_per_cta,
+                              int32_t *ipiv, int32_t *info) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ldl = w | 1;
+    T *loc = reinterpret_cast<T *>(smem_raw);                 // rows_per_cta x ldl
+    T *xch = loc + (size_t)rows_per_cta * ldl;                 // [2][3][kLeafMax]
+    // xch[slot][0] = candidate row, xch[slot][1] = row `col`, xch[slot][2] = pivot row
+    __shared__ T s_cmag[2];
+    __shared__ int s_crow[2];
+    __shared__ T s_mag[kClusterLeafThreads / 32];
+    __shared__ int s_row[kClusterLeafThreads / 32];
+    __shared__ int s_piv, s_wcta;
+
+    const int CS = (int)cluster.num_blocks(), cta = (int)cluster.block_rank();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kClusterLeafThreads / 32;
+    const int r0 = c + cta * rows_per_cta;
+    const int nloc = max(0, min(rows_per_cta, n - r0));
+    const int col_owner = 0;  // row `col` is always within CTA (col - c) / rows_per_cta
+    (void)col_owner;
+
+    for (int e = tid; e < nloc * w; e += kClusterLeafThreads) {
+        const int r = e / w, j = e - r * w;
+        loc[r * ldl + j] = A[(int64_t)(r0 + r) * lda + c + j];
+    }
+    __syncthreads();
+
+    for (int j = 0; j < w; ++j) {
+        const int col = c + j;
+        const int slot = j & 1;
+        T *myx = xch + (size_t)slot * 3 * kLeafMax;
+        T best = T(-1);
+        int brow = INT32_MAX;
+        for (int r = tid; r < nloc; r += kClusterLeafThreads) {
+            const int gr = r0 + r;
+            if (gr < col) continue;
+            const T m = fabs(loc[r * ldl + j]);
+            if (!(m > T(0))) continue;
+            if (m > best || (m == best && gr < brow)) {
+                best = m;
+                brow = gr;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const T om = __shfl_xor_sync(0xffffffffu, best, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            if (om > best || (om == best && orow < brow)) {
+                best = om;
+                brow = orow;
+            }
+        }
+        if (lane == 0) {
+            s_mag[warp] = best;
+            s_row[warp] = brow;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            best = lane < NW ? s_mag[lane] : T(-1);
+            brow = lane < NW ? s_row[lane] : INT32_MAX;
+            for (int o = 16; o > 0; o >>= 1) {
+                const T om = __shfl_xor_sync(0xffffffffu, best, o);
+                const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                if (om > best || (om == best && orow < brow)) {
+                    best = om;
+                    brow = orow;
+                }
+            }
+            if (lane == 0) {
+                s_cmag[slot] = best;
+                s_crow[slot] = brow;
+            }
+            if (brow != INT32_MAX)
+                for (int q = lane; q < w; q += 32) myx[q] = loc[(brow - r0) * ldl + q];
+            if (col >= r0 && col < r0 + nloc)
+                for (int q = lane; q < w; q += 32) myx[kLeafMax + q] = loc[(col - r0) * ldl + q];
+        }
+        cluster.sync();  // candidates and row `col` visible cluster-wide
+        if (warp == 0) {
+            best = T(-1);
+            brow = INT32_MAX;
+            int bcta = -1;
+            if (lane < CS) {
+                const T *rm = cluster.map_shared_rank(&s_cmag[slot], lane);
+                const int *rr = cluster.map_shared_rank(&s_crow[slot], lane);
+                best = *rm;
+                brow = *rr;
+                bcta = lane;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const T om = __shfl_xor_sync(0xffffffffu, best, o);
+                const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                const int octa = __shfl_xor_sync(0xffffffffu, bcta, o);
+                if (om > best || (om == best && orow < brow)) {
+                    best = om;
+                    brow = orow;
+                    bcta = octa;
+                }
+            }
+            if (lane == 0) {
+                s_piv = brow;
+                s_wcta = bcta;
+            }
+        }
+        __syncthreads();
+        const bool none = s_piv == INT32_MAX;
+        const int piv = none ? col : s_piv;
+        const int col_cta = (col - c) / rows_per_cta;
+        T *prow = myx + 2 * kLeafMax;
+        if (tid < w) {
+            const T *src = none ? cluster.map_shared_rank(xch + (size_t)slot * 3 * kLeafMax + kLeafMax,
+                                                          col_cta)
+                                : cluster.map_shared_rank(xch + (size_t)slot * 3 * kLeafMax, s_wcta);
+            prow[tid] = src[tid];
+        }
+        __syncthreads();
+        if (piv != col) {
+            if (col >= r0 && col < r0 + nloc)
+                for (int q = tid; q < w; q += kClusterLeafThreads) loc[(col - r0) * ldl + q] = prow[q];
+            if (piv >= r0 && piv < r0 + nloc) {
+                const T *oldcol =
+                    cluster.map_shared_rank(xch + (size_t)slot * 3 * kLeafMax + kLeafMax, col_cta);
+                for (int q = tid; q < w; q += kClusterLeafThreads)
+                    loc[(piv - r0) * ldl + q] = oldcol[q];
+            }
+        }
+        if (cta == 0 && tid == 0) {
+            ipiv[col] = piv;
+            if (none && *info == 0) *info = col + 1;
+        }
+        __syncthreads();
+        T p = prow[j];
+        if (p == T(0)) p = pivot_floor<T>::value;
+        for (int r = tid; r < nloc; r += kClusterLeafThreads) {
+            const int gr = r0 + r;
+            if (gr <= col) continue;
+            const T l = loc[r * ldl + j] / p;
+            loc[r * ldl + j] = l;
+            for (int jj = j + 1; jj < w; ++jj) loc[r * ldl + jj] -= l * prow[jj];
+        }
+        __syncthreads();
+    }
+    // No CTA may leave while others can still read its shared memory.
+    cluster.sync();
+    for (int e = tid; e < nloc * w; e += kClusterLeafThreads) {
+        const int r = e / w, j = e - r * w;
+        A[(int64_t)(r0 + r) * lda + c + j] = loc[r * ldl + j];
+    }
+}
+
 // Apply interchanges ipiv[c..c+w) to the columns outside [c, c+w) of rows of
 // A (ncols wide).  One thread per column, swaps in order.
 template <typename T>
@@ -329,11 +491,51 @@ struct LuRun {
     int32_t *info;
     LeafScratch<T> sc;
     int max_ctas;
+    int cluster;  // CTAs per cluster for the cluster leaf (0: not available)
 };
+
+// Shared-memory bytes the cluster leaf needs for an m-row panel of width w.
+template <typename T>
+static size_t cluster_leaf_smem(int m, int w, int cs) {
+    const size_t rpc = (size_t)ceil_div(m, cs);
+    return sizeof(T) * (rpc * (size_t)(w | 1) + 6 * (size_t)kLeafMax);
+}
+
+// Widest leaf (multiple of 8, <= kLeafW) the cluster leaf can hold for an
+// m-row panel; 0 if even 8 columns do not fit (the cooperative leaf runs).
+template <typename T>
+static int leaf_width(const LuRun<T> &R, int m) {
+    if (R.cluster <= 0) return kLeafW;
+    for (int w = kLeafW; w >= 8; w -= 8)
+        if (cluster_leaf_smem<T>(m, w, R.cluster) + 2048 <= R.ctx->smem_optin) return w;
+    return kLeafW;
+}
 
 template <typename T>
 static int leaf(LuRun<T> &R, int c, int w) {
     const int m = R.n - c;
+    const int threads = 256;
+    if (R.cluster > 0 && cluster_leaf_smem<T>(m, w, R.cluster) + 2048 <= R.ctx->smem_optin) {
+        int rpc = (int)ceil_div(m, R.cluster);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(R.cluster);
+        cfg.blockDim = dim3(kClusterLeafThreads);
+        cfg.dynamicSmemBytes = cluster_leaf_smem<T>(m, w, R.cluster);
+        cfg.stream = R.st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = R.cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        NMX_CUDA_TRY(cudaLaunchKernelEx(&cfg, getrf_cluster_leaf_kernel<T>, R.A, R.lda, R.n, c, w,
+                                        rpc, R.ipiv, R.info));
+        laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(
+            R.A, R.lda, R.n, c, w, R.ipiv, c, c + w);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     int G = (int)std::min<int64_t>(R.max_ctas, ceil_div(m, 32));
     G = std::max(G, 1);
     int rpc = (int)ceil_div(m, G);
@@ -347,7 +549,6 @@ static int leaf(LuRun<T> &R, int c, int w) {
     NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)getrf_leaf_kernel<T>, dim3(G),
                                              dim3(kLeafThreads), args, smem, R.st));
     // The interchanges across the rest of the width.
-    int threads = 256;
     laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(R.A, R.lda, R.n, c, w,
                                                                              R.ipiv, c, c + w);
     NMX_CUDA_TRY(cudaGetLastError());
@@ -419,8 +620,11 @@ int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
 
 template <typename T>
 static int getrf2(LuRun<T> &R, int c, int w) {
-    if (w <= kLeafW) return leaf<T>(R, c, w);
-    int hw = (w / 2 + kLeafW - 1) / kLeafW * kLeafW;
+    const int lw = leaf_width<T>(R, R.n - c);
+    if (w <= lw) return leaf<T>(R, c, w);
+    // Split on multiples of the leaf width (a multiple of 8, which keeps every
+    // block offset 16-byte aligned for the tensor-core update).
+    int hw = std::min(w - 1, (w / 2 + lw - 1) / lw * lw);
     int rc = getrf2<T>(R, c, hw);
     if (rc) return rc;
     // U12 := L11^-1 A12 over the right half's columns.
@@ -472,7 +676,56 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
         set_error("matrix order %lld too large for the leaf panel", (long long)n);
         return NMX_ERR_UNSUPPORTED;
     }
-    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas};
+    // Thread-block cluster for the cluster leaf: 16 CTAs (non-portable) when
+    // the device can co-schedule them, else 8, else none.
+    int cluster = 0;
+    {
+        auto kern = getrf_cluster_leaf_kernel<T>;
+        const size_t smax = ctx->smem_optin - 2048;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) ==
+            cudaSuccess) {
+            for (int cs : {16, 8}) {
+                if (cs > 8 &&
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                        cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(cs);
+                cfg.blockDim = dim3(kClusterLeafThreads);
+                cfg.dynamicSmemBytes = smax;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = cs;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                int clusters = 0;
+                if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) == cudaSuccess &&
+                    clusters >= 1) {
+                    cluster = cs;
+                    break;
+                }
+                cudaGetLastError();
+            }
+        } else {
+            cudaGetLastError();
+        }
+    }
+    // A tuned cluster size is rounded down to a power of two no larger than
+    // the one the device can co-schedule; 0 selects the cooperative leaf.
+    if (ctx->tune_lu_cluster >= 0) {
+        int cs = 0;
+        for (int p = 16; p >= 1; p /= 2)
+            if (p <= cluster && p <= ctx->tune_lu_cluster) {
+                cs = p;
+                break;
+            }
+        cluster = cs;
+    }
+    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas, cluster};
     return getrf2<T>(R, 0, (int)n);
 }
 

@@ -135,3 +135,29 @@ def test_lu_leading_dimension_and_argument_errors():
                                   np.random.Generator(np.random.PCG64(5)).standard_normal((n, n + 9))[:, n:])
     assert lib.nmx_getrf_f64(ctx, 4, None, 4, None, None, None) == -3
     assert lib.nmx_getrf_f64(ctx, 4, big.data_ptr(), 3, None, None, None) == -4
+
+
+@pytest.mark.parametrize("cluster", [0, 2, -1])
+def test_lu_leaf_paths_match_lapack(cluster):
+    """The panel leaf runs as a thread-block cluster exchanging candidates
+    through distributed shared memory, or as a cooperative grid exchanging
+    through global memory ("lu.cluster" = 0).  A 2-CTA cluster holds only
+    part of a 4000-row panel, which narrows the leaves to 8 and 16 columns
+    near the top and leaves the tallest panels to the cooperative kernel, so
+    every leaf form runs here; all must give LAPACK's pivots."""
+    import scipy.linalg as sl
+    from numax_b200 import _lib, linalg
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    n = 4000
+    rng = np.random.Generator(np.random.PCG64(4000))
+    a = rng.standard_normal((n, n))
+    lib.nmx_tune_set(ctx, b"lu.cluster", cluster)
+    try:
+        f = linalg.lu_factor(torch.from_numpy(a).cuda())
+    finally:
+        lib.nmx_tune_set(ctx, b"lu.cluster", -1)
+    lu, piv = sl.lu_factor(a)
+    np.testing.assert_array_equal(f.pivots.cpu().numpy(), piv)
+    assert f.info == 0
+    assert rel(f.factored.cpu().numpy(), lu) <= 1e-12
