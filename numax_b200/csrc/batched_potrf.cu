@@ -36,6 +36,9 @@ namespace nmx {
 constexpr int kPotrfMaxN = 128;
 constexpr int kPotrfMaxRhs = 8;
 constexpr int kDiagNB = 16;
+constexpr int kPotrfStage = kDiagNB * kPotrfMaxRhs > kDiagNB * (kDiagNB + 1) / 2
+                                ? kDiagNB * kPotrfMaxRhs
+                                : kDiagNB * (kDiagNB + 1) / 2;
 
 struct BatchedPotrfArgs {
     const int32_t *order;  // matrix indices, bucket-contiguous, largest first
@@ -52,11 +55,12 @@ struct BatchedPotrfArgs {
 
 // Shared-memory words (of T) one CTA needs for matrices up to nmax: the
 // packed lower triangle (row i at i(i+1)/2), nrhs full rows of B^T below it,
-// and a 16 x nrhs staging block for the back solve.  The inverse of each
+// and a staging area: a 16 x nrhs block in the back solve, before that the
+// packed 16 x 16 diagonal block of L on its way to global memory.  The inverse of each
 // 16x16 diagonal block is kept in place of that block once the block of L
 // has been written out.
 __host__ __device__ inline int potrf_smem_elems(int nmax, int nrhs) {
-    return nmax * (nmax + 1) / 2 + nrhs * nmax + kDiagNB * kPotrfMaxRhs + 2;
+    return nmax * (nmax + 1) / 2 + nrhs * nmax + kPotrfStage + 2;
 }
 
 // Row of packed lower-triangle index e (e = i(i+1)/2 + j, 0 <= j <= i).
@@ -73,92 +77,92 @@ __device__ __forceinline__ int prow_off(int i, int n) {
     return i < n ? (i * (i + 1)) / 2 : (n * (n + 1)) / 2 + (i - n) * n;
 }
 
-// 1/sqrt(g) for g > 0 in float64: a float32 hardware seed refined by two
-// Newton-Raphson steps r <- r (3 - g r^2) / 2 (the classical iteration for the
-// reciprocal square root; each step squares the relative error, so 1e-7
-// becomes < 1e-28).  Outside float32's normal range, or for g <= 0 / NaN, the
-// library rsqrt is used (and gives NaN for negative g, as numax's sqrt of a
-// guarded negative pivot does).
-__device__ __forceinline__ double rsqrt_nr(double g) {
-    if (!(g > 1e-36 && g < 1e36)) return rsqrt(g);
-    double r = (double)rsqrtf((float)g);
-    const double h = 0.5 * g;
-    r = r * (1.5 - h * r * r);
-    r = r * (1.5 - h * r * r);
-    return r;
-}
-__device__ __forceinline__ float rsqrt_nr(float g) { return rsqrtf(g); }
+// 1/sqrt(g) from CUDA's rsqrt (faster on this chain, measured, than a
+// float32 seed refined by Newton steps in float64).  A negative g gives NaN,
+// as numax's sqrt of a guarded negative pivot does.
+__device__ __forceinline__ double inv_sqrt(double g) { return rsqrt(g); }
+__device__ __forceinline__ float inv_sqrt(float g) { return rsqrtf(g); }
 
 // One warp factors the kb x kb diagonal block at (k, k) in registers (lane i
 // holds row i) with numax's Array-tier rule l_jj = sqrt(guard_nonzero(d,
-// 1e-30)) (a negative d gives NaN; info records the first d <= 0), writes
-// the block of L to global memory, then replaces it in shared memory by
-// W = L_kk^-1 (lower, W[i][i] = 1/l_ii), formed by a right-looking
-// substitution with lane j holding column j.
+// 1e-30)) (a negative d gives NaN; info records the first d <= 0), and builds
+// W = L_kk^-1 (lower, W[i][i] = 1/l_ii) in the same loop by the product form
+// W = L_kb-1^-1 ... L_0^-1, where L_j is the identity with column j of L:
+// step j scales row j of W by 1/l_jj and subtracts l_ij times it from each
+// row i > j.  W then replaces the block in shared memory.
+//
+// The pivot chain per column is shfl(d_j) -> 1/sqrt -> l_{j+1,j} -> d_{j+1}:
+// each row's diagonal entry is kept in a scalar so that the next pivot does
+// not wait on the broadcast of the column.  Columns of L go to a packed
+// staging triangle in shared memory (row i at i(i+1)/2: the 16 row offsets
+// are distinct modulo 16, so a column store is conflict-free) and leave for
+// global memory as whole rows at the end.
 template <typename T>
-__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *Lg, int lane,
-                                                 int *s_info) {
+__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *Lg, T *Lst,
+                                                 int lane, int *s_info) {
     const T floor_ = pivot_floor<T>::value;
     // Every index into a[] and w[] below is a compile-time constant (the
     // loops are unrolled), so both stay in registers.
-    T a[kDiagNB];
-    int ro[kDiagNB];
-#pragma unroll
-    for (int i = 0; i < kDiagNB; ++i) ro[i] = prow_off(k + min(i, kb - 1), n) + k;
+    T a[kDiagNB];  // strictly lower part of row `lane`
+    T w[kDiagNB];  // row `lane` of W
+    const bool act = lane < kb;
     const int myro = prow_off(k + min(lane, kb - 1), n) + k;
 #pragma unroll
-    for (int c = 0; c < kDiagNB; ++c) a[c] = (lane < kb && c <= lane) ? S[myro + c] : T(0);
-    T myinv = T(0);
+    for (int c = 0; c < kDiagNB; ++c) a[c] = (act && c < lane) ? S[myro + c] : T(0);
+    T dg = act ? S[myro + min(lane, kDiagNB - 1)] : T(1);
+#pragma unroll
+    for (int c = 0; c < kDiagNB; ++c) w[c] = (c == lane) ? T(1) : T(0);
+    T *lst = Lst + (lane * (lane + 1)) / 2;  // staging row `lane` (used by lanes < kb)
     int bad = 0;
 #pragma unroll
     for (int j = 0; j < kDiagNB; ++j) {
         if (j < kb) {  // warp-uniform
-            const T d = __shfl_sync(0xffffffffu, a[j], j);
+            const T d = __shfl_sync(0xffffffffu, dg, j);
             if (!bad && d <= T(0)) bad = k + j + 1;
             const T g = guard_nonzero(d, floor_);
-            const T inv = rsqrt_nr(g);  // 1 / l_jj, also W's diagonal entry
+            const T inv = inv_sqrt(g);  // 1 / l_jj, also W's diagonal entry
+            T lij = T(0);
             if (lane == j) {
-                a[j] = g * inv;
-                myinv = inv;
+                dg = g * inv;
+                lst[j] = dg;
             }
-            if (lane > j) a[j] *= inv;
-            const T lij = a[j];
+            if (lane > j) {
+                lij = a[j] * inv;
+                dg -= lij * lij;
+                if (act) lst[j] = lij;
+            }
 #pragma unroll
             for (int c = j + 1; c < kDiagNB; ++c) {
+                // Entries at or above a lane's diagonal are never read, so
+                // this runs unpredicated (lij is 0 on lanes <= j); a
+                // predicate on `lane > c` makes the compiler index a[] at
+                // run time.
                 const T lcj = __shfl_sync(0xffffffffu, lij, c);
-                if (lane > j && c <= lane) a[c] -= lij * lcj;
+                a[c] -= lij * lcj;
+            }
+            if (lane == j) {
+#pragma unroll
+                for (int c = 0; c <= j; ++c) w[c] *= inv;
+            }
+#pragma unroll
+            for (int c = 0; c <= j; ++c) {
+                const T wjc = __shfl_sync(0xffffffffu, w[c], j);
+                if (lane > j) w[c] -= lij * wjc;
             }
         }
     }
     if (lane == 0 && bad && *s_info == 0) *s_info = bad;
-    if (lane < kb) {
-        T *lrow = Lg + (int64_t)(k + lane) * n + k;
+    if (act) {
 #pragma unroll
         for (int c = 0; c < kDiagNB; ++c)
-            if (c <= lane) {
-                S[myro + c] = a[c];
-                lrow[c] = a[c];
-            }
+            if (c <= lane) S[myro + c] = w[c];
     }
     __syncwarp();
-    // Column `lane` of W: w = L^-1 e_lane, right-looking over the rows of L.
-    T w[kDiagNB];
+    // Two rows of the block per warp-wide store.
 #pragma unroll
-    for (int i = 0; i < kDiagNB; ++i) w[i] = (i == lane) ? T(1) : T(0);
-#pragma unroll
-    for (int p = 0; p < kDiagNB; ++p) {
-        if (p < kb) {
-            w[p] *= __shfl_sync(0xffffffffu, myinv, p);
-#pragma unroll
-            for (int i = p + 1; i < kDiagNB; ++i)
-                if (i < kb) w[i] -= S[ro[i] + p] * w[p];
-        }
-    }
-    __syncwarp();
-    if (lane < kb) {
-#pragma unroll
-        for (int i = 0; i < kDiagNB; ++i)
-            if (i >= lane && i < kb) S[ro[i] + lane] = w[i];
+    for (int e = lane; e < kDiagNB * kDiagNB; e += 32) {
+        const int r = e >> 4, c = e & 15;
+        if (r < kb && c <= r) Lg[(int64_t)(k + r) * n + k + c] = Lst[(r * (r + 1)) / 2 + c];
     }
     __syncwarp();
 }
@@ -389,7 +393,7 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
 
     for (int k = 0; k < n; k += kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        if (warp == 0) potrf_diag_block<T>(S, n, k, kb, L, lane, s_info);
+        if (warp == 0) potrf_diag_block<T>(S, n, k, kb, L, xb, lane, s_info);
         __syncthreads();
 
         // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T, W
