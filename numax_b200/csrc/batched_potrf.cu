@@ -97,9 +97,14 @@ __device__ __forceinline__ float inv_sqrt(float g) { return rsqrtf(g); }
 // staging triangle in shared memory (row i at i(i+1)/2: the 16 row offsets
 // are distinct modulo 16, so a column store is conflict-free) and leave for
 // global memory as whole rows at the end.
-template <typename T>
-__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *Lg, T *Lst,
+//
+// FULL (kb == 16, every block but a matrix's last) drops the per-column
+// bound test, so the loop is one basic block and the compiler can overlap a
+// column's updates with the next column's pivot chain.
+template <typename T, bool FULL>
+__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb_, T *Lg, T *Lst,
                                                  int lane, int *s_info) {
+    const int kb = FULL ? kDiagNB : kb_;
     const T floor_ = pivot_floor<T>::value;
     // Every index into a[] and w[] below is a compile-time constant (the
     // loops are unrolled), so both stay in registers.
@@ -116,7 +121,7 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
     int bad = 0;
 #pragma unroll
     for (int j = 0; j < kDiagNB; ++j) {
-        if (j < kb) {  // warp-uniform
+        if (FULL || j < kb) {  // warp-uniform
             const T d = __shfl_sync(0xffffffffu, dg, j);
             if (!bad && d <= T(0)) bad = k + j + 1;
             const T g = guard_nonzero(d, floor_);
@@ -169,8 +174,10 @@ __device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb, T *
 
 // ---- panel solve and trailing update, CUDA-core form (float32) ----------
 
+// The panel rows of L are final here, so they also go to global memory (rows
+// < n; the rows below are the right-hand sides).
 template <typename T, int NT>
-__device__ __forceinline__ void panel_simt(T *S, int n, int R, int k, int kb) {
+__device__ __forceinline__ void panel_simt(T *S, int n, int R, int k, int kb, T *Lg) {
     const int tid = threadIdx.x;
     const int r0 = k + kb;
     int wro[kDiagNB];
@@ -188,6 +195,7 @@ __device__ __forceinline__ void panel_simt(T *S, int n, int R, int k, int kb) {
 #pragma unroll
                 for (int i = 0; i <= j; ++i) out += a[i] * S[wro[j] + i];
                 S[ro + j] = out;
+                if (r < n) Lg[(int64_t)r * n + k + j] = out;
             }
         }
     }
@@ -266,8 +274,9 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 }
 
 // Panel rows in 8-row blocks, one warp per block: rows x 16 times W^T (16 x 16).
+// The results are final rows of L: they go to shared and global memory.
 template <int NT>
-__device__ __forceinline__ void panel_dmma(double *S, int n, int R, int k, int kb) {
+__device__ __forceinline__ void panel_dmma(double *S, int n, int R, int k, int kb, double *Lg) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
     const int r0 = k + kb;
@@ -303,66 +312,83 @@ __device__ __forceinline__ void panel_dmma(double *S, int n, int R, int k, int k
 #pragma unroll
                 for (int v = 0; v < 2; ++v) {
                     const int j = jb * 8 + 2 * t + v;
-                    if (j < kb) S[ro + j] = c[jb][v];
+                    if (j < kb) {
+                        S[ro + j] = c[jb][v];
+                        if (row < n) Lg[(int64_t)row * n + k + j] = c[jb][v];
+                    }
                 }
         }
     }
 }
 
-// Trailing update in 8x8 blocks of the augmented trapezoid, one warp each.
+// Trailing update in 16x16 tiles of the augmented trapezoid, one warp each:
+// 2 x 2 DMMA tiles per warp, so each fragment loaded from shared memory
+// feeds two DMMAs, and four independent accumulator chains keep the FP64
+// pipe busy.  On a diagonal tile the block above the diagonal is skipped.
 template <int NT>
 __device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, int kb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
     const int r0 = k + kb;
     const int g = lane >> 2, t = lane & 3;
-    const int TR = (R - r0 + 7) >> 3, TN = (n - r0 + 7) >> 3;
+    const int TR = (R - r0 + 15) >> 4, TN = (n - r0 + 15) >> 4;
     if (TN <= 0) return;
     const int tiles = TN * (TN + 1) / 2 + (TR - TN) * TN;
-    // Two tiles per pass: independent accumulator chains for the DMMA pipe.
-    for (int e = warp; e < tiles; e += 2 * NW) {
-        const int e2 = e + NW;
-        const bool two = e2 < tiles;
-        int ti, tj, ti2 = 0, tj2 = 0;
+    for (int e = warp; e < tiles; e += NW) {
+        int ti, tj;
         trap_tile(e, TN, ti, tj);
-        if (two) trap_tile(e2, TN, ti2, tj2);
-        const int i0 = r0 + 8 * ti, j0 = r0 + 8 * tj;
-        const int i02 = r0 + 8 * ti2, j02 = r0 + 8 * tj2;
-        const int arow = prow_off(min(i0 + g, R - 1), n) + k;
-        const int brow = prow_off(min(j0 + g, n - 1), n) + k;
-        const int arow2 = prow_off(min(i02 + g, R - 1), n) + k;
-        const int brow2 = prow_off(min(j02 + g, n - 1), n) + k;
-        double a[4], b[4], a2[4], b2[4];
+        const int i0 = r0 + 16 * ti, j0 = r0 + 16 * tj;
+        const bool upper_skip = ti == tj;  // rows i0..i0+7 x cols j0+8..j0+15 lie above the diagonal
+        int ar[2], br[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            ar[h] = prow_off(min(i0 + 8 * h + g, R - 1), n) + k;
+            br[h] = prow_off(min(j0 + 8 * h + g, n - 1), n) + k;
+        }
+        double a[2][4], b[2][4];
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
             const int p = kk * 4 + t;
-            a[kk] = p < kb ? S[arow + p] : 0.0;
-            b[kk] = p < kb ? S[brow + p] : 0.0;
-            a2[kk] = (two && p < kb) ? S[arow2 + p] : 0.0;
-            b2[kk] = (two && p < kb) ? S[brow2 + p] : 0.0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                a[h][kk] = p < kb ? S[ar[h] + p] : 0.0;
+                b[h][kk] = p < kb ? S[br[h] + p] : 0.0;
+            }
         }
-        double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+        double c[2][2][2] = {};
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
-            dmma_8x8x4(c0, c1, a[kk], b[kk]);
-            dmma_8x8x4(d0, d1, a2[kk], b2[kk]);
+            dmma_8x8x4(c[0][0][0], c[0][0][1], a[0][kk], b[0][kk]);
+            dmma_8x8x4(c[1][0][0], c[1][0][1], a[1][kk], b[0][kk]);
+            dmma_8x8x4(c[1][1][0], c[1][1][1], a[1][kk], b[1][kk]);
+            if (!upper_skip) dmma_8x8x4(c[0][1][0], c[0][1][1], a[0][kk], b[1][kk]);
         }
-        int i = i0 + g;
-        if (i < R) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = i0 + 8 * h + g;
+            if (i >= R) continue;
             const int ro = prow_off(i, n);
-            const int j = j0 + 2 * t;
-            if (j < n && j <= i) S[ro + j] -= c0;
-            if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c1;
-        }
-        i = i02 + g;
-        if (two && i < R) {
-            const int ro = prow_off(i, n);
-            const int j = j02 + 2 * t;
-            if (j < n && j <= i) S[ro + j] -= d0;
-            if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= d1;
+#pragma unroll
+            for (int hb = 0; hb < 2; ++hb) {
+                const int j = j0 + 8 * hb + 2 * t;
+                if (j < n && j <= i) S[ro + j] -= c[h][hb][0];
+                if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c[h][hb][1];
+            }
         }
     }
 }
+
+// One element global -> shared without a register round trip (cp.async), so
+// a thread keeps all of its staging loads in flight at once.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(unsigned dst, const T *src) {
+    static_assert(sizeof(T) == 8 || sizeof(T) == 4, "element size");
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <typename T, int NT>
 __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *xb, int *s_info) {
@@ -378,34 +404,42 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
     if (tid == 0) *s_info = 0;
 
     // Stage the lower triangle and B^T.  The packed index e of (i, j) is
-    // i(i+1)/2 + j, so the copy is one flat, independent-load loop.
+    // i(i+1)/2 + j, so the copy is one flat loop of asynchronous copies.
     const int bro = (n * (n + 1)) / 2;
-#pragma unroll 4
-    for (int e = tid; e < bro; e += NT) {
-        int i = tri_row(e);
-        S[e] = A[(int64_t)i * n + (e - (i * (i + 1)) / 2)];
-    }
-    for (int e = tid; e < n * nrhs; e += NT) {
-        int j = e / nrhs, r = e - j * nrhs;
-        S[bro + r * n + j] = B[e];
+    {
+        const unsigned sbase = (unsigned)__cvta_generic_to_shared(S);
+        for (int e = tid; e < bro; e += NT) {
+            const int i = tri_row(e);
+            cp_async_elem<T>(sbase + (unsigned)e * sizeof(T),
+                             A + (int64_t)i * n + (e - (i * (i + 1)) / 2));
+        }
+        for (int e = tid; e < n * nrhs; e += NT) {
+            const int j = e / nrhs, r = e - j * nrhs;
+            cp_async_elem<T>(sbase + (unsigned)(bro + r * n + j) * sizeof(T), B + e);
+        }
+        cp_async_wait_all();
     }
     __syncthreads();
 
     for (int k = 0; k < n; k += kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        if (warp == 0) potrf_diag_block<T>(S, n, k, kb, L, xb, lane, s_info);
+        if (warp == 0) {
+            if (kb == kDiagNB)
+                potrf_diag_block<T, true>(S, n, k, kb, L, xb, lane, s_info);
+            else
+                potrf_diag_block<T, false>(S, n, k, kb, L, xb, lane, s_info);
+        }
         __syncthreads();
 
         // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T, W
         // (the block's inverse) sitting where the block of L was; then the
         // trailing update of the augmented trapezoid.
-        const int r0 = k + kb;
         if constexpr (std::is_same<T, double>::value) {
-            panel_dmma<NT>(S, n, R, k, kb);
+            panel_dmma<NT>(S, n, R, k, kb, L);
             __syncthreads();
             trailing_dmma<NT>(S, n, R, k, kb);
         } else {
-            panel_simt<T, NT>(S, n, R, k, kb);
+            panel_simt<T, NT>(S, n, R, k, kb, L);
             __syncthreads();
             trailing_simt<T, NT>(S, n, R, k, kb);
         }
@@ -413,37 +447,39 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
     }
 
     // Rows n..n+nrhs of S now hold y^T = (L^-1 B)^T.  Back substitution
-    // L^T x = y, 16-row blocks bottom-up, with the stored block inverses.
-    for (int k = ((n - 1) / kDiagNB) * kDiagNB; k >= 0; k -= kDiagNB) {
+    // L^T x = y, 16-row blocks bottom-up, with the stored block inverses:
+    // x_blk = W^T y_blk, then y[0:k] -= L[k:k+kb, 0:k]^T x_blk.  (L itself
+    // went to global memory block by block during the factorization.)
+    for (int k = nrhs > 0 ? ((n - 1) / kDiagNB) * kDiagNB : -1; k >= 0; k -= kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        if (tid < kb * nrhs) {  // x_blk = W^T y_blk
-            const int j = tid / nrhs, c = tid - j * nrhs;
+        for (int q = tid; q < kDiagNB * nrhs; q += NT) {
+            const int j = q & (kDiagNB - 1), c = q >> 4;
             const T *y = S + bro + c * n + k;
-            T s = T(0);
-            for (int i = j; i < kb; ++i) s += S[prow_off(k + i, n) + k + j] * y[i];
-            xb[j * kPotrfMaxRhs + c] = s;
+            T acc = T(0);
+#pragma unroll
+            for (int i = 0; i < kDiagNB; ++i)
+                if (i >= j && i < kb) acc += S[prow_off(k + i, n) + k + j] * y[i];
+            xb[j * kPotrfMaxRhs + c] = j < kb ? acc : T(0);  // zero rows past kb
         }
         __syncthreads();
-        if (tid < kb * nrhs) {
-            const int j = tid / nrhs, c = tid - j * nrhs;
-            S[bro + c * n + k + j] = xb[j * kPotrfMaxRhs + c];
+        for (int q = tid; q < kDiagNB * nrhs; q += NT) {
+            const int j = q & (kDiagNB - 1), c = q >> 4;
+            if (j < kb) S[bro + c * n + k + j] = xb[j * kPotrfMaxRhs + c];
         }
-        for (int e = tid; e < k * nrhs; e += NT) {  // y[0:k] -= L[k:k+kb, 0:k]^T x_blk
-            const int i = e / nrhs, c = e - i * nrhs;
-            T s = T(0);
-            for (int j = 0; j < kb; ++j) s += S[prow_off(k + j, n) + i] * xb[j * kPotrfMaxRhs + c];
-            S[bro + c * n + i] -= s;
+        for (int i = tid; i < k; i += NT) {
+            T l[kDiagNB];
+#pragma unroll
+            for (int q = 0; q < kDiagNB; ++q) l[q] = q < kb ? S[prow_off(k + q, n) + i] : T(0);
+            for (int r = 0; r < nrhs; ++r) {
+                T acc = T(0);
+#pragma unroll
+                for (int q = 0; q < kDiagNB; ++q) acc += l[q] * xb[q * kPotrfMaxRhs + r];
+                S[bro + r * n + i] -= acc;
+            }
         }
         __syncthreads();
     }
 
-    // Write back L's off-diagonal blocks (the diagonal blocks went out as
-    // they were factored) and X.
-#pragma unroll 4
-    for (int e = tid; e < bro; e += NT) {
-        const int i = tri_row(e), j = e - (i * (i + 1)) / 2;
-        if (j < (i / kDiagNB) * kDiagNB) L[(int64_t)i * n + j] = S[e];
-    }
     for (int e = tid; e < n * nrhs; e += NT) {
         int j = e / nrhs, r = e - j * nrhs;
         X[e] = S[bro + r * n + j];

@@ -68,7 +68,8 @@ def test_batched_potrf_potrs_matches_oracle(oracle, dtype):
 
 @pytest.mark.parametrize("nrhs", [0, 1, 8])
 def test_batched_rhs_counts_and_aliasing(oracle, nrhs):
-    ns = np.array([5, 128, 33, 1, 64, 100], dtype=np.int32)
+    # 16 and 32 put 16 x 8 = 128 back-solve items on a 64-thread CTA.
+    ns = np.array([5, 128, 33, 1, 64, 100, 16, 32, 31], dtype=np.int32)
     A, B = make_batch(ns, nrhs, np.float64, seed=nrhs)
     gotA, gotX, info = run_gpu(ns, A, B, nrhs, alias=nrhs > 0)
     wantL, wantX = oracle.batched_cholesky_solve(ns, A, B if nrhs else np.zeros(0), nrhs)
