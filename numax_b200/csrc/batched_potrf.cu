@@ -36,9 +36,7 @@ namespace nmx {
 constexpr int kPotrfMaxN = 128;
 constexpr int kPotrfMaxRhs = 8;
 constexpr int kDiagNB = 16;
-constexpr int kPotrfStage = kDiagNB * kPotrfMaxRhs > kDiagNB * (kDiagNB + 1) / 2
-                                ? kDiagNB * kPotrfMaxRhs
-                                : kDiagNB * (kDiagNB + 1) / 2;
+constexpr int kPotrfStage = kDiagNB * kPotrfMaxRhs;
 
 struct BatchedPotrfArgs {
     const int32_t *order;  // matrix indices, bucket-contiguous, largest first
@@ -55,12 +53,12 @@ struct BatchedPotrfArgs {
 
 // Shared-memory words (of T) one CTA needs for matrices up to nmax: the
 // packed lower triangle (row i at i(i+1)/2), nrhs full rows of B^T below it,
-// and a staging area: a 16 x nrhs block in the back solve, before that the
-// packed 16 x 16 diagonal block of L on its way to global memory.  The inverse of each
+// the reciprocals 1/l_ii of L's diagonal (nmax), and a 16 x nrhs staging
+// block for the back solve.  The inverse of each
 // 16x16 diagonal block is kept in place of that block once the block of L
 // has been written out.
 __host__ __device__ inline int potrf_smem_elems(int nmax, int nrhs) {
-    return nmax * (nmax + 1) / 2 + nrhs * nmax + kPotrfStage + 2;
+    return nmax * (nmax + 1) / 2 + nrhs * nmax + nmax + kPotrfStage + 2;
 }
 
 // Row of packed lower-triangle index e (e = i(i+1)/2 + j, 0 <= j <= i).
@@ -83,123 +81,118 @@ __device__ __forceinline__ int prow_off(int i, int n) {
 __device__ __forceinline__ double inv_sqrt(double g) { return rsqrt(g); }
 __device__ __forceinline__ float inv_sqrt(float g) { return rsqrtf(g); }
 
-// One warp factors the kb x kb diagonal block at (k, k) in registers (lane i
-// holds row i) with numax's Array-tier rule l_jj = sqrt(guard_nonzero(d,
-// 1e-30)) (a negative d gives NaN; info records the first d <= 0), and builds
-// W = L_kk^-1 (lower, W[i][i] = 1/l_ii) in the same loop by the product form
-// W = L_kb-1^-1 ... L_0^-1, where L_j is the identity with column j of L:
-// step j scales row j of W by 1/l_jj and subtracts l_ij times it from each
-// row i > j.  W then replaces the block in shared memory.
+// Start of row k + i of the diagonal block at (k, k) in the packed store
+// (k + i < n): tri(k + i) + k = tri(k) + i k + tri(i) + k.
+__device__ __forceinline__ int blk_row(int tk, int k, int i) { return tk + i * k + (i * (i + 1)) / 2 + k; }
+
+// One warp factors the kb x kb diagonal block at (k, k) in place (lane i
+// holds row i in registers) with numax's Array-tier rule
+// l_jj = sqrt(guard_nonzero(d, 1e-30)) (a negative d gives NaN; info records
+// the first d <= 0).  Column j of L is written to shared memory as it is
+// formed (the rows' packed offsets are distinct modulo 16 within a block, so
+// the column store is conflict-free) and read back as broadcasts by the
+// updates of the later columns; 1/l_jj goes to Dv[k + j] for the panel and
+// the back solve.  At the end the block leaves for global memory as rows.
 //
-// The pivot chain per column is shfl(d_j) -> 1/sqrt -> l_{j+1,j} -> d_{j+1}:
-// each row's diagonal entry is kept in a scalar so that the next pivot does
-// not wait on the broadcast of the column.  Columns of L go to a packed
-// staging triangle in shared memory (row i at i(i+1)/2: the 16 row offsets
-// are distinct modulo 16, so a column store is conflict-free) and leave for
-// global memory as whole rows at the end.
+// The pivot chain per column is l_{j+1,j} -> d_{j+1} -> shfl -> 1/sqrt: each
+// row keeps its diagonal entry in a scalar, and the next pivot's reciprocal
+// square root is issued before the column's updates, which run in its
+// shadow.
 //
 // FULL (kb == 16, every block but a matrix's last) drops the per-column
-// bound test, so the loop is one basic block and the compiler can overlap a
-// column's updates with the next column's pivot chain.
+// bound tests, so the loop is one basic block.
 template <typename T, bool FULL>
-__device__ __forceinline__ void potrf_diag_block(T *S, int n, int k, int kb_, T *Lg, T *Lst,
+__device__ __noinline__ void potrf_diag_block(T *S, int n, int k, int kb_, T *Lg, T *Dv,
                                                  int lane, int *s_info) {
     const int kb = FULL ? kDiagNB : kb_;
     const T floor_ = pivot_floor<T>::value;
-    // Every index into a[] and w[] below is a compile-time constant (the
-    // loops are unrolled), so both stay in registers.
+    const int tk = (k * (k + 1)) / 2;
+    // Every index into a[] below is a compile-time constant (the loops are
+    // unrolled), so it stays in registers.
     T a[kDiagNB];  // strictly lower part of row `lane`
-    T w[kDiagNB];  // row `lane` of W
     const bool act = lane < kb;
-    const int myro = prow_off(k + min(lane, kb - 1), n) + k;
+    const int myro = blk_row(tk, k, min(lane, kb - 1));
 #pragma unroll
     for (int c = 0; c < kDiagNB; ++c) a[c] = (act && c < lane) ? S[myro + c] : T(0);
     T dg = act ? S[myro + min(lane, kDiagNB - 1)] : T(1);
-#pragma unroll
-    for (int c = 0; c < kDiagNB; ++c) w[c] = (c == lane) ? T(1) : T(0);
-    T *lst = Lst + (lane * (lane + 1)) / 2;  // staging row `lane` (used by lanes < kb)
     int bad = 0;
+    // guard_nonzero(d) is d itself for |d| >= floor (and for NaN), so the
+    // reciprocal square root need not wait on the guard.
+    T d = __shfl_sync(0xffffffffu, dg, 0);
+    T inv = inv_sqrt(d);
+    if (!(fabs(d) >= floor_)) inv = inv_sqrt(guard_nonzero(d, floor_));
 #pragma unroll
     for (int j = 0; j < kDiagNB; ++j) {
         if (FULL || j < kb) {  // warp-uniform
-            const T d = __shfl_sync(0xffffffffu, dg, j);
             if (!bad && d <= T(0)) bad = k + j + 1;
-            const T g = guard_nonzero(d, floor_);
-            const T inv = inv_sqrt(g);  // 1 / l_jj, also W's diagonal entry
-            T lij = T(0);
-            if (lane == j) {
-                dg = g * inv;
-                lst[j] = dg;
+            // Lane roles by selects, not branches: divergent branches here
+            // cost more than the few redundant multiplies.
+            const T ljj = guard_nonzero(d, floor_) * inv;
+            const T lij = lane > j ? a[j] * inv : T(0);
+            dg = lane == j ? ljj : dg - lij * lij;
+            if (act && lane >= j) S[myro + j] = lane == j ? ljj : lij;
+            if (lane == j) Dv[k + j] = inv;
+            __syncwarp();
+            if (FULL ? j + 1 < kDiagNB : j + 1 < kb) {
+                d = __shfl_sync(0xffffffffu, dg, (j + 1) & 31);
+                inv = inv_sqrt(d);
+                if (!(fabs(d) >= floor_)) inv = inv_sqrt(guard_nonzero(d, floor_));
             }
-            if (lane > j) {
-                lij = a[j] * inv;
-                dg -= lij * lij;
-                if (act) lst[j] = lij;
-            }
+            // Entries at or above a lane's diagonal are never read, so the
+            // update runs unpredicated in the lane (lij is 0 on lanes <= j).
 #pragma unroll
-            for (int c = j + 1; c < kDiagNB; ++c) {
-                // Entries at or above a lane's diagonal are never read, so
-                // this runs unpredicated (lij is 0 on lanes <= j); a
-                // predicate on `lane > c` makes the compiler index a[] at
-                // run time.
-                const T lcj = __shfl_sync(0xffffffffu, lij, c);
-                a[c] -= lij * lcj;
-            }
-            if (lane == j) {
-#pragma unroll
-                for (int c = 0; c <= j; ++c) w[c] *= inv;
-            }
-#pragma unroll
-            for (int c = 0; c <= j; ++c) {
-                const T wjc = __shfl_sync(0xffffffffu, w[c], j);
-                if (lane > j) w[c] -= lij * wjc;
-            }
+            for (int c = j + 1; c < kDiagNB; ++c)
+                if (FULL || c < kb) a[c] -= lij * S[blk_row(tk, k, c) + j];
         }
     }
     if (lane == 0 && bad && *s_info == 0) *s_info = bad;
-    if (act) {
-#pragma unroll
-        for (int c = 0; c < kDiagNB; ++c)
-            if (c <= lane) S[myro + c] = w[c];
-    }
     __syncwarp();
     // Two rows of the block per warp-wide store.
 #pragma unroll
     for (int e = lane; e < kDiagNB * kDiagNB; e += 32) {
         const int r = e >> 4, c = e & 15;
-        if (r < kb && c <= r) Lg[(int64_t)(k + r) * n + k + c] = Lst[(r * (r + 1)) / 2 + c];
+        if (r < kb && c <= r) Lg[(int64_t)(k + r) * n + k + c] = S[blk_row(tk, k, r) + c];
     }
-    __syncwarp();
 }
 
-// ---- panel solve and trailing update, CUDA-core form (float32) ----------
-
-// The panel rows of L are final here, so they also go to global memory (rows
-// < n; the rows below are the right-hand sides).
-template <typename T, int NT>
-__device__ __forceinline__ void panel_simt(T *S, int n, int R, int k, int kb, T *Lg) {
-    const int tid = threadIdx.x;
-    const int r0 = k + kb;
-    int wro[kDiagNB];
-#pragma unroll
-    for (int j = 0; j < kDiagNB; ++j) wro[j] = prow_off(k + min(j, kb - 1), n) + k;
-    for (int r = r0 + tid; r < R; r += NT) {
+// Panel: rows r in [k+kb, R) solve x L_kk^T = S[r, k:k+kb], one thread per
+// row, right-looking over the columns (x_j *= 1/l_jj, then x_i -= x_j l_ij);
+// the entries of L_kk are shared-memory broadcasts.  The results are final
+// rows of L (rows < n; the rows below are the right-hand sides' forward
+// substitution), so they go to shared and global memory.
+//
+// FULL (kb == 16) drops the bound tests: loads under a run-time condition
+// cannot be scheduled ahead, and that serializes the solve.
+template <typename T, int NT, bool FULL>
+__device__ __forceinline__ void panel_trsm(T *S, int n, int R, int k, int kb_, const T *Dv,
+                                           T *Lg) {
+    const int kb = FULL ? kDiagNB : kb_;
+    const int tk = (k * (k + 1)) / 2;
+    for (int r = k + kb + (int)threadIdx.x; r < R; r += NT) {
         const int ro = prow_off(r, n) + k;
-        T a[kDiagNB];
+        T x[kDiagNB];
 #pragma unroll
-        for (int j = 0; j < kDiagNB; ++j) a[j] = j < kb ? S[ro + j] : T(0);
+        for (int j = 0; j < kDiagNB; ++j) x[j] = (FULL || j < kb) ? S[ro + j] : T(0);
 #pragma unroll
         for (int j = 0; j < kDiagNB; ++j) {
-            if (j < kb) {
-                T out = T(0);
+            if (FULL || j < kb) {
+                x[j] *= Dv[k + j];
 #pragma unroll
-                for (int i = 0; i <= j; ++i) out += a[i] * S[wro[j] + i];
-                S[ro + j] = out;
-                if (r < n) Lg[(int64_t)r * n + k + j] = out;
+                for (int i = j + 1; i < kDiagNB; ++i)
+                    if (FULL || i < kb) x[i] -= x[j] * S[blk_row(tk, k, i) + j];
             }
         }
+        T *lrow = Lg + (int64_t)r * n + k;
+#pragma unroll
+        for (int j = 0; j < kDiagNB; ++j)
+            if (FULL || j < kb) {
+                S[ro + j] = x[j];
+                if (r < n) lrow[j] = x[j];
+            }
     }
 }
+
+// ---- trailing update, CUDA-core form (float32) ---------------------------
 
 // Flat index of a tile of the augmented trapezoid -> (tile row, tile col):
 // the first TN tile rows are triangular, the rest are full TN-wide.
@@ -273,55 +266,8 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// Panel rows in 8-row blocks, one warp per block: rows x 16 times W^T (16 x 16).
-// The results are final rows of L: they go to shared and global memory.
-template <int NT>
-__device__ __forceinline__ void panel_dmma(double *S, int n, int R, int k, int kb, double *Lg) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = NT / 32;
-    const int r0 = k + kb;
-    const int g = lane >> 2, t = lane & 3;
-    // B fragments: W^T, B[i][j] = W[j][i] (zero above W's diagonal / past kb).
-    double bw[2][4];
-#pragma unroll
-    for (int jb = 0; jb < 2; ++jb)
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int j = jb * 8 + g, i = kk * 4 + t;
-            bw[jb][kk] = (j < kb && i <= j) ? S[prow_off(k + j, n) + k + i] : 0.0;
-        }
-    const int blocks = (R - r0 + 7) >> 3;
-    for (int b = warp; b < blocks; b += NW) {
-        const int row = r0 + 8 * b + g;
-        const int ro = prow_off(min(row, R - 1), n) + k;
-        double a[4];
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int i = kk * 4 + t;
-            a[kk] = i < kb ? S[ro + i] : 0.0;
-        }
-        double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll
-        for (int jb = 0; jb < 2; ++jb)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) dmma_8x8x4(c[jb][0], c[jb][1], a[kk], bw[jb][kk]);
-        __syncwarp();
-        if (row < R) {
-#pragma unroll
-            for (int jb = 0; jb < 2; ++jb)
-#pragma unroll
-                for (int v = 0; v < 2; ++v) {
-                    const int j = jb * 8 + 2 * t + v;
-                    if (j < kb) {
-                        S[ro + j] = c[jb][v];
-                        if (row < n) Lg[(int64_t)row * n + k + j] = c[jb][v];
-                    }
-                }
-        }
-    }
-}
-
-// Trailing update in 16x16 tiles of the augmented trapezoid, one warp each:
+// Trailing update in 16x16 tiles of the augmented trapezoid, one warp each
+// (a block with a trailing part is always 16 wide, so kb == 16 here):
 // 2 x 2 DMMA tiles per warp, so each fragment loaded from shared memory
 // feeds two DMMAs, and four independent accumulator chains keep the FP64
 // pipe busy.  On a diagonal tile the block above the diagonal is skipped.
@@ -351,8 +297,8 @@ __device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, in
             const int p = kk * 4 + t;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                a[h][kk] = p < kb ? S[ar[h] + p] : 0.0;
-                b[h][kk] = p < kb ? S[br[h] + p] : 0.0;
+                a[h][kk] = S[ar[h] + p];
+                b[h][kk] = S[br[h] + p];
             }
         }
         double c[2][2][2] = {};
@@ -378,6 +324,127 @@ __device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, in
     }
 }
 
+// ---- back substitution on the FP64 tensor cores ----------------------------
+
+// W_b = L_bb^-1 for every 16 x 16 diagonal block, one thread per (block,
+// column c): L_bb w = e_c, right-looking (w_p *= 1/l_pp, w_i -= l_ip w_p).
+// Done once after the factorization, off its critical path; W_b then
+// replaces L_bb in shared memory (L_bb has gone to global memory).  Needs
+// NT >= 16 * ceil(n / 16), which every bucket's thread count meets.
+template <int NT>
+__device__ __forceinline__ void diag_inverses(double *S, int n, const double *Dv) {
+    const int q = threadIdx.x;
+    const int k = (q >> 4) * kDiagNB, c = q & 15;
+    const int kb = min(kDiagNB, n - k);
+    const bool act = k < n && c < kb;
+    const int tk = (k * (k + 1)) / 2;
+    double w[kDiagNB];
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < kDiagNB; ++i) w[i] = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+        for (int p = 0; p < kDiagNB; ++p) {
+            w[p] *= Dv[k + min(p, kb - 1)];
+#pragma unroll
+            for (int i = p + 1; i < kDiagNB; ++i) {
+                // Rows past kb are clamped for the address; w stays 0 there.
+                const double lip = S[blk_row(tk, k, min(i, kb - 1)) + p];
+                if (i < kb) w[i] -= lip * w[p];
+            }
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < kDiagNB; ++i)
+            if (i >= c && i < kb) S[blk_row(tk, k, i) + c] = w[i];
+    }
+    __syncthreads();
+}
+
+// One warp: x_blk = W^T y_blk for the block at k (16 x 16 times 16 x 8, the
+// right-hand sides padded to 8 columns), 2 x 4 DMMAs.  x_blk replaces y_blk
+// and goes to the staging block xb (16 x 8) for the update of the rows above.
+__device__ __forceinline__ void back_block_dmma(double *S, int n, int nrhs, int k, int kb,
+                                                int bro, double *xb) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int tk = (k * (k + 1)) / 2;
+    double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        const int i = kk * 4 + t;  // row of W and of y_blk
+        const double bv = (g < nrhs && i < kb) ? S[bro + g * n + k + i] : 0.0;
+        const int ri = blk_row(tk, k, min(i, kb - 1));
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = 8 * h + g;  // row of W^T = column of W
+            const double av = (j <= i && i < kb) ? S[ri + j] : 0.0;
+            dmma_8x8x4(c[h][0], c[h][1], av, bv);
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int j = 8 * h + g, col = 2 * t + v;
+            xb[j * kPotrfMaxRhs + col] = c[h][v];  // 0 for j >= kb or col >= nrhs
+            if (col < nrhs && j < kb) S[bro + col * n + k + j] = c[h][v];
+        }
+}
+
+// y[0:k] -= L[k:k+16, 0:k]^T x_blk, 8-row blocks of y, one warp each,
+// 4 DMMAs per block (xb rows past kb are 0).
+template <int NT>
+__device__ __forceinline__ void back_update_dmma(double *S, int n, int nrhs, int k, int kb,
+                                                 int bro, const double *xb) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    constexpr int NW = NT / 32;
+    double bx[4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) bx[kk] = xb[(kk * 4 + t) * kPotrfMaxRhs + g];
+    int rq[4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        const int q = min(kk * 4 + t, kb - 1);
+        rq[kk] = ((k + q) * (k + q + 1)) / 2;  // start of row k + q
+    }
+    for (int b = warp; b < (k >> 3); b += NW) {
+        const int i = 8 * b + g;
+        double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) dmma_8x8x4(c0, c1, S[rq[kk] + i], bx[kk]);
+        if (2 * t < nrhs) S[bro + (2 * t) * n + i] -= c0;
+        if (2 * t + 1 < nrhs) S[bro + (2 * t + 1) * n + i] -= c1;
+    }
+}
+
+// x_blk = L_kk^-T y_blk for one right-hand side (y in shared memory, rows
+// k..k+kb), bottom-up: x_j = y_j / l_jj, then y_i -= l_ji x_j for i < j.
+// The result replaces y and goes to column xs[0], xs[kPotrfMaxRhs], ... of
+// the staging block, zero past kb.
+template <typename T, bool FULL>
+__device__ __forceinline__ void block_back_solve(T *y, const T *S, const T *Dv, int tk, int k,
+                                                 int kb_, T *xs) {
+    const int kb = FULL ? kDiagNB : kb_;
+    T yv[kDiagNB];
+#pragma unroll
+    for (int i = 0; i < kDiagNB; ++i) yv[i] = (FULL || i < kb) ? y[min(i, kb - 1)] : T(0);
+#pragma unroll
+    for (int j = kDiagNB - 1; j >= 0; --j) {
+        if (FULL || j < kb) {
+            yv[j] *= Dv[k + j];
+            const int rj = blk_row(tk, k, j);
+#pragma unroll
+            for (int i = 0; i < j; ++i) yv[i] -= S[rj + i] * yv[j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kDiagNB; ++i) {
+        if (FULL || i < kb) y[i] = yv[i];
+        xs[i * kPotrfMaxRhs] = (FULL || i < kb) ? yv[i] : T(0);
+    }
+}
+
 // One element global -> shared without a register round trip (cp.async), so
 // a thread keeps all of its staging loads in flight at once.
 template <typename T>
@@ -391,7 +458,8 @@ __device__ __forceinline__ void cp_async_elem(unsigned dst, const T *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <typename T, int NT>
-__device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *xb, int *s_info) {
+__device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *Dv, T *xb,
+                                int *s_info) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
     const int n = args.ns[mi];
@@ -425,56 +493,71 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *x
         const int kb = min(kDiagNB, n - k);
         if (warp == 0) {
             if (kb == kDiagNB)
-                potrf_diag_block<T, true>(S, n, k, kb, L, xb, lane, s_info);
+                potrf_diag_block<T, true>(S, n, k, kb, L, Dv, lane, s_info);
             else
-                potrf_diag_block<T, false>(S, n, k, kb, L, xb, lane, s_info);
+                potrf_diag_block<T, false>(S, n, k, kb, L, Dv, lane, s_info);
         }
         __syncthreads();
 
-        // Panel: rows r in [k+kb, R): S[r, k:k+kb] := S[r, k:k+kb] W^T, W
-        // (the block's inverse) sitting where the block of L was; then the
-        // trailing update of the augmented trapezoid.
-        if constexpr (std::is_same<T, double>::value) {
-            panel_dmma<NT>(S, n, R, k, kb, L);
-            __syncthreads();
+        // Panel, then the trailing update of the augmented trapezoid.
+        if (kb == kDiagNB)
+            panel_trsm<T, NT, true>(S, n, R, k, kb, Dv, L);
+        else
+            panel_trsm<T, NT, false>(S, n, R, k, kb, Dv, L);
+        __syncthreads();
+        if constexpr (std::is_same<T, double>::value)
             trailing_dmma<NT>(S, n, R, k, kb);
-        } else {
-            panel_simt<T, NT>(S, n, R, k, kb, L);
-            __syncthreads();
+        else
             trailing_simt<T, NT>(S, n, R, k, kb);
-        }
         __syncthreads();
     }
 
     // Rows n..n+nrhs of S now hold y^T = (L^-1 B)^T.  Back substitution
-    // L^T x = y, 16-row blocks bottom-up, with the stored block inverses:
-    // x_blk = W^T y_blk, then y[0:k] -= L[k:k+kb, 0:k]^T x_blk.  (L itself
-    // went to global memory block by block during the factorization.)
-    for (int k = nrhs > 0 ? ((n - 1) / kDiagNB) * kDiagNB : -1; k >= 0; k -= kDiagNB) {
+    // L^T x = y, 16-row blocks bottom-up.  FP64: the diagonal blocks are
+    // inverted once (W_b), then per block x_blk = W^T y_blk and
+    // y[0:k] -= L[k:k+kb, 0:k]^T x_blk are both DMMA products.
+    if constexpr (std::is_same<T, double>::value) {
+        if (nrhs > 0) {
+            diag_inverses<NT>(S, n, Dv);
+            for (int k = ((n - 1) / kDiagNB) * kDiagNB; k >= 0; k -= kDiagNB) {
+                const int kb = min(kDiagNB, n - k);
+                if (warp == 0) back_block_dmma(S, n, nrhs, k, kb, bro, xb);
+                __syncthreads();
+                back_update_dmma<NT>(S, n, nrhs, k, kb, bro, xb);
+                __syncthreads();
+            }
+        }
+    }
+    // float32: x_blk solves L_kk^T x_blk = y_blk (one thread per right-hand
+    // side), then y[0:k] -= L[k:k+kb, 0:k]^T x_blk (one thread per row, every
+    // right-hand side at once).
+    for (int k = (nrhs > 0 && !std::is_same<T, double>::value) ? ((n - 1) / kDiagNB) * kDiagNB : -1;
+         k >= 0; k -= kDiagNB) {
         const int kb = min(kDiagNB, n - k);
-        for (int q = tid; q < kDiagNB * nrhs; q += NT) {
-            const int j = q & (kDiagNB - 1), c = q >> 4;
-            const T *y = S + bro + c * n + k;
-            T acc = T(0);
-#pragma unroll
-            for (int i = 0; i < kDiagNB; ++i)
-                if (i >= j && i < kb) acc += S[prow_off(k + i, n) + k + j] * y[i];
-            xb[j * kPotrfMaxRhs + c] = j < kb ? acc : T(0);  // zero rows past kb
+        const int tk = (k * (k + 1)) / 2;
+        for (int c = tid; c < nrhs; c += NT) {
+            if (kb == kDiagNB)
+                block_back_solve<T, true>(S + bro + c * n + k, S, Dv, tk, k, kb, xb + c);
+            else
+                block_back_solve<T, false>(S + bro + c * n + k, S, Dv, tk, k, kb, xb + c);
         }
         __syncthreads();
-        for (int q = tid; q < kDiagNB * nrhs; q += NT) {
-            const int j = q & (kDiagNB - 1), c = q >> 4;
-            if (j < kb) S[bro + c * n + k + j] = xb[j * kPotrfMaxRhs + c];
-        }
         for (int i = tid; i < k; i += NT) {
             T l[kDiagNB];
 #pragma unroll
-            for (int q = 0; q < kDiagNB; ++q) l[q] = q < kb ? S[prow_off(k + q, n) + i] : T(0);
-            for (int r = 0; r < nrhs; ++r) {
-                T acc = T(0);
+            for (int q = 0; q < kDiagNB; ++q) l[q] = S[blk_row(tk, k, min(q, kb - 1)) - k + i];  // xb is 0 past kb
+            // The loads and multiplies run for all 4 columns of a pass (xb
+            // has kPotrfMaxRhs columns; those >= nrhs are never stored):
+            // loads under a run-time condition would serialize the pass.
+            for (int r0 = 0; r0 < nrhs; r0 += 4) {  // 4 independent chains per pass
+                T acc[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
-                for (int q = 0; q < kDiagNB; ++q) acc += l[q] * xb[q * kPotrfMaxRhs + r];
-                S[bro + r * n + i] -= acc;
+                for (int q = 0; q < kDiagNB; ++q)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) acc[r] += l[q] * xb[q * kPotrfMaxRhs + r0 + r];
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r0 + r < nrhs) S[bro + (r0 + r) * n + i] -= acc[r];
             }
         }
         __syncthreads();
@@ -496,7 +579,8 @@ __global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
     potrf_potrs_batched_kernel(BatchedPotrfArgs args, int begin, int end, int nmax, int *counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *S = reinterpret_cast<T *>(smem_raw);
-    T *xb = S + nmax * (nmax + 1) / 2 + args.nrhs * nmax;
+    T *Dv = S + nmax * (nmax + 1) / 2 + args.nrhs * nmax;
+    T *xb = Dv + nmax;
     __shared__ int s_item, s_info;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -504,7 +588,7 @@ __global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
         const int item = begin + s_item;
         __syncthreads();
         if (item >= end) break;
-        potrf_potrs_one<T, NT>(args, args.order[item], S, xb, &s_info);
+        potrf_potrs_one<T, NT>(args, args.order[item], S, Dv, xb, &s_info);
     }
 }
 
