@@ -34,6 +34,9 @@
 namespace nmx {
 
 constexpr int kPotrfMaxN = 128;
+
+// Dynamic shared memory of the batched kernels (one matrix's working set).
+extern __shared__ __align__(16) unsigned char bp_smem[];
 constexpr int kPotrfMaxRhs = 8;
 constexpr int kDiagNB = 16;
 constexpr int kPotrfStage = kDiagNB * kPotrfMaxRhs;
@@ -81,6 +84,16 @@ __device__ __forceinline__ int prow_off(int i, int n) {
 __device__ __forceinline__ double inv_sqrt(double g) { return rsqrt(g); }
 __device__ __forceinline__ float inv_sqrt(float g) { return rsqrtf(g); }
 
+// Named CTA barriers (ids 1..15; 0 is __syncthreads): a producer warp
+// arrives without waiting, consumers wait for the producer and each other.
+// Arrive releases and sync acquires the shared-memory writes before them.
+__device__ __forceinline__ void named_barrier_arrive(int id, int nthreads) {
+    asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void named_barrier_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // Start of row k + i of the diagonal block at (k, k) in the packed store
 // (k + i < n): tri(k + i) + k = tri(k) + i k + tri(i) + k.
 __device__ __forceinline__ int blk_row(int tk, int k, int i) { return tk + i * k + (i * (i + 1)) / 2 + k; }
@@ -101,9 +114,21 @@ __device__ __forceinline__ int blk_row(int tk, int k, int i) { return tk + i * k
 //
 // FULL (kb == 16, every block but a matrix's last) drops the per-column
 // bound tests, so the loop is one basic block.
-template <typename T, bool FULL>
-__device__ __noinline__ void potrf_diag_block(T *S, int n, int k, int kb_, T *Lg, T *Dv,
-                                                 int lane, int *s_info) {
+//
+// The function is not inlined, so it gets a register allocation of its own
+// (inlined, it competes with the kernel's other phases and spills); the
+// packed store is reached through the dynamic shared-memory symbol itself,
+// which keeps its accesses in the shared window (32-bit addresses) rather
+// than generic pointers.  dv_off is Dv's offset from the start of S.
+//
+// PIPE: after each pair of columns (2m, 2m+1) the warp arrives on named
+// barrier 1 + m (nthreads = the CTA), releasing those columns to the
+// warps that run the panel solve alongside (panel_trsm_pipe).
+template <typename T, bool FULL, bool PIPE>
+__device__ __noinline__ void potrf_diag_block(int dv_off, int n, int k, int kb_, T *Lg, int lane,
+                                              int *s_info, int nthreads) {
+    T *S = reinterpret_cast<T *>(bp_smem);
+    T *Dv = S + dv_off;
     const int kb = FULL ? kDiagNB : kb_;
     const T floor_ = pivot_floor<T>::value;
     const int tk = (k * (k + 1)) / 2;
@@ -143,6 +168,10 @@ __device__ __noinline__ void potrf_diag_block(T *S, int n, int k, int kb_, T *Lg
 #pragma unroll
             for (int c = j + 1; c < kDiagNB; ++c)
                 if (FULL || c < kb) a[c] -= lij * S[blk_row(tk, k, c) + j];
+            if (PIPE && ((j & 1) || j + 1 == kb)) {
+                __syncwarp();
+                named_barrier_arrive(1 + (j >> 1), nthreads);
+            }
         }
     }
     if (lane == 0 && bad && *s_info == 0) *s_info = bad;
@@ -182,6 +211,50 @@ __device__ __forceinline__ void panel_trsm(T *S, int n, int R, int k, int kb_, c
                     if (FULL || i < kb) x[i] -= x[j] * S[blk_row(tk, k, i) + j];
             }
         }
+        T *lrow = Lg + (int64_t)r * n + k;
+#pragma unroll
+        for (int j = 0; j < kDiagNB; ++j)
+            if (FULL || j < kb) {
+                S[ro + j] = x[j];
+                if (r < n) lrow[j] = x[j];
+            }
+    }
+}
+
+// Panel solve of block column k run by warps 1.. while warp 0 factors the
+// diagonal block (potrf_diag_block<PIPE>): each thread takes one panel row
+// (rows k+16.. of the augmented block; the thread count always covers
+// them), waits on named barrier 1 + m for columns 2m, 2m+1 of L_kk, and
+// applies them (x_j *= 1/l_jj, x_i -= x_j l_ij).  Every thread of warps 1..
+// takes part in every barrier, with or without a row.
+template <typename T, int NT, bool FULL>
+__device__ __forceinline__ void panel_trsm_pipe(T *S, int n, int R, int k, int kb_, const T *Dv,
+                                                T *Lg) {
+    const int kb = FULL ? kDiagNB : kb_;
+    const int tk = (k * (k + 1)) / 2;
+    const int r = k + kb + (int)threadIdx.x - 32;
+    const bool has = r < R;
+    if (k + kb + (int)(threadIdx.x & ~31u) - 32 >= R) {  // no row in this warp: barriers only
+#pragma unroll
+        for (int j = 0; j < kDiagNB; j += 2)
+            if (FULL || j < kb) named_barrier_sync(1 + (j >> 1), NT);
+        return;
+    }
+    const int ro = prow_off(min(r, R - 1), n) + k;
+    T x[kDiagNB];
+#pragma unroll
+    for (int j = 0; j < kDiagNB; ++j) x[j] = (has && (FULL || j < kb)) ? S[ro + j] : T(0);
+#pragma unroll
+    for (int j = 0; j < kDiagNB; ++j) {
+        if (FULL || j < kb) {
+            if ((j & 1) == 0) named_barrier_sync(1 + (j >> 1), NT);
+            x[j] *= Dv[k + j];
+#pragma unroll
+            for (int i = j + 1; i < kDiagNB; ++i)
+                if (FULL || i < kb) x[i] -= x[j] * S[blk_row(tk, k, i) + j];
+        }
+    }
+    if (has) {
         T *lrow = Lg + (int64_t)r * n + k;
 #pragma unroll
         for (int j = 0; j < kDiagNB; ++j)
@@ -266,61 +339,65 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// Trailing update in 16x16 tiles of the augmented trapezoid, one warp each
-// (a block with a trailing part is always 16 wide, so kb == 16 here):
-// 2 x 2 DMMA tiles per warp, so each fragment loaded from shared memory
-// feeds two DMMAs, and four independent accumulator chains keep the FP64
-// pipe busy.  On a diagonal tile the block above the diagonal is skipped.
-template <int NT>
-__device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, int kb) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = NT / 32;
-    const int r0 = k + kb;
-    const int g = lane >> 2, t = lane & 3;
-    const int TR = (R - r0 + 15) >> 4, TN = (n - r0 + 15) >> 4;
-    if (TN <= 0) return;
-    const int tiles = TN * (TN + 1) / 2 + (TR - TN) * TN;
-    for (int e = warp; e < tiles; e += NW) {
-        int ti, tj;
-        trap_tile(e, TN, ti, tj);
-        const int i0 = r0 + 16 * ti, j0 = r0 + 16 * tj;
-        const bool upper_skip = ti == tj;  // rows i0..i0+7 x cols j0+8..j0+15 lie above the diagonal
-        int ar[2], br[2];
+// One 16 x 16 tile (rows i0.., cols j0..) of the trailing update
+// S[i][j] -= sum_p S[i][k+p] S[j][k+p] (p < 16), by one warp: 2 x 2 DMMA
+// tiles, so each fragment loaded from shared memory feeds two DMMAs, and
+// four independent accumulator chains keep the FP64 pipe busy.  On a tile
+// that straddles the diagonal (i0 == j0) the block above it is skipped.
+__device__ __forceinline__ void trailing_tile_dmma(double *S, int n, int R, int k, int i0, int j0) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const bool upper_skip = i0 == j0;  // rows i0..i0+7 x cols j0+8..j0+15 lie above the diagonal
+    int ar[2], br[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        ar[h] = prow_off(min(i0 + 8 * h + g, R - 1), n) + k;
+        br[h] = prow_off(min(j0 + 8 * h + g, n - 1), n) + k;
+    }
+    double a[2][4], b[2][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        const int p = kk * 4 + t;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            ar[h] = prow_off(min(i0 + 8 * h + g, R - 1), n) + k;
-            br[h] = prow_off(min(j0 + 8 * h + g, n - 1), n) + k;
+            a[h][kk] = S[ar[h] + p];
+            b[h][kk] = S[br[h] + p];
         }
-        double a[2][4], b[2][4];
+    }
+    double c[2][2][2] = {};
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int p = kk * 4 + t;
+    for (int kk = 0; kk < 4; ++kk) {
+        dmma_8x8x4(c[0][0][0], c[0][0][1], a[0][kk], b[0][kk]);
+        dmma_8x8x4(c[1][0][0], c[1][0][1], a[1][kk], b[0][kk]);
+        dmma_8x8x4(c[1][1][0], c[1][1][1], a[1][kk], b[1][kk]);
+        if (!upper_skip) dmma_8x8x4(c[0][1][0], c[0][1][1], a[0][kk], b[1][kk]);
+    }
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                a[h][kk] = S[ar[h] + p];
-                b[h][kk] = S[br[h] + p];
-            }
+    for (int h = 0; h < 2; ++h) {
+        const int i = i0 + 8 * h + g;
+        if (i >= R) continue;
+        const int ro = prow_off(i, n);
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb) {
+            const int j = j0 + 8 * hb + 2 * t;
+            if (j < n && j <= i) S[ro + j] -= c[h][hb][0];
+            if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c[h][hb][1];
         }
-        double c[2][2][2] = {};
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            dmma_8x8x4(c[0][0][0], c[0][0][1], a[0][kk], b[0][kk]);
-            dmma_8x8x4(c[1][0][0], c[1][0][1], a[1][kk], b[0][kk]);
-            dmma_8x8x4(c[1][1][0], c[1][1][1], a[1][kk], b[1][kk]);
-            if (!upper_skip) dmma_8x8x4(c[0][1][0], c[0][1][1], a[0][kk], b[1][kk]);
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = i0 + 8 * h + g;
-            if (i >= R) continue;
-            const int ro = prow_off(i, n);
-#pragma unroll
-            for (int hb = 0; hb < 2; ++hb) {
-                const int j = j0 + 8 * hb + 2 * t;
-                if (j < n && j <= i) S[ro + j] -= c[h][hb][0];
-                if (j + 1 < n && j + 1 <= i) S[ro + j + 1] -= c[h][hb][1];
-            }
-        }
+    }
+}
+
+// Trailing update of block column k (16 wide) over the trapezoid with origin
+// o (rows o..R, columns o..n, j <= i): BAND = only the 16 columns o..o+15,
+// else every column from o on.  Tiles go to warps w0, w0 + nw, ...
+template <bool BAND>
+__device__ __forceinline__ void trailing_dmma(double *S, int n, int R, int k, int o, int w0, int nw) {
+    const int warp = threadIdx.x >> 5;
+    const int TR = (R - o + 15) >> 4, TN = (n - o + 15) >> 4;
+    if (TN <= 0 || warp < w0) return;
+    const int tiles = BAND ? TR : TN * (TN + 1) / 2 + (TR - TN) * TN;
+    for (int e = warp - w0; e < tiles; e += nw) {
+        int ti = e, tj = 0;
+        if (!BAND) trap_tile(e, TN, ti, tj);
+        trailing_tile_dmma(S, n, R, k, o + 16 * ti, o + 16 * tj);
     }
 }
 
@@ -471,15 +548,15 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *D
     T *X = static_cast<T *>(args.X) + args.b_off[mi];
     if (tid == 0) *s_info = 0;
 
-    // Stage the lower triangle and B^T.  The packed index e of (i, j) is
-    // i(i+1)/2 + j, so the copy is one flat loop of asynchronous copies.
+    // Stage the lower triangle (row i at i(i+1)/2) and B^T with asynchronous
+    // copies, so every thread keeps all of its loads in flight.
     const int bro = (n * (n + 1)) / 2;
     {
         const unsigned sbase = (unsigned)__cvta_generic_to_shared(S);
-        for (int e = tid; e < bro; e += NT) {
-            const int i = tri_row(e);
-            cp_async_elem<T>(sbase + (unsigned)e * sizeof(T),
-                             A + (int64_t)i * n + (e - (i * (i + 1)) / 2));
+        for (int i = warp; i < n; i += NW) {  // row i: i + 1 elements, coalesced
+            const unsigned drow = sbase + (unsigned)((i * (i + 1)) / 2) * sizeof(T);
+            const T *arow = A + (int64_t)i * n;
+            for (int j = lane; j <= i; j += 32) cp_async_elem<T>(drow + (unsigned)j * sizeof(T), arow + j);
         }
         for (int e = tid; e < n * nrhs; e += NT) {
             const int j = e / nrhs, r = e - j * nrhs;
@@ -489,27 +566,54 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *D
     }
     __syncthreads();
 
-    for (int k = 0; k < n; k += kDiagNB) {
-        const int kb = min(kDiagNB, n - k);
-        if (warp == 0) {
-            if (kb == kDiagNB)
-                potrf_diag_block<T, true>(S, n, k, kb, L, Dv, lane, s_info);
-            else
-                potrf_diag_block<T, false>(S, n, k, kb, L, Dv, lane, s_info);
+    const int dv_off = (int)(Dv - S);
+    if constexpr (std::is_same<T, double>::value) {
+        // Look-ahead: while warp 0 factors diagonal block k+16, the other
+        // warps finish block k's trailing update beyond block column k+16
+        // and then solve block k+16's panel column pair by column pair as
+        // warp 0 releases them.  Block column k+16 itself (the band) is
+        // updated first by every warp.
+        auto diag_and_panel = [&](int k) {
+            const int kb = min(kDiagNB, n - k);
+            if (warp == 0) {
+                if (kb == kDiagNB)
+                    potrf_diag_block<T, true, true>(dv_off, n, k, kb, L, lane, s_info, NT);
+                else
+                    potrf_diag_block<T, false, true>(dv_off, n, k, kb, L, lane, s_info, NT);
+            } else {
+                if (k > 0 && k + kDiagNB < n)
+                    trailing_dmma<false>(S, n, R, k - kDiagNB, k + kDiagNB, 1, NW - 1);
+                if (kb == kDiagNB)
+                    panel_trsm_pipe<T, NT, true>(S, n, R, k, kb, Dv, L);
+                else
+                    panel_trsm_pipe<T, NT, false>(S, n, R, k, kb, Dv, L);
+            }
+            __syncthreads();
+        };
+        diag_and_panel(0);
+        for (int k = kDiagNB; k < n; k += kDiagNB) {
+            trailing_dmma<true>(S, n, R, k - kDiagNB, k, 0, NW);  // the band
+            __syncthreads();
+            diag_and_panel(k);
         }
-        __syncthreads();
-
-        // Panel, then the trailing update of the augmented trapezoid.
-        if (kb == kDiagNB)
-            panel_trsm<T, NT, true>(S, n, R, k, kb, Dv, L);
-        else
-            panel_trsm<T, NT, false>(S, n, R, k, kb, Dv, L);
-        __syncthreads();
-        if constexpr (std::is_same<T, double>::value)
-            trailing_dmma<NT>(S, n, R, k, kb);
-        else
+    } else {
+        for (int k = 0; k < n; k += kDiagNB) {
+            const int kb = min(kDiagNB, n - k);
+            if (warp == 0) {
+                if (kb == kDiagNB)
+                    potrf_diag_block<T, true, false>(dv_off, n, k, kb, L, lane, s_info, NT);
+                else
+                    potrf_diag_block<T, false, false>(dv_off, n, k, kb, L, lane, s_info, NT);
+            }
+            __syncthreads();
+            if (kb == kDiagNB)
+                panel_trsm<T, NT, true>(S, n, R, k, kb, Dv, L);
+            else
+                panel_trsm<T, NT, false>(S, n, R, k, kb, Dv, L);
+            __syncthreads();
             trailing_simt<T, NT>(S, n, R, k, kb);
-        __syncthreads();
+            __syncthreads();
+        }
     }
 
     // Rows n..n+nrhs of S now hold y^T = (L^-1 B)^T.  Back substitution
@@ -572,13 +676,15 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *D
 }
 
 // CTAs per SM each thread count is tuned for (register budget).
-__host__ __device__ constexpr int potrf_min_blocks(int nt) { return nt >= 256 ? 3 : (nt >= 128 ? 6 : 12); }
+// Threads of the CTA for matrices above 64: 6 warps, so 3 CTAs per SM (the
+// shared-memory limit at n = 128) leave each thread 112 registers.
+constexpr int kPotrfBigThreads = 192;
+__host__ __device__ constexpr int potrf_min_blocks(int nt) { return nt >= kPotrfBigThreads ? 3 : (nt >= 128 ? 6 : 12); }
 
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
     potrf_potrs_batched_kernel(BatchedPotrfArgs args, int begin, int end, int nmax, int *counter) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *S = reinterpret_cast<T *>(smem_raw);
+    T *S = reinterpret_cast<T *>(bp_smem);
     T *Dv = S + nmax * (nmax + 1) / 2 + args.nrhs * nmax;
     T *xb = Dv + nmax;
     __shared__ int s_item, s_info;
@@ -616,7 +722,7 @@ namespace nmx {
 
 static const int kBucketEdges[] = {32, 64, 96, 128};
 
-static int potrf_threads_for(int nmax) { return nmax <= 32 ? 64 : (nmax <= 64 ? 128 : 256); }
+static int potrf_threads_for(int nmax) { return nmax <= 32 ? 64 : (nmax <= 64 ? 128 : kPotrfBigThreads); }
 
 template <typename T>
 static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s::Bucket &b,
@@ -629,7 +735,7 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
         break;
         NMX_CASE(64)
         NMX_CASE(128)
-        NMX_CASE(256)
+        NMX_CASE(192)
 #undef NMX_CASE
         default:
             set_error("unsupported thread count %d", b.threads);
@@ -670,7 +776,7 @@ static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
         break;
             NMX_OCC(64)
             NMX_OCC(128)
-            NMX_OCC(256)
+            NMX_OCC(192)
 #undef NMX_OCC
         }
         if (per_sm < 1) {
@@ -909,7 +1015,7 @@ struct NoAllocDevice {
     bool ready = false;
     unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
     int sm_count = 0;
-    int per_sm[2] = {0, 0};  // potrf_potrs_batched_kernel<T, 256> at nmax=128, nrhs=8
+    int per_sm[2] = {0, 0};  // potrf_potrs_batched_kernel<T, kPotrfBigThreads> at nmax=128, nrhs=8
 };
 static NoAllocDevice g_noalloc_dev[64];
 static std::mutex g_noalloc_mu;
@@ -934,11 +1040,11 @@ static int noalloc_setup(nmx_ctx ctx, NoAllocDevice **out) {
         d.ready = true;
     }
     if (d.per_sm[ti] == 0) {
-        auto kern = potrf_potrs_batched_kernel<T, 256>;
+        auto kern = potrf_potrs_batched_kernel<T, kPotrfBigThreads>;
         NMX_CUDA_TRY(set_max_dynamic_smem(kern, ctx));
         size_t smem = sizeof(T) * (size_t)potrf_smem_elems(kPotrfMaxN, kPotrfMaxRhs);
         int per_sm = 0;
-        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPotrfBigThreads, smem));
         if (per_sm < 1) {
             set_error("allocation-free kernel does not fit an SM");
             return NMX_ERR_UNSUPPORTED;
@@ -986,7 +1092,7 @@ static int run_noalloc(nmx_ctx ctx, int64_t count, const int32_t *n_host, int nr
     const size_t smem = sizeof(T) * (size_t)potrf_smem_elems(nmax, nrhs);
     const int grid = (int)std::min<int64_t>(count, (int64_t)d->per_sm[sizeof(T) == 8 ? 0 : 1] *
                                                        d->sm_count);
-    potrf_potrs_batched_kernel<T, 256><<<grid, 256, smem, st>>>(args, 0, (int)count, nmax,
+    potrf_potrs_batched_kernel<T, kPotrfBigThreads><<<grid, kPotrfBigThreads, smem, st>>>(args, 0, (int)count, nmax,
                                                                 v.counter);
     NMX_CUDA_TRY(cudaGetLastError());
     return 0;
