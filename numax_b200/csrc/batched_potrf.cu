@@ -675,11 +675,16 @@ __device__ void potrf_potrs_one(const BatchedPotrfArgs &args, int mi, T *S, T *D
     __syncthreads();
 }
 
-// CTAs per SM each thread count is tuned for (register budget).
-// Threads of the CTA for matrices above 64: 6 warps, so 3 CTAs per SM (the
-// shared-memory limit at n = 128) leave each thread 112 registers.
+// CTA shapes by bucket, each with the CTAs per SM its register budget is
+// tuned for: n <= 32: 2 warps x 12; n <= 96: 4 warps x 5; n <= 128: 6 warps
+// x 3 (the shared-memory limit at n = 128), which leaves 96-112 registers a
+// thread in the two large shapes.  Every shape has
+// threads - 32 >= n + nrhs - 16 (one panel row per thread of warps 1..) and
+// threads >= 16 ceil(n / 16) (one block-inverse column per thread).
 constexpr int kPotrfBigThreads = 192;
-__host__ __device__ constexpr int potrf_min_blocks(int nt) { return nt >= kPotrfBigThreads ? 3 : (nt >= 128 ? 6 : 12); }
+__host__ __device__ constexpr int potrf_min_blocks(int nt) {
+    return nt >= 192 ? 3 : (nt >= 128 ? 5 : (nt >= 96 ? 8 : 12));
+}
 
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
@@ -722,7 +727,9 @@ namespace nmx {
 
 static const int kBucketEdges[] = {32, 64, 96, 128};
 
-static int potrf_threads_for(int nmax) { return nmax <= 32 ? 64 : (nmax <= 64 ? 128 : kPotrfBigThreads); }
+static int potrf_threads_for(int nmax) {
+    return nmax <= 32 ? 64 : (nmax <= 96 ? 128 : kPotrfBigThreads);
+}
 
 template <typename T>
 static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s::Bucket &b,
@@ -734,6 +741,7 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
                                                                         b.nmax, counter);    \
         break;
         NMX_CASE(64)
+        NMX_CASE(96)
         NMX_CASE(128)
         NMX_CASE(192)
 #undef NMX_CASE
@@ -760,6 +768,12 @@ template <typename T>
 static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
     for (auto &b : p->buckets) {
         b.threads = potrf_threads_for(b.nmax);
+        if (b.threads - 32 < b.nmax + p->nrhs - std::min(b.nmax, kDiagNB) ||
+            b.threads < kDiagNB * (int)ceil_div(b.nmax, kDiagNB)) {
+            set_error("internal: %d threads cannot cover n=%d with %d right-hand sides", b.threads,
+                      b.nmax, p->nrhs);
+            return NMX_ERR_INTERNAL;
+        }
         b.smem = sizeof(T) * (size_t)potrf_smem_elems(b.nmax, p->nrhs);
         if (b.smem + 64 > ctx->smem_optin) {
             set_error("bucket nmax=%d needs %zu B of shared memory (> %zu)", b.nmax, b.smem,
@@ -775,6 +789,7 @@ static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
             &per_sm, potrf_potrs_batched_kernel<T, NTV>, NTV, b.smem));                        \
         break;
             NMX_OCC(64)
+            NMX_OCC(96)
             NMX_OCC(128)
             NMX_OCC(192)
 #undef NMX_OCC
