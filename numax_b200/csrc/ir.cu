@@ -36,6 +36,8 @@ namespace nmx {
 
 constexpr int kTrsvRB = 64;
 constexpr int kTrsvThreads = 256;
+constexpr int kTrsvPitch = kTrsvRB + 4;
+constexpr size_t kTrsvSmem = (sizeof(double) + sizeof(float)) * kTrsvRB * kTrsvPitch;
 constexpr long long kTrsvSpin = 1ll << 25;
 
 __device__ __forceinline__ int ld_acquire_i32(const int *p) {
@@ -97,14 +99,66 @@ __global__ void __launch_bounds__(kTrsvRB)
 // of the FP32 factor F (n x n, ldf) in place on the FP64 vector x, using the
 // precomputed FP64 inverses Inv of its 64 x 64 diagonal blocks.
 // counter[0]: block ticket, counter[1]: blocks finished, counter[2]: error.
+//
+// A CTA takes 64-row blocks in solve order.  It accumulates the block's row
+// segments against the solution blocks finished so far as they appear, all
+// but the adjacent one (the block finished just before it); meanwhile the
+// F tile against that adjacent block and the block's Inv are copied into
+// shared memory asynchronously.  So once the adjacent block is released,
+// what remains on the chain from block to block is one 64-value read of x,
+// two 64 x 64 products out of shared memory, and the release.
+__device__ __forceinline__ void cp_async_4(unsigned dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(unsigned dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all_() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <bool UPPER>
 __global__ void __launch_bounds__(kTrsvThreads)
     trsv_f32f64_kernel(const float *F, int64_t ldf, int n, const double *Inv, double *x,
                        int *counter) {
-    __shared__ double ys[kTrsvRB];
+    // Dynamic shared memory: Is[64][68] (Inv of this block, FP64) then
+    // Ft[64][68] (the F tile against the adjacent block).  Row pitch 68 with
+    // thread (i, part) reading columns part + 4m keeps both conflict-free.
+    extern __shared__ __align__(16) unsigned char trsv_smem[];
+    auto Is = reinterpret_cast<double(*)[kTrsvPitch]>(trsv_smem);
+    auto Ft = reinterpret_cast<float(*)[kTrsvPitch]>(trsv_smem + sizeof(double) * kTrsvRB * kTrsvPitch);
+    __shared__ double accS[kTrsvRB], xs[kTrsvRB], ys[kTrsvRB];
     __shared__ int s_blk, s_avail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int NB = (n + kTrsvRB - 1) / kTrsvRB;
+    // Column range of the finished blocks with solve-order indices [d0, d1).
+    auto cols = [&](int d0, int d1, int &c0, int &c1) {
+        if (!UPPER) {
+            c0 = d0 * kTrsvRB;
+            c1 = min(n, d1 * kTrsvRB);
+        } else {
+            c0 = (NB - d1) * kTrsvRB;
+            c1 = min(n, (NB - d0) * kTrsvRB);
+        }
+    };
+    // Wait (thread 0, bounded) until more than `done` blocks are finished.
+    auto wait_for = [&](int done) -> int {
+        if (tid == 0) {
+            long long spins = 0;
+            int avail;
+            while ((avail = ld_acquire_i32(&counter[1])) <= done) {
+                if (++spins > kTrsvSpin) {
+                    atomicExch(&counter[2], 1);
+                    avail = -1;
+                    break;
+                }
+                if (spins > 1024) __nanosleep(32);
+            }
+            s_avail = avail;
+        }
+        __syncthreads();
+        const int avail = s_avail;
+        __syncthreads();
+        return avail;
+    };
     for (;;) {
         if (tid == 0) s_blk = atomicAdd(&counter[0], 1);
         __syncthreads();
@@ -113,48 +167,51 @@ __global__ void __launch_bounds__(kTrsvThreads)
         if (ticket >= NB) return;
         const int b = UPPER ? NB - 1 - ticket : ticket;  // row block
         const int r0 = b * kTrsvRB, rows = min(kTrsvRB, n - r0);
-        // Each warp owns rows r0 + 8*warp .. +8; lanes stride the columns.
+        // Inv of this block -> shared (16-byte chunks; rows are 64 doubles).
+        {
+            const unsigned is0 = (unsigned)__cvta_generic_to_shared(&Is[0][0]);
+            const double *inv = Inv + (size_t)b * kTrsvRB * kTrsvRB;
+            for (int e = tid; e < kTrsvRB * kTrsvRB / 2; e += kTrsvThreads) {
+                const int i = e >> 5, c = (e & 31) * 2;
+                cp_async_16(is0 + (unsigned)(i * kTrsvPitch + c) * 8u, inv + i * kTrsvRB + c);
+            }
+        }
+        // Row segments against all finished blocks but the adjacent one:
+        // warp w owns rows 8w..8w+7, lanes stride the columns.
         double acc[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) acc[q] = 0.0;
-        int done = 0;  // column blocks consumed
-        while (done < ticket) {
-            if (tid == 0) {
-                long long spins = 0;
-                int avail;
-                while ((avail = ld_acquire_i32(&counter[1])) <= done) {
-                    if (++spins > kTrsvSpin) {
-                        atomicExch(&counter[2], 1);
-                        avail = -1;
-                        break;
-                    }
-                    if (spins > 1024) __nanosleep(32);
-                }
-                s_avail = avail;
+        int done = 0;
+        while (done < ticket - 1) {
+            const int avail = wait_for(done);
+            if (avail < 0) {
+                cp_async_wait_all_();
+                return;
             }
-            __syncthreads();
-            const int avail = s_avail;
-            __syncthreads();
-            if (avail < 0) return;
-            // Columns of the newly finished blocks (for the upper solve, the
-            // blocks finished so far are the last ones: block NB-1 first).
-            const int nd = min(avail, ticket);
+            const int nd = min(avail, ticket - 1);
             int c0, c1;
-            if (!UPPER) {
-                c0 = done * kTrsvRB;
-                c1 = nd * kTrsvRB;
-            } else {
-                c1 = done == 0 ? n : (NB - done) * kTrsvRB;
-                c0 = (NB - nd) * kTrsvRB;
-            }
+            cols(done, nd, c0, c1);
+            // Two columns per lane (float2 / double2 loads: c0 is a multiple
+            // of 64, rows are 32-byte aligned, x 16-byte aligned), the 8 rows
+            // and 2 iterations in flight: this stream must keep ahead of the
+            // chain of blocks, so it needs memory-level parallelism.
+            int c = c0 + 2 * lane;
+#pragma unroll 2
+            for (; c + 1 < c1; c += 64) {
+                const double2 xv = __ldcg(reinterpret_cast<const double2 *>(x + c));
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int i = 8 * warp + q;
-                if (i < rows) {
-                    const float *row = F + (int64_t)(r0 + i) * ldf;
-                    double s = 0.0;
-                    for (int c = c0 + lane; c < c1; c += 32) s += (double)row[c] * __ldcg(&x[c]);
-                    acc[q] += s;
+                for (int q = 0; q < 8; ++q) {
+                    const int i = min(8 * warp + q, rows - 1);
+                    const float2 f = *reinterpret_cast<const float2 *>(F + (int64_t)(r0 + i) * ldf + c);
+                    acc[q] += (double)f.x * xv.x + (double)f.y * xv.y;
+                }
+            }
+            if (c < c1) {  // an odd last column
+                const double xv = __ldcg(&x[c]);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int i = min(8 * warp + q, rows - 1);
+                    acc[q] += (double)F[(int64_t)(r0 + i) * ldf + c] * xv;
                 }
             }
             done = nd;
@@ -163,27 +220,51 @@ __global__ void __launch_bounds__(kTrsvThreads)
         for (int q = 0; q < 8; ++q) {
             double s = acc[q];
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            const int i = 8 * warp + q;
-            if (lane == 0) ys[i] = i < rows ? x[r0 + i] - s : 0.0;
+            if (lane == 0) accS[8 * warp + q] = s;
+        }
+        // The F tile against the adjacent block -> shared, zero outside.
+        int a0 = 0, a1 = 0;
+        if (ticket > 0) cols(ticket - 1, ticket, a0, a1);
+        {
+            const unsigned ft0 = (unsigned)__cvta_generic_to_shared(&Ft[0][0]);
+            for (int e = tid; e < kTrsvRB * kTrsvRB; e += kTrsvThreads) {
+                const int i = e >> 6, c = e & 63;
+                if (i < rows && a0 + c < a1)
+                    cp_async_4(ft0 + (unsigned)(i * kTrsvPitch + c) * 4u,
+                               F + (int64_t)(r0 + i) * ldf + a0 + c);
+                else
+                    Ft[i][c] = 0.0f;
+            }
+        }
+        if (ticket > 0) {
+            const int avail = wait_for(ticket - 1);
+            if (avail < 0) {
+                cp_async_wait_all_();
+                return;
+            }
+        }
+        if (tid < kTrsvRB) xs[tid] = (a0 + tid < a1) ? __ldcg(&x[a0 + tid]) : 0.0;
+        cp_async_wait_all_();
+        __syncthreads();
+        // ys = x_blk - F_row . x: thread (i, part) sums 16 of the tile's columns.
+        const int i = tid >> 2, part = tid & 3;
+        {
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) s += (double)Ft[i][part + 4 * m] * xs[part + 4 * m];
+            s += __shfl_xor_sync(0xffffffffu, s, 1);
+            s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if (part == 0) ys[i] = i < rows ? x[r0 + i] - accS[i] - s : 0.0;
         }
         __syncthreads();
-        // x_blk = Inv_bb y_blk: warp w rows 8w..8w+7, lanes split the 64 terms.
-        const double *inv = Inv + (size_t)b * kTrsvRB * kTrsvRB;
-        double res[8];
+        // x_blk = Inv ys.
+        {
+            double s = 0.0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = 8 * warp + q;
-            double s = __ldcg(&inv[i * kTrsvRB + lane]) * ys[lane] +
-                       __ldcg(&inv[i * kTrsvRB + lane + 32]) * ys[lane + 32];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            res[q] = s;
-        }
-        if (lane < 8 && 8 * warp + lane < rows) {
-            double v = res[0];
-#pragma unroll
-            for (int q = 1; q < 8; ++q)
-                if (lane == q) v = res[q];
-            x[r0 + 8 * warp + lane] = v;
+            for (int m = 0; m < 16; ++m) s += Is[i][part + 4 * m] * ys[part + 4 * m];
+            s += __shfl_xor_sync(0xffffffffu, s, 1);
+            s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if (part == 0 && i < rows) x[r0 + i] = s;
         }
         __threadfence();
         __syncthreads();
@@ -333,11 +414,19 @@ static int lu_solve_inplace(IrRun &R, double *v) {
     const int want = R.ctx->tune_ir_trsv_ctas > 0 ? (int)R.ctx->tune_ir_trsv_ctas
                                                   : 2 * R.ctx->sm_count;
     const int grid = std::max(1, std::min(NB, want));
+    static bool attr_set[64] = {};
+    if (R.ctx->device < 64 && !attr_set[R.ctx->device]) {
+        NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_f32f64_kernel<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+        NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_f32f64_kernel<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+        attr_set[R.ctx->device] = true;
+    }
     NMX_CUDA_TRY(cudaMemsetAsync(R.counters, 0, 6 * sizeof(int), R.st));
-    trsv_f32f64_kernel<false><<<grid, kTrsvThreads, 0, R.st>>>(R.W, R.ldw, R.n, R.invL, v,
-                                                               R.counters);
-    trsv_f32f64_kernel<true><<<grid, kTrsvThreads, 0, R.st>>>(R.W, R.ldw, R.n, R.invU, v,
-                                                              R.counters + 3);
+    trsv_f32f64_kernel<false><<<grid, kTrsvThreads, kTrsvSmem, R.st>>>(R.W, R.ldw, R.n, R.invL, v,
+                                                                       R.counters);
+    trsv_f32f64_kernel<true><<<grid, kTrsvThreads, kTrsvSmem, R.st>>>(R.W, R.ldw, R.n, R.invU, v,
+                                                                      R.counters + 3);
     NMX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
