@@ -67,7 +67,10 @@ NMX_API int nmx_version(void);
  *   "lu.leaf_ctas"  CTAs of the cooperative LU leaf panel
  *   "lu.cluster"    cap on the CTAs of the cluster LU leaf (-1 = no cap,
  *                   0 = never use the cluster leaf)
- *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop */
+ *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop
+ *   "ir.tc_min"     smallest inner GEMM dimension the mixed-precision LU
+ *                   sends to the tensor cores (-1 = 256; thinner updates
+ *                   run in FP32) */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
 NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
 

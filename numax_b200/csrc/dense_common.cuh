@@ -127,6 +127,7 @@ struct GemmSub {
     cublasHandle_t h = nullptr;
     cudaStream_t st = nullptr;
     int precision = 0;
+    int64_t tc_min = 256;
     void *ws = nullptr;
     size_t ws_bytes = 0;
     int operator()(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
@@ -140,7 +141,10 @@ struct GemmSub {
     }
     int operator()(int64_t m, int64_t n, int64_t k, const float *A, int64_t lda, const float *B,
                    int64_t ldb, float *C, int64_t ldc) const {
-        if (precision)
+        // Tensor cores for the updates with both inner dimensions >= tc_min;
+        // the thin ones near the recursion's leaves stay FP32 (their operand
+        // rounding passes and launches would cost more than they save).
+        if (precision && n >= tc_min && k >= tc_min)
             return tc_gemm_sub_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes);
         cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
         if (s != CUBLAS_STATUS_SUCCESS) {

@@ -506,6 +506,7 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     gs.h = R.h;
     gs.st = st;
     gs.precision = prec == NMX_IR_FP32 ? 0 : (prec == NMX_IR_FP16 ? NMX_PREC_FP16 : NMX_PREC_BF16);
+    if (ctx->tune_ir_tc_min >= 0) gs.tc_min = ctx->tune_ir_tc_min;
     if (gs.precision) {
         const int64_t half = (n / 2 + 31) / 32 * 32;
         gs.ws_bytes = tc_gemm_workspace_bytes(n - half, n - half, half) + 4096;
