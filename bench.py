@@ -272,14 +272,20 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
         del lu
         # BF16 factors + FP64 refinement (GMRES-IR when plain IR stalls).
         res = {"fp64_lu_solve_ms": t64, "fp64_backward_error": be64}
-        for prec, mode in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO),
-                           ("fp16", _lib.NMX_IR_FP16 | _lib.NMX_IR_AUTO)):
+        # bf16: one BF16 rounding per update operand (8 significant bits);
+        # bf16x3: BF16 tensor cores on hi/lo operand splits (~16 bits);
+        # fp16: FP16 operands after power-of-two equilibration (11 bits).
+        # Plain bf16 gets fewer refinement steps: its factors are too coarse
+        # for this order, and the leg only records how far it gets.
+        for prec, mode, iters in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO, 4),
+                                  ("bf16x3", _lib.NMX_IR_BF16X3 | _lib.NMX_IR_AUTO, 30),
+                                  ("fp16", _lib.NMX_IR_FP16 | _lib.NMX_IR_AUTO, 30)):
             x = torch.empty_like(b)
             st = _lib.IrStats()
             e0.record(stream)
             rc = _lib.load().nmx_gesv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
                                              C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
-                                             mode, 1e-14, 30, C.byref(st),
+                                             mode, 1e-14, iters, C.byref(st),
                                              C.c_void_p(stream.cuda_stream))
             e1.record(stream)
             torch.cuda.synchronize(dev)
@@ -294,6 +300,7 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
                         f"{prec}_used_gmres": bool(st.used_gmres),
                         f"{prec}_factor_ms": st.factor_ms, f"{prec}_refine_ms": st.refine_ms,
                         f"{prec}_forward_diff_vs_fp64": fe,
+                        f"{prec}_converged": bool(st.converged),
                         f"speedup_fp64_over_{prec}_ir": t64 / tir})
         out[f"{kappa:.0e}"] = res
         del a, b, s

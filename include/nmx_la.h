@@ -261,6 +261,7 @@ NMX_API int nmx_orgqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, in
 #define NMX_IR_BF16 1
 #define NMX_IR_FP16 2
 #define NMX_IR_FP32 3
+#define NMX_IR_BF16X3 4 /* BF16 tensor cores on hi/lo splits (see NMX_PREC_BF16X3) */
 #define NMX_IR_GMRES 0x10
 #define NMX_IR_AUTO 0x20
 
@@ -279,13 +280,17 @@ typedef struct {
 /* The trailing-update primitive of the mixed-precision factorizations on its
  * own: C[M x N] -= round(A)[M x K] * round(B)[K x N] for fp32 row-major
  * operands, A and B rounded to BF16 (precision 1) or FP16 (precision 2) and
- * the products accumulated in FP32 on the tcgen05 tensor cores.  C must be
+ * the products accumulated in FP32 on the tcgen05 tensor cores.  Precision 3
+ * (BF16X3) splits each operand into BF16 hi + lo (lo = the rounding
+ * residual) and forms hi*hi + hi*lo + lo*hi as one BF16 GEMM over 3K: about
+ * 16 significant bits per operand instead of 8.  C must be
  * 16-byte aligned with ldc a multiple of 4 and ldc >= N rounded up to 8: the
  * update runs on N (and K) rounded up to 8 with zero padding, so C's columns
  * N .. round8(N)-1 are read and written back unchanged.  No numax
  * counterpart (the role MAX's matmul plays in numax/linalg/lu.mojo:646-673). */
 #define NMX_PREC_BF16 1
 #define NMX_PREC_FP16 2
+#define NMX_PREC_BF16X3 3
 NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64_t K, const float *A,
                              int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc,
                              int precision, void *stream);

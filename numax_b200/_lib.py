@@ -65,6 +65,7 @@ SIGNATURES = {
 NMX_IR_BF16 = 1
 NMX_IR_FP16 = 2
 NMX_IR_FP32 = 3
+NMX_IR_BF16X3 = 4
 NMX_IR_GMRES = 0x10
 NMX_IR_AUTO = 0x20
 

@@ -96,6 +96,31 @@ __global__ void round_block_kernel(const float *src, int64_t lds, int rows, int 
     dst[(int64_t)r * ldd + c] = Elem(v);
 }
 
+// BF16X3 operands: A' = [hi(A) | hi(A) | lo(A)] (rows x 3 cols_p) and
+// B' = [hi(B); lo(B); hi(B)] (3 rows_p x cols_p), lo = bf16(x - hi), so one
+// GEMM over 3 K gives hi*hi + hi*lo + lo*hi.  Zero past rows x cols.
+template <bool IS_A>
+__global__ void round_split_bf16_kernel(const float *src, int64_t lds, int rows, int cols,
+                                        int rows_p, int cols_p, cutlass::bfloat16_t *dst,
+                                        int64_t ldd) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)rows_p * cols_p) return;
+    const int r = (int)(e / cols_p), c = (int)(e - (int64_t)r * cols_p);
+    const float v = (r < rows && c < cols) ? src[(int64_t)r * lds + c] : 0.0f;
+    const cutlass::bfloat16_t hi(v);
+    const cutlass::bfloat16_t lo(v - float(hi));
+    if (IS_A) {
+        cutlass::bfloat16_t *d = dst + (int64_t)r * ldd;
+        d[c] = hi;
+        d[cols_p + c] = hi;
+        d[2 * cols_p + c] = lo;
+    } else {
+        dst[(int64_t)r * ldd + c] = hi;
+        dst[(int64_t)(rows_p + r) * ldd + c] = lo;
+        dst[(int64_t)(2 * rows_p + r) * ldd + c] = hi;
+    }
+}
+
 // The GEMM runs on K and N rounded up to multiples of 8 (the 16-byte TMA and
 // epilogue granularity): the padded rows/columns of the 16-bit operands are
 // zero, so the extra columns of C (up to N rounded to 8) get C - 0 and are
@@ -107,7 +132,7 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
                     size_t ws_bytes) {
     if (M <= 0 || N <= 0 || K <= 0) return 0;
     const int64_t Kp = up8(K), Np = up8(N);
-    const size_t need = tc_gemm_workspace_bytes(M, N, K);
+    const size_t need = tc_gemm_workspace_bytes(M, N, K, precision);
     if (need > ws_bytes) {
         set_error("tensor-core update needs %zu B of workspace, have %zu", need, ws_bytes);
         return NMX_ERR_INTERNAL;
@@ -116,8 +141,9 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         set_error("tensor-core update: C must be 16-byte aligned, ldc %% 4 == 0, ldc >= N rounded to 8");
         return NMX_ERR_INTERNAL;
     }
+    const int64_t Kw = precision == NMX_PREC_BF16X3 ? 3 * Kp : Kp;  // K of the 16-bit GEMM
     auto *a16 = static_cast<unsigned char *>(ws);
-    auto *b16 = a16 + ((2 * (size_t)M * Kp + 255) & ~size_t(255));
+    auto *b16 = a16 + ((2 * (size_t)M * Kw + 255) & ~size_t(255));
     const int threads = 256;
     const unsigned ga = (unsigned)ceil_div(M * Kp, threads), gb = (unsigned)ceil_div(Kp * Np, threads);
     int rc;
@@ -130,6 +156,15 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
                                                                     (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
         rc = tc::fp16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st);
+    } else if (precision == NMX_PREC_BF16X3) {
+        auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
+        auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
+        round_split_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                              (int)Kp, a, Kw);
+        round_split_bf16_kernel<false><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N, (int)Kp,
+                                                               (int)Np, b, Np);
+        NMX_CUDA_TRY(cudaGetLastError());
+        rc = tc::bf16::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st);
     } else {
         auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
         auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
@@ -149,8 +184,8 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
     return 0;
 }
 
-size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K) {
-    const int64_t Kp = up8(K), Np = up8(N);
+size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision) {
+    const int64_t Kp = up8(K) * (precision == NMX_PREC_BF16X3 ? 3 : 1), Np = up8(N);
     return ((2 * (size_t)M * Kp + 255) & ~size_t(255)) + 2 * (size_t)Kp * Np + 512;
 }
 
@@ -169,12 +204,13 @@ extern "C" NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64
     NMX_ARG_CHECK(ldb >= std::max<int64_t>(1, N), 8, "ldb < N");
     NMX_ARG_CHECK(C != nullptr || M * N == 0, 9, "C is NULL");
     NMX_ARG_CHECK(ldc >= std::max<int64_t>(1, N), 10, "ldc < N");
-    NMX_ARG_CHECK(precision == NMX_PREC_BF16 || precision == NMX_PREC_FP16, 11,
-                  "precision must be NMX_PREC_BF16 or NMX_PREC_FP16");
+    NMX_ARG_CHECK(precision == NMX_PREC_BF16 || precision == NMX_PREC_FP16 ||
+                      precision == NMX_PREC_BF16X3,
+                  11, "precision must be NMX_PREC_BF16, NMX_PREC_FP16 or NMX_PREC_BF16X3");
     if (M == 0 || N == 0 || K == 0) return 0;
     DeviceGuard g(ctx->device);
     void *ws = nullptr;
-    const size_t bytes = tc_gemm_workspace_bytes(M, N, K);
+    const size_t bytes = tc_gemm_workspace_bytes(M, N, K, precision);
     int rc = ctx->ensure_slot(kWsGemm16, bytes, &ws);
     if (rc) return rc;
     return tc_gemm_sub_f32(static_cast<cudaStream_t>(stream), precision, M, N, K, A, lda, B, ldb, C,

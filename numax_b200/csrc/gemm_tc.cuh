@@ -7,6 +7,7 @@
 #ifndef NMX_PREC_BF16
 #define NMX_PREC_BF16 1
 #define NMX_PREC_FP16 2
+#define NMX_PREC_BF16X3 3
 #endif
 
 namespace nmx {
@@ -19,6 +20,6 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
                     size_t ws_bytes);
 
 // Workspace tc_gemm_sub_f32 needs for an M x N x K update.
-size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K);
+size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision = NMX_PREC_BF16);
 
 }  // namespace nmx

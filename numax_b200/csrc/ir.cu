@@ -338,18 +338,33 @@ __global__ void row_scale_kernel(const double *rowmax, int n, double *rs, int en
     if (i < n) rs[i] = enabled ? pow2_inv(rowmax[i]) : 1.0;
 }
 
-// Column maxima of R A (one thread per column, coalesced across threads).
-__global__ void col_scale_kernel(const double *A, int64_t lda, int n, const double *rs, double *cs,
-                                 int enabled) {
+// Column maxima of R A: a grid of column tiles x row chunks, each thread a
+// column over its chunk's rows (coalesced across the warp, 4 rows in
+// flight), combined with an atomic max on the (nonnegative) bit patterns.
+constexpr int kColChunks = 64;
+__global__ void col_max_kernel(const double *A, int64_t lda, int n, const double *rs,
+                               unsigned long long *cmax) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
-    if (!enabled) {
-        cs[j] = 1.0;
-        return;
+    const int per = (n + kColChunks - 1) / kColChunks;
+    const int i0 = blockIdx.y * per, i1 = min(n, i0 + per);
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    int i = i0;
+    for (; i + 3 < i1; i += 4) {
+        m0 = fmax(m0, fabs(A[(int64_t)i * lda + j] * rs[i]));
+        m1 = fmax(m1, fabs(A[(int64_t)(i + 1) * lda + j] * rs[i + 1]));
+        m2 = fmax(m2, fabs(A[(int64_t)(i + 2) * lda + j] * rs[i + 2]));
+        m3 = fmax(m3, fabs(A[(int64_t)(i + 3) * lda + j] * rs[i + 3]));
     }
-    double m = 0.0;
-    for (int i = 0; i < n; ++i) m = fmax(m, fabs(A[(int64_t)i * lda + j] * rs[i]));
-    cs[j] = pow2_inv(m);
+    for (; i < i1; ++i) m0 = fmax(m0, fabs(A[(int64_t)i * lda + j] * rs[i]));
+    const double m = fmax(fmax(m0, m1), fmax(m2, m3));
+    atomicMax(&cmax[j], (unsigned long long)__double_as_longlong(m));
+}
+
+// Column scales from the column maxima (1 when equilibration is off).
+__global__ void col_scale_kernel(const unsigned long long *cmax, int n, double *cs, int enabled) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) cs[j] = enabled ? pow2_inv(__longlong_as_double((long long)cmax[j])) : 1.0;
 }
 
 // W = (float)(R A C).
@@ -461,8 +476,9 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     NMX_ARG_CHECK(x != nullptr, 6, "x is NULL");
     const int prec = mode & 0xF;
     const bool gmres = (mode & NMX_IR_GMRES) != 0;
-    NMX_ARG_CHECK(prec == NMX_IR_BF16 || prec == NMX_IR_FP16 || prec == NMX_IR_FP32, 7,
-                  "mode must be NMX_IR_BF16/FP16/FP32, optionally | NMX_IR_GMRES");
+    NMX_ARG_CHECK(prec == NMX_IR_BF16 || prec == NMX_IR_FP16 || prec == NMX_IR_FP32 ||
+                      prec == NMX_IR_BF16X3,
+                  7, "mode must be NMX_IR_BF16/FP16/FP32/BF16X3, optionally | NMX_IR_GMRES");
     NMX_ARG_CHECK(tol >= 0.0, 8, "tol < 0");
     NMX_ARG_CHECK(max_iter >= 1 && max_iter <= 10000, 9, "max_iter must be in 1..10000");
     const int n = (int)n64;
@@ -505,11 +521,14 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     GemmSub gs;
     gs.h = R.h;
     gs.st = st;
-    gs.precision = prec == NMX_IR_FP32 ? 0 : (prec == NMX_IR_FP16 ? NMX_PREC_FP16 : NMX_PREC_BF16);
+    gs.precision = prec == NMX_IR_FP32    ? 0
+                   : prec == NMX_IR_FP16   ? NMX_PREC_FP16
+                   : prec == NMX_IR_BF16X3 ? NMX_PREC_BF16X3
+                                           : NMX_PREC_BF16;
     if (ctx->tune_ir_tc_min >= 0) gs.tc_min = ctx->tune_ir_tc_min;
     if (gs.precision) {
         const int64_t half = (n / 2 + 31) / 32 * 32;
-        gs.ws_bytes = tc_gemm_workspace_bytes(n - half, n - half, half) + 4096;
+        gs.ws_bytes = tc_gemm_workspace_bytes(n - half, n - half, half, gs.precision) + 4096;
         rc = ctx->ensure_slot(kWsGemm16, gs.ws_bytes, &gs.ws);
         if (rc) return rc;
     }
@@ -527,7 +546,15 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     row_norms_kernel<<<wb, threads, 0, st>>>(A, lda, n, R.norms, R.rowmax);
     const int equil = prec == NMX_IR_FP16 ? 1 : 0;
     row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
-    col_scale_kernel<<<vb, threads, 0, st>>>(A, lda, n, R.rs, R.cs, equil);
+    if (equil) {
+        // The column maxima go through R.tmp's bits (free until the solve).
+        unsigned long long *cmax = reinterpret_cast<unsigned long long *>(R.tmp);
+        NMX_CUDA_TRY(cudaMemsetAsync(cmax, 0, sizeof(double) * n, st));
+        col_max_kernel<<<dim3(vb, kColChunks), threads, 0, st>>>(A, lda, n, R.rs, cmax);
+        col_scale_kernel<<<vb, threads, 0, st>>>(cmax, n, R.cs, 1);
+    } else {
+        col_scale_kernel<<<vb, threads, 0, st>>>(nullptr, n, R.cs, 0);
+    }
     scale_to_f32_kernel<<<(unsigned)ceil_div((int64_t)n * n, threads), threads, 0, st>>>(
         A, lda, n, R.rs, R.cs, R.W, R.ldw);
     NMX_CUDA_TRY(cudaGetLastError());

@@ -209,7 +209,8 @@ def qr_factor(a) -> QR:
     return QR(f, tau)
 
 
-_IR_MODES = {"bf16": _lib.NMX_IR_BF16, "fp16": _lib.NMX_IR_FP16, "fp32": _lib.NMX_IR_FP32}
+_IR_MODES = {"bf16": _lib.NMX_IR_BF16, "fp16": _lib.NMX_IR_FP16, "fp32": _lib.NMX_IR_FP32,
+             "bf16x3": _lib.NMX_IR_BF16X3}
 
 
 def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: float = 1e-14,

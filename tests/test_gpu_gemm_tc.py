@@ -29,3 +29,30 @@ def test_gemm_sub_tc(prec, m, n, k):
     torch.cuda.synchronize()
     err = float((C[:, :n].double() - want).norm() / want.norm())
     assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 256, 64), (1000, 513, 257), (37, 64, 16)])
+def test_gemm_sub_bf16x3_reaches_fp32_level(m, n, k):
+    """Precision 3 (BF16 hi/lo splits, hi*hi + hi*lo + lo*hi) against the
+    FP64 product of the unrounded FP32 operands: the dropped lo*lo term and
+    the FP32 accumulation leave about 1e-5 relative at most, where one BF16
+    rounding of the operands alone costs ~3e-3."""
+    from numax_b200 import _lib
+    g = torch.Generator(device="cuda")
+    g.manual_seed(m * 13 + n * 5 + k)
+    lda, ldb, ldc = k + 3, n + 1, (n + 7) // 8 * 8
+    A = torch.randn((m, lda), generator=g, device="cuda", dtype=torch.float32)
+    B = torch.randn((k, ldb), generator=g, device="cuda", dtype=torch.float32)
+    C = torch.randn((m, ldc), generator=g, device="cuda", dtype=torch.float32)
+    prod = A[:, :k].double() @ B[:, :n].double()
+    want = C[:, :n].double() - prod
+    rc = _lib.load().nmx_gemm_sub_f32(_lib.context(0), m, n, k, A.data_ptr(), lda, B.data_ptr(),
+                                       ldb, C.data_ptr(), ldc, 3,
+                                       torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    err = float((C[:, :n].double() - want).norm() / prod.norm())
+    assert err <= 2e-5, err
+    one = float(((A[:, :k].bfloat16().double() @ B[:, :n].bfloat16().double()) - prod).norm()
+                / prod.norm())
+    assert err < one / 20, (err, one)

@@ -29,11 +29,12 @@ def berr(a, x, b):
 
 
 # Converging cases: 16-bit factors with plain/auto refinement at kappa 1e2,
-# FP16 factors with GMRES-IR at 1e5, FP32 factors through 1e8.  BF16 factors
-# at kappa >= 1e5 are reported by the benchmark, not asserted here.
+# FP16 factors with GMRES-IR at 1e5, FP32 factors through 1e8, split-BF16
+# (bf16x3) updates through 1e5.  Single-BF16 factors at kappa >= 1e5 are
+# reported by the benchmark, not asserted here.
 @pytest.mark.parametrize("precision,gmres,kappa", [
     ("bf16", "auto", 1e2), ("fp16", "auto", 1e2), ("fp16", True, 1e5),
-    ("fp32", "auto", 1e5), ("fp32", True, 1e8),
+    ("fp32", "auto", 1e5), ("fp32", True, 1e8), ("bf16x3", "auto", 1e2), ("bf16x3", "auto", 1e5),
 ])
 def test_ir_reaches_fp64_backward_error(precision, gmres, kappa):
     from numax_b200 import linalg
