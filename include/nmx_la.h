@@ -114,6 +114,32 @@ NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, cons
                                         float *L, const float *B, float *X, int32_t *info,
                                         void *stream);
 
+/* Autotuner (no numax counterpart; numax launches one problem per thread at
+ * a compile-time n): times every CTA shape (64, 96, 128, 192 threads) that
+ * covers each size bucket of the plan on these buffers -- the bucket's
+ * persistent kernel alone, best of `reps` runs, CUDA events -- and keeps the
+ * fastest in the plan.  Every run computes the whole bucket, so L, X and
+ * info hold a valid result afterwards.  A and B as for the run entry points
+ * of the plan's dtype.  Synchronizes `stream`.  reps: 1..100. */
+NMX_API int nmx_batched_plan_autotune(nmx_ctx ctx, nmx_batched_plan plan, const void *A, void *L,
+                                      const void *B, void *X, int32_t *info, int reps,
+                                      void *stream);
+/* The plan's schedule: per bucket (largest n first) its largest n, threads
+ * per CTA and CTAs launched; up to max_buckets entries, *nbuckets = count. */
+NMX_API int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *threads,
+                                      int32_t *ctas, int max_buckets, int32_t *nbuckets);
+/* Run the plan through a CUDA graph (no numax counterpart): the first call
+ * with a given set of buffers captures the plan's launches (counter reset +
+ * one persistent kernel per bucket) on an internal stream into a graph kept
+ * in the plan; later calls with the same buffers replay it on `stream` with
+ * one launch.  New buffers or an autotune re-capture. */
+NMX_API int nmx_potrf_potrs_batched_graph_f64(nmx_ctx ctx, nmx_batched_plan plan, const double *A,
+                                              double *L, const double *B, double *X,
+                                              int32_t *info, void *stream);
+NMX_API int nmx_potrf_potrs_batched_graph_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A,
+                                              float *L, const float *B, float *X, int32_t *info,
+                                              void *stream);
+
 /* Allocation-free form of nmx_potrf_potrs_batched_f64, with no counterpart
  * in the reference (numax allocates per call).  For callers that cannot
  * allocate device memory -- a host runtime whose allocator already owns the

@@ -41,6 +41,10 @@ SIGNATURES = {
     "nmx_batched_plan_sizes": (ci, [vp, C.POINTER(i64), C.POINTER(i64)]),
     "nmx_potrf_potrs_batched_f64": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "nmx_potrf_potrs_batched_f32": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "nmx_batched_plan_autotune": (ci, [vp, vp, vp, vp, vp, vp, vp, ci, vp]),
+    "nmx_batched_plan_schedule": (ci, [vp, vp, vp, vp, ci, vp]),
+    "nmx_potrf_potrs_batched_graph_f64": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "nmx_potrf_potrs_batched_graph_f32": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "nmx_syevj_batched_plan": (ci, [vp, i64, vp, C.POINTER(vp)]),
     "nmx_syevj_plan_destroy": (ci, [vp]),
     "nmx_syevj_plan_sizes": (ci, [vp, C.POINTER(i64), C.POINTER(i64)]),

@@ -105,11 +105,7 @@ class CholeskySolveBatch:
                 pass
             self._plan = None
 
-    def run(self, A: torch.Tensor, B: torch.Tensor | None, X: torch.Tensor | None = None,
-            info: torch.Tensor | None = None, L: torch.Tensor | None = None):
-        """Enqueue on the current stream.  The factors' lower triangles go to
-        L (default: A itself, in place; the upper triangles are not written).
-        Returns (L, X, info) without synchronizing."""
+    def _operands(self, A, B, X, info, L):
         _check_tensor("A", A, self.dtype, self.a_elems, self.device)
         if L is None:
             L = A
@@ -122,10 +118,40 @@ class CholeskySolveBatch:
         if info is None:
             info = torch.empty(self.count, dtype=torch.int32, device=self.device)
         _check_tensor("info", info, torch.int32, self.count, self.device)
-        _lib.call(f"nmx_potrf_potrs_batched_{self._suffix}", self._ctx, self._plan, A.data_ptr(),
-                  L.data_ptr(), B.data_ptr() if self.nrhs else None,
-                  X.data_ptr() if self.nrhs else None, info.data_ptr(), _stream_ptr(self.device))
         return L, X, info
+
+    def _ptrs(self, A, B, X, info, L):
+        return (A.data_ptr(), L.data_ptr(), B.data_ptr() if self.nrhs else None,
+                X.data_ptr() if self.nrhs else None, info.data_ptr())
+
+    def run(self, A: torch.Tensor, B: torch.Tensor | None, X: torch.Tensor | None = None,
+            info: torch.Tensor | None = None, L: torch.Tensor | None = None, graph: bool = False):
+        """Enqueue on the current stream.  The factors' lower triangles go to
+        L (default: A itself, in place; the upper triangles are not written).
+        graph=True replays a CUDA graph of the plan's launches (captured the
+        first time these buffers are seen).  Returns (L, X, info) without
+        synchronizing."""
+        L, X, info = self._operands(A, B, X, info, L)
+        fn = f"nmx_potrf_potrs_batched_{'graph_' if graph else ''}{self._suffix}"
+        _lib.call(fn, self._ctx, self._plan, *self._ptrs(A, B, X, info, L),
+                  _stream_ptr(self.device))
+        return L, X, info
+
+    def autotune(self, A, B, X=None, info=None, L=None, reps: int = 3):
+        """Time every CTA shape that covers each size bucket on these
+        buffers and keep the fastest (synchronizes; the outputs hold a valid
+        result afterwards).  Returns the schedule."""
+        L, X, info = self._operands(A, B, X, info, L)
+        _lib.call("nmx_batched_plan_autotune", self._ctx, self._plan, *self._ptrs(A, B, X, info, L),
+                  int(reps), _stream_ptr(self.device))
+        return self.schedule()
+
+    def schedule(self):
+        """Per size bucket (largest n first): n_max, threads per CTA, CTAs."""
+        nmax, thr, ctas = (C.c_int32 * 8)(), (C.c_int32 * 8)(), (C.c_int32 * 8)()
+        nb = C.c_int32()
+        _lib.call("nmx_batched_plan_schedule", self._plan, nmax, thr, ctas, 8, C.byref(nb))
+        return [{"n_max": nmax[i], "threads": thr[i], "ctas": ctas[i]} for i in range(nb.value)]
 
     def __call__(self, A, B, X=None, info=None, L=None):
         """Synchronous, like numax: factor (in place unless L is given),

@@ -721,6 +721,9 @@ struct nmx_batched_plan_s {
         size_t smem;
     };
     std::vector<Bucket> buckets;
+    // CUDA graph of one run, for the buffers in graph_key (A, L, B, X, info).
+    cudaGraphExec_t graph = nullptr;
+    const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace nmx {
@@ -764,12 +767,41 @@ static cudaError_t set_max_dynamic_smem(K kernel, nmx_ctx ctx) {
                                 (int)(ctx->smem_optin - fa.sharedSizeBytes));
 }
 
+// Whether a CTA of `threads` covers a bucket of matrices up to nmax with nrhs
+// right-hand sides (one panel row per thread of warps 1.., one
+// block-inverse column per thread).
+static bool shape_covers(int threads, int nmax, int nrhs) {
+    return threads - 32 >= nmax + nrhs - std::min(nmax, kDiagNB) &&
+           threads >= kDiagNB * (int)ceil_div(nmax, kDiagNB);
+}
+
+// CTAs per SM of the kernel with `threads` at `smem` bytes (0: does not fit).
+template <typename T>
+static int shape_occupancy(nmx_ctx ctx, int threads, size_t smem, int *per_sm) {
+    *per_sm = 0;
+    switch (threads) {
+#define NMX_OCC(NTV)                                                                           \
+    case NTV:                                                                                  \
+        NMX_CUDA_TRY(set_max_dynamic_smem(potrf_potrs_batched_kernel<T, NTV>, ctx));        \
+        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                            \
+            per_sm, potrf_potrs_batched_kernel<T, NTV>, NTV, smem));                           \
+        break;
+        NMX_OCC(64)
+        NMX_OCC(96)
+        NMX_OCC(128)
+        NMX_OCC(192)
+#undef NMX_OCC
+        default:
+            break;
+    }
+    return 0;
+}
+
 template <typename T>
 static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
     for (auto &b : p->buckets) {
         b.threads = potrf_threads_for(b.nmax);
-        if (b.threads - 32 < b.nmax + p->nrhs - std::min(b.nmax, kDiagNB) ||
-            b.threads < kDiagNB * (int)ceil_div(b.nmax, kDiagNB)) {
+        if (!shape_covers(b.threads, b.nmax, p->nrhs)) {
             set_error("internal: %d threads cannot cover n=%d with %d right-hand sides", b.threads,
                       b.nmax, p->nrhs);
             return NMX_ERR_INTERNAL;
@@ -781,19 +813,8 @@ static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
             return NMX_ERR_UNSUPPORTED;
         }
         int per_sm = 0;
-        switch (b.threads) {
-#define NMX_OCC(NTV)                                                                           \
-    case NTV:                                                                                  \
-        NMX_CUDA_TRY(set_max_dynamic_smem(potrf_potrs_batched_kernel<T, NTV>, ctx));        \
-        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                            \
-            &per_sm, potrf_potrs_batched_kernel<T, NTV>, NTV, b.smem));                        \
-        break;
-            NMX_OCC(64)
-            NMX_OCC(96)
-            NMX_OCC(128)
-            NMX_OCC(192)
-#undef NMX_OCC
-        }
+        int rc = shape_occupancy<T>(ctx, b.threads, b.smem, &per_sm);
+        if (rc) return rc;
         if (per_sm < 1) {
             set_error("bucket nmax=%d does not fit on an SM (smem %zu)", b.nmax, b.smem);
             return NMX_ERR_UNSUPPORTED;
@@ -826,6 +847,115 @@ static int run_potrf_potrs(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L,
         int rc = launch_bucket<T>(args, plan->buckets[bi], plan->d_counters + bi, st);
         if (rc) return rc;
     }
+    return 0;
+}
+
+// Time every covering CTA shape of every bucket on these buffers (each
+// bucket's kernel alone, best of `reps` runs, CUDA events on `st`) and keep
+// the fastest.  Every run computes the full bucket, so the outputs hold a
+// valid result afterwards.
+template <typename T>
+static int autotune(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const T *B, T *X,
+                    int32_t *info, int reps, cudaStream_t st) {
+    BatchedPotrfArgs args{plan->d_order, plan->d_n, plan->d_aoff, plan->d_boff, A,
+                          L,             B,         X,            info,         plan->nrhs};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NMX_CUDA_TRY(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        NMX_CUDA_TRY(ce);
+    }
+    int rc = 0;
+    for (size_t bi = 0; bi < plan->buckets.size() && !rc; ++bi) {
+        auto best = plan->buckets[bi];
+        float best_ms = 3.4e38f;
+        for (int threads : {64, 96, 128, 192}) {
+            auto cand = plan->buckets[bi];
+            if (!shape_covers(threads, cand.nmax, plan->nrhs)) continue;
+            cand.threads = threads;
+            int per_sm = 0;
+            rc = shape_occupancy<T>(ctx, threads, cand.smem, &per_sm);
+            if (rc) break;
+            if (per_sm < 1) continue;
+            cand.grid = (int)std::min<int64_t>(cand.end - cand.begin, (int64_t)per_sm * ctx->sm_count);
+            float ms = 3.4e38f;
+            for (int r = 0; r < std::max(1, reps) && !rc; ++r) {
+                if (cudaMemsetAsync(plan->d_counters + bi, 0, sizeof(int32_t), st) != cudaSuccess ||
+                    cudaEventRecord(e0, st) != cudaSuccess) {
+                    set_error("autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                    rc = NMX_ERR_CUDA;
+                    break;
+                }
+                rc = launch_bucket<T>(args, cand, plan->d_counters + bi, st);
+                float t = 0.f;
+                if (!rc && (cudaEventRecord(e1, st) != cudaSuccess ||
+                            cudaEventSynchronize(e1) != cudaSuccess ||
+                            cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)) {
+                    set_error("autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                    rc = NMX_ERR_CUDA;
+                }
+                ms = std::min(ms, t);
+            }
+            if (rc) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = cand;
+            }
+        }
+        plan->buckets[bi] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (plan->graph) {  // the captured shapes are stale
+        cudaGraphExecDestroy(plan->graph);
+        plan->graph = nullptr;
+    }
+    return rc;
+}
+
+// Run the plan through a CUDA graph of its launches (counter reset and one
+// persistent kernel per bucket), captured on an internal stream the first
+// time these buffers are seen and replayed on `stream` after that.
+template <typename T>
+static int run_graph(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const T *B, T *X,
+                     int32_t *info, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    if (plan->count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    const void *key[5] = {A, L, B, X, info};
+    if (!plan->graph || !std::equal(key, key + 5, plan->graph_key)) {
+        if (plan->graph) {
+            cudaGraphExecDestroy(plan->graph);
+            plan->graph = nullptr;
+        }
+        cudaStream_t cs = nullptr;
+        NMX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        int rc = 0;
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            set_error("graph capture: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = NMX_ERR_CUDA;
+        } else {
+            rc = run_potrf_potrs<T>(ctx, plan, A, L, B, X, info, cs);
+            cudaError_t e = cudaStreamEndCapture(cs, &graph);
+            if (!rc && e != cudaSuccess) {
+                set_error("graph capture: %s", cudaGetErrorString(e));
+                rc = NMX_ERR_CUDA;
+            }
+        }
+        if (!rc && cudaGraphInstantiate(&plan->graph, graph, 0) != cudaSuccess) {
+            set_error("graph instantiate: %s", cudaGetErrorString(cudaGetLastError()));
+            plan->graph = nullptr;
+            rc = NMX_ERR_CUDA;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (rc) return rc;
+        std::copy(key, key + 5, plan->graph_key);
+    }
+    NMX_CUDA_TRY(cudaGraphLaunch(plan->graph, static_cast<cudaStream_t>(stream)));
     return 0;
 }
 
@@ -913,6 +1043,7 @@ int nmx_potrf_potrs_batched_plan(nmx_ctx ctx, int dtype, int64_t count, const in
 int nmx_batched_plan_destroy(nmx_batched_plan plan) {
     if (!plan) return 0;
     nmx::DeviceGuard g(plan->device);
+    if (plan->graph) cudaGraphExecDestroy(plan->graph);
     if (plan->dev) cudaFree(plan->dev);
     delete plan;
     return 0;
@@ -933,6 +1064,53 @@ int nmx_potrf_potrs_batched_f64(nmx_ctx ctx, nmx_batched_plan plan, const double
 int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A, float *L,
                                 const float *B, float *X, int32_t *info, void *stream) {
     return nmx::run_potrf_potrs<float>(ctx, plan, A, L, B, X, info, stream);
+}
+
+int nmx_batched_plan_autotune(nmx_ctx ctx, nmx_batched_plan plan, const void *A, void *L,
+                              const void *B, void *X, int32_t *info, int reps, void *stream) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    NMX_ARG_CHECK(A != nullptr || plan->count == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(L != nullptr || plan->count == 0, 4, "L is NULL");
+    NMX_ARG_CHECK(B != nullptr || plan->nrhs == 0 || plan->count == 0, 5, "B is NULL");
+    NMX_ARG_CHECK(X != nullptr || plan->nrhs == 0 || plan->count == 0, 6, "X is NULL");
+    NMX_ARG_CHECK(info != nullptr || plan->count == 0, 7, "info is NULL");
+    NMX_ARG_CHECK(reps >= 1 && reps <= 100, 8, "reps must be in 1..100");
+    if (plan->count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->dtype == NMX_F64)
+        return autotune<double>(ctx, plan, static_cast<const double *>(A), static_cast<double *>(L),
+                                static_cast<const double *>(B), static_cast<double *>(X), info,
+                                reps, st);
+    return autotune<float>(ctx, plan, static_cast<const float *>(A), static_cast<float *>(L),
+                           static_cast<const float *>(B), static_cast<float *>(X), info, reps, st);
+}
+
+int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *threads,
+                              int32_t *ctas, int max_buckets, int32_t *nbuckets) {
+    NMX_ARG_CHECK(plan != nullptr, 1, "plan is NULL");
+    NMX_ARG_CHECK(max_buckets >= 0, 5, "max_buckets < 0");
+    const int nb = (int)plan->buckets.size();
+    for (int i = 0; i < nb && i < max_buckets; ++i) {
+        if (nmax) nmax[i] = plan->buckets[i].nmax;
+        if (threads) threads[i] = plan->buckets[i].threads;
+        if (ctas) ctas[i] = plan->buckets[i].grid;
+    }
+    if (nbuckets) *nbuckets = nb;
+    return 0;
+}
+
+int nmx_potrf_potrs_batched_graph_f64(nmx_ctx ctx, nmx_batched_plan plan, const double *A,
+                                      double *L, const double *B, double *X, int32_t *info,
+                                      void *stream) {
+    return nmx::run_graph<double>(ctx, plan, A, L, B, X, info, stream);
+}
+
+int nmx_potrf_potrs_batched_graph_f32(nmx_ctx ctx, nmx_batched_plan plan, const float *A, float *L,
+                                      const float *B, float *X, int32_t *info, void *stream) {
+    return nmx::run_graph<float>(ctx, plan, A, L, B, X, info, stream);
 }
 
 }  // extern "C"

@@ -130,3 +130,37 @@ def test_batched_rejects_bad_arguments():
     with pytest.raises(ValueError):
         plan(torch.zeros(10, dtype=torch.float64, device="cuda"),
              torch.zeros(9, dtype=torch.float64, device="cuda"))
+
+
+def test_batched_autotune_and_graph_replay(oracle):
+    """The autotuner picks a covering CTA shape per size bucket and leaves
+    valid outputs; a CUDA-graph replay of the plan gives bit-identical
+    results to the direct launches, and re-captures for new buffers."""
+    import numax_b200 as nb
+    ns = np.array([5, 128, 33, 100, 64, 17, 96, 120, 8, 70], dtype=np.int32)
+    nrhs = 4
+    A, B = make_batch(ns, nrhs, np.float64, seed=21)
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, nrhs)
+    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float64)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    L = torch.empty_like(dA)
+    X = torch.empty_like(dB)
+    info = torch.empty(len(ns), dtype=torch.int32, device="cuda")
+    sched = plan.autotune(dA, dB, X, info, L, reps=2)
+    assert len(sched) == 4 and all(s["threads"] in (64, 96, 128, 192) and s["ctas"] >= 1
+                                   for s in sched)
+    torch.cuda.synchronize()
+    assert int(info.abs().sum()) == 0
+    assert relerr(X.cpu().numpy(), wantX) <= 1e-12
+    # Zero-filled L buffers: the plan writes only the lower triangles.
+    L1, X1, _ = plan.run(dA, dB, torch.empty_like(dB), info, torch.zeros_like(dA))
+    X1, L1 = X1.clone(), L1.clone()
+    Lg, Xg = torch.zeros_like(dA), torch.empty_like(dB)
+    for _ in range(2):  # capture, then replay
+        plan.run(dA, dB, Xg, info, Lg, graph=True)
+        torch.cuda.synchronize()
+        assert torch.equal(Xg, X1) and torch.equal(Lg, L1)
+    Xh = torch.empty_like(dB)  # new buffers: a new capture
+    plan.run(dA, dB, Xh, info, Lg, graph=True)
+    torch.cuda.synchronize()
+    assert torch.equal(Xh, X1)
