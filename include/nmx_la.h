@@ -67,6 +67,7 @@ NMX_API int nmx_version(void);
  *   "lu.leaf_ctas"  CTAs of the cooperative LU leaf panel
  *   "lu.cluster"    cap on the CTAs of the cluster LU leaf (-1 = no cap,
  *                   0 = never use the cluster leaf)
+ *   "lu.leaf_w"     widest LU leaf panel in columns (0 = 32; 8..64)
  *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop
  *   "ir.tc_min"     smallest inner GEMM dimension the mixed-precision LU
  *                   sends to the tensor cores (-1 = 256; thinner updates

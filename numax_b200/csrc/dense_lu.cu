@@ -492,6 +492,7 @@ struct LuRun {
     LeafScratch<T> sc;
     int max_ctas;
     int cluster;  // CTAs per cluster for the cluster leaf (0: not available)
+    int max_w;    // widest leaf (multiple of 8, <= kLeafMax)
 };
 
 // Shared-memory bytes the cluster leaf needs for an m-row panel of width w.
@@ -501,14 +502,15 @@ static size_t cluster_leaf_smem(int m, int w, int cs) {
     return sizeof(T) * (rpc * (size_t)(w | 1) + 6 * (size_t)kLeafMax);
 }
 
-// Widest leaf (multiple of 8, <= kLeafW) the cluster leaf can hold for an
-// m-row panel; 0 if even 8 columns do not fit (the cooperative leaf runs).
+// Widest leaf (multiple of 8, <= R.max_w) the cluster leaf can hold for an
+// m-row panel; R.max_w if even 8 columns do not fit (the cooperative leaf
+// runs).
 template <typename T>
 static int leaf_width(const LuRun<T> &R, int m) {
-    if (R.cluster <= 0) return kLeafW;
-    for (int w = kLeafW; w >= 8; w -= 8)
+    if (R.cluster <= 0) return R.max_w;
+    for (int w = R.max_w; w >= 8; w -= 8)
         if (cluster_leaf_smem<T>(m, w, R.cluster) + 2048 <= R.ctx->smem_optin) return w;
-    return kLeafW;
+    return R.max_w;
 }
 
 template <typename T>
@@ -725,7 +727,10 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
             }
         cluster = cs;
     }
-    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas, cluster};
+    const int max_w = ctx->tune_lu_leaf_w > 0
+                          ? (int)std::min<int64_t>(kLeafMax, ctx->tune_lu_leaf_w / 8 * 8)
+                          : kLeafW;
+    LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas, cluster, std::max(8, max_w)};
     return getrf2<T>(R, 0, (int)n);
 }
 

@@ -67,6 +67,7 @@ struct nmx_context {
     int64_t tune_lu_leaf_ctas = 0;    // CTAs of the cooperative LU leaf panel
     int64_t tune_ir_trsv_ctas = 0;    // CTAs of the persistent triangular solves
     int64_t tune_lu_cluster = -1;     // cap on the LU cluster leaf's CTAs (-1: none, 0: off)
+    int64_t tune_lu_leaf_w = 0;       // widest LU leaf panel (0: 32; multiple of 8, <= 64)
     int64_t tune_ir_tc_min = -1;      // smallest GEMM inner dimension on the tensor cores (-1: 256)
     // Grow-only named device buffers, one per use, kept for the context's life.
     static constexpr int kSlots = 8;
