@@ -308,6 +308,83 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
     return out
 
 
+def run_dense(dev, n=8192, nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
+    """The dense factorizations at the single-matrix configs: FP64 LU + 16-RHS
+    solve and FP64 Cholesky + 16-RHS solve at order n, FP32 Householder QR
+    (geqrf, then orgqr) of qr_m x qr_n.  Device time (CUDA events) of one
+    call each after a warm-up call; rates against FP64 37 TF/s and FP32
+    75 TF/s nominal (MEASURED_PEAKS.json has no FP64/FP32 figure)."""
+    import torch
+    from numax_b200 import _lib
+    ctx = _lib.context(dev.index)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 31)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1)
+
+    out = {"n": n, "nrhs": nrhs}
+    a = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+    b = torch.randn((n, nrhs), generator=gen, dtype=torch.float64, device=dev)
+    lu, x = torch.empty_like(a), torch.empty_like(b)
+    piv = torch.empty(n, dtype=torch.int32, device=dev)
+    info = torch.empty(1, dtype=torch.int32, device=dev)
+
+    def lu_solve():
+        lu.copy_(a)
+        x.copy_(b)
+        _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(), sp)
+        _lib.call("nmx_getrs_f64", ctx, n, nrhs, lu.data_ptr(), n, piv.data_ptr(), x.data_ptr(),
+                  nrhs, sp)
+    ms = timed(lu_solve)
+    fl = 2 * n ** 3 / 3 + 2 * n * n * nrhs
+    berr = float((b - a @ x).abs().max() / (a.abs().sum(1).max() * x.abs().max() + b.abs().max()))
+    out["lu_f64"] = {"ms": ms, "tflops": fl / ms / 1e9, "fp64_frac_nominal": fl / ms / 1e9 / 37.0,
+                     "backward_error": berr}
+    g = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+    spd = g @ g.T / n + torch.eye(n, dtype=torch.float64, device=dev)
+    del g
+
+    def chol_solve():
+        lu.copy_(spd)
+        x.copy_(b)
+        _lib.call("nmx_potrf_f64", ctx, n, lu.data_ptr(), n, info.data_ptr(), sp)
+        _lib.call("nmx_potrs_f64", ctx, n, nrhs, lu.data_ptr(), n, x.data_ptr(), nrhs, sp)
+    ms = timed(chol_solve)
+    fl = n ** 3 / 3 + 2 * n * n * nrhs
+    berr = float((b - spd @ x).abs().max() / (spd.abs().sum(1).max() * x.abs().max() + b.abs().max()))
+    out["cholesky_f64"] = {"ms": ms, "tflops": fl / ms / 1e9, "fp64_frac_nominal": fl / ms / 1e9 / 37.0,
+                           "backward_error": berr}
+    del a, b, lu, x, spd
+    q = torch.randn((qr_m, qr_n), generator=gen, dtype=torch.float32, device=dev)
+    f = torch.empty_like(q)
+    qq = torch.empty_like(q)
+    tau = torch.empty(qr_n, dtype=torch.float32, device=dev)
+
+    def geqrf():
+        f.copy_(q)
+        _lib.call("nmx_geqrf_f32", ctx, qr_m, qr_n, f.data_ptr(), qr_n, tau.data_ptr(), sp)
+    ms = timed(geqrf)
+    fl = 2 * qr_m * qr_n ** 2 - 2 * qr_n ** 3 / 3
+    ms_q = timed(lambda: _lib.call("nmx_orgqr_f32", ctx, qr_m, qr_n, f.data_ptr(), qr_n,
+                                   tau.data_ptr(), qq.data_ptr(), qr_n, sp))
+    orth = float((qq.T.double() @ qq.double() - torch.eye(qr_n, dtype=torch.float64, device=dev)).abs().max())
+    out["qr_f32"] = {"m": qr_m, "n": qr_n, "geqrf_ms": ms, "geqrf_tflops": fl / ms / 1e9,
+                     "fp32_frac_nominal": fl / ms / 1e9 / 75.0, "orgqr_ms": ms_q,
+                     "q_orthogonality_err": orth}
+    return out
+
+
 def make_eigh_batch(count, dev, seed=SEED):
     """Half harmonic-well Hamiltonians (n = 24 on [-4, 4], omega ~ U[0.5, 2];
     diagonal 1/dx^2 + omega^2 x^2 / 2, off-diagonal -1/(2 dx^2)) and half
@@ -532,6 +609,13 @@ def run_ours(args):
         except Exception as exc:
             eigh = {"error": f"{type(exc).__name__}: {exc}"}
 
+    dense = None
+    if world == 1 and args.dense:
+        try:
+            dense = run_dense(dev)
+        except Exception as exc:
+            dense = {"error": f"{type(exc).__name__}: {exc}"}
+
     lu_ir = None
     if world == 1 and args.lu_n > 0:
         try:
@@ -573,6 +657,7 @@ def run_ours(args):
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
         "eigh": eigh,
+        "dense": dense,
         "lu_ir": lu_ir,
     }
     print(json.dumps(line), flush=True)
@@ -593,6 +678,8 @@ def main():
     ap.add_argument("--lu-kappas", default="1e2",
                     help="comma-separated condition numbers for the comparison")
     ap.add_argument("--only-lu", action="store_true", help="run only the LU/IR comparison")
+    ap.add_argument("--no-dense", dest="dense", action="store_false",
+                    help="skip the dense LU/Cholesky/QR leg")
     ap.add_argument("--eigh-count", type=int, default=65536,
                     help="matrices in the batched Jacobi eigh leg (0 skips it)")
     args = ap.parse_args()
