@@ -39,9 +39,12 @@ __global__ void potrf_leaf_kernel(T *A, int64_t lda, int c, int w, int32_t *info
                 if (first_bad == 0) first_bad = c + j + 1;
                 d = pivot_floor<T>::value;
             }
-            const T root = sqrt(d);
-            if (lane == j) a[j] = root;
-            if (lane > j) a[j] = a[j] / root;
+            // 1/l_jj once per column: the column scales by a product
+            // instead of a division on every lane (the pivot chain is
+            // d -> rsqrt -> scale -> update).
+            const T inv = rsqrt(d);
+            if (lane == j) a[j] = d * inv;
+            if (lane > j) a[j] = a[j] * inv;
             const T lij = a[j];
 #pragma unroll
             for (int cc = j + 1; cc < kCholLeaf; ++cc) {
@@ -63,10 +66,15 @@ __global__ void potrf_leaf_kernel(T *A, int64_t lda, int c, int w, int32_t *info
 template <typename T>
 __global__ void trsm_right_lt_leaf_kernel(T *A, int64_t lda, int c, int w, int r0, int r1) {
     __shared__ T Ls[kCholLeaf][kCholLeaf + 1];
+    __shared__ T inv_d[kCholLeaf];
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         int i = e / w, j = e - i * w;
         Ls[i][j] = A[(int64_t)(c + i) * lda + c + j];
     }
+    __syncthreads();
+    // Reciprocals of the diagonal once per block, so each row's solve is a
+    // chain of multiply-adds without a division per column.
+    if (threadIdx.x < w) inv_d[threadIdx.x] = T(1) / Ls[threadIdx.x][threadIdx.x];
     __syncthreads();
     const int r = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= r1) return;
@@ -81,7 +89,7 @@ __global__ void trsm_right_lt_leaf_kernel(T *A, int64_t lda, int c, int w, int r
 #pragma unroll
             for (int p = 0; p < kCholLeaf; ++p)
                 if (p < j) acc += x[p] * Ls[j][p];
-            x[j] = (x[j] - acc) / Ls[j][j];
+            x[j] = (x[j] - acc) * inv_d[j];
         }
     }
 #pragma unroll
