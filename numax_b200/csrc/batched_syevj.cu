@@ -116,13 +116,17 @@ __device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float
                 int p = min(a, b), q = max(a, b);
                 double c = 1.0, s = 0.0;
                 if (q < n) {
+                    // numax's angle, evaluated with reciprocal square roots
+                    // and one correctly rounded reciprocal (the chain of two
+                    // square roots and two divisions is the round's latency).
                     double apq = As[p * ld + q], app = As[p * ld + p], aqq = As[q * ld + q];
                     double d = aqq - app;
                     double two = 2.0 * apq;
-                    double radius = sqrt(d * d + two * two);
+                    const double r2 = d * d + two * two;
+                    const double radius = r2 > 0.0 ? r2 * rsqrt(r2) : 0.0;
                     double safe = guard_nonzero(fabs(d) + radius, 1e-30);
-                    double t = copysign(1.0, d) * two / safe;
-                    c = 1.0 / sqrt(1.0 + t * t);
+                    double t = copysign(1.0, d) * two * __drcp_rn(safe);
+                    c = rsqrt(1.0 + t * t);
                     s = t * c;
                 }
                 cs[2 * k] = c;
