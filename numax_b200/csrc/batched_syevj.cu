@@ -54,29 +54,35 @@ __device__ __forceinline__ void group_sync() {
         __syncthreads();
 }
 
-// Per-group shared-memory floats for matrices up to nmax.
+// A matrix of order n is worked on at the even order m = n + (n & 1): an odd
+// n gets a zero row and column (and a zero row/column in V), whose pairs
+// always rotate by the identity (a_pq = 0 gives t = 0), so every pair of a
+// round is a full 2x2 update without branches.  Row pitch m_max + 1 (odd).
+__host__ __device__ inline int syevj_even(int n) { return n + (n & 1); }
+__host__ __device__ inline int syevj_ld(int nmax) { return syevj_even(nmax) + 1; }
+
+// Per-group shared-memory floats for matrices up to nmax: A and V (m_max
+// rows of pitch ld), the round's rotations (float2 c, s) and pairs (int4
+// p, q, p*ld, q*ld), and a float64 reduction scratch.
 __host__ __device__ inline int syevj_group_floats(int nmax) {
-    int ld = nmax | 1;
-    // A, V, then rotations (c, s as float2 pairs of doubles -> 4 floats) and
-    // index pairs (2 ints), and a float64 reduction scratch.
-    return 2 * nmax * ld + (nmax / 2 + 1) * 4 + (nmax / 2 + 1) * 2 + 2 * 64;
+    const int m = syevj_even(nmax), half = m / 2 + 1;
+    return 2 * m * syevj_ld(nmax) + half * 2 + half * 4 + 2 * 64 + 4;
 }
 
 template <int G>
-__device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float *Vs, double *cs,
-                          int *pq, double *red, int gt) {
+__device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float *Vs, float2 *csf,
+                          int4 *pqo, double *red, int gt, int ld) {
     const int n = args.ns[mi];
-    const int ld = n | 1;
-    const int m = n + (n & 1);
+    const int m = syevj_even(n);
     const int half = m / 2;
     const float *A = args.A + args.a_off[mi];
     float *V = args.V + args.a_off[mi];
     float *W = args.W + args.w_off[mi];
 
-    for (int e = gt; e < n * n; e += G) {
-        int i = e / n, j = e - i * n;
-        As[i * ld + j] = A[e];
-        Vs[i * ld + j] = i == j ? 1.f : 0.f;
+    for (int e = gt; e < m * m; e += G) {
+        const int i = e / m, j = e - i * m;
+        As[i * ld + j] = (i < n && j < n) ? A[i * n + j] : 0.f;
+        Vs[i * ld + j] = (i == j && i < n) ? 1.f : 0.f;
     }
     group_sync<G>();
 
@@ -110,81 +116,58 @@ __device__ void syevj_one(const BatchedSyevjArgs &args, int mi, float *As, float
         if (!(off > args.tol * args.tol * tot) || sweep >= args.max_sweeps) break;
 
         for (int r = 0; r < m - 1; ++r) {
-            // Pairs and float64 rotations for this round.
+            // Pairs and float64 rotations for this round (the padding pair of
+            // an odd n gets c = 1, s = 0).
             for (int k = gt; k < half; k += G) {
-                int a = tourney(k, r, m), b = tourney(m - 1 - k, r, m);
-                int p = min(a, b), q = max(a, b);
-                double c = 1.0, s = 0.0;
-                if (q < n) {
-                    // numax's angle, evaluated with reciprocal square roots
-                    // and one correctly rounded reciprocal (the chain of two
-                    // square roots and two divisions is the round's latency).
-                    double apq = As[p * ld + q], app = As[p * ld + p], aqq = As[q * ld + q];
-                    double d = aqq - app;
-                    double two = 2.0 * apq;
-                    const double r2 = d * d + two * two;
-                    const double radius = r2 > 0.0 ? r2 * rsqrt(r2) : 0.0;
-                    double safe = guard_nonzero(fabs(d) + radius, 1e-30);
-                    double t = copysign(1.0, d) * two * __drcp_rn(safe);
-                    c = rsqrt(1.0 + t * t);
-                    s = t * c;
-                }
-                cs[2 * k] = c;
-                cs[2 * k + 1] = s;
-                pq[2 * k] = p;
-                pq[2 * k + 1] = q;
+                const int a = tourney(k, r, m), b = tourney(m - 1 - k, r, m);
+                const int p = min(a, b), q = max(a, b);
+                // numax's angle, evaluated with reciprocal square roots and
+                // one correctly rounded reciprocal (the chain of two square
+                // roots and two divisions is the round's latency).
+                const double apq = As[p * ld + q], app = As[p * ld + p], aqq = As[q * ld + q];
+                const double d = aqq - app;
+                const double two = 2.0 * apq;
+                const double r2 = d * d + two * two;
+                const double radius = r2 > 0.0 ? r2 * rsqrt(r2) : 0.0;
+                const double safe = guard_nonzero(fabs(d) + radius, 1e-30);
+                const double t = copysign(1.0, d) * two * __drcp_rn(safe);
+                const double c = rsqrt(1.0 + t * t);
+                csf[k] = make_float2((float)c, (float)(t * c));
+                pqo[k] = make_int4(p, q, p * ld, q * ld);
             }
             group_sync<G>();
-            // 2x2 blocks: rows of pair kr, columns of pair kc.  The rotations
-            // were formed in float64; they are applied to the float32 data in
-            // float32.  Lane = column pair (half <= 32), warp = row pairs.
+            // 2x2 blocks B' = R_k^T B R_l: lane = column pair l, warps = row
+            // pairs k.  The rotations were formed in float64; they are applied
+            // to the float32 data in float32.
             {
                 constexpr int NWG = G / 32;
                 const int lane = gt & 31, wg = gt >> 5;
-                const int kc = lane;
-                const bool colok = kc < half;
-                const int u = colok ? pq[2 * kc] : 0, v = colok ? pq[2 * kc + 1] : 0;
-                const float cc = colok ? (float)cs[2 * kc] : 1.f;
-                const float sc = colok ? (float)cs[2 * kc + 1] : 0.f;
-                for (int kr = wg; kr < half; kr += NWG) {
-                    if (!colok) continue;
-                    const int p = pq[2 * kr], q = pq[2 * kr + 1];
-                    if (q >= n && v >= n) continue;
-                    const float cr = (float)cs[2 * kr], sr = (float)cs[2 * kr + 1];
-                    if (q < n && v < n) {
-                        const float b00 = As[p * ld + u], b01 = As[p * ld + v];
-                        const float b10 = As[q * ld + u], b11 = As[q * ld + v];
-                        // rows: [c -s; s c] applied from the left
-                        const float r00 = cr * b00 - sr * b10, r01 = cr * b01 - sr * b11;
-                        const float r10 = sr * b00 + cr * b10, r11 = sr * b01 + cr * b11;
-                        // columns: [c s; -s c] applied from the right
-                        float o00 = cc * r00 - sc * r01, o01 = sc * r00 + cc * r01;
-                        float o10 = cc * r10 - sc * r11, o11 = sc * r10 + cc * r11;
-                        if (kr == kc) {
-                            o01 = 0.f;  // the annihilated pair
-                            o10 = 0.f;
-                        }
-                        As[p * ld + u] = o00;
-                        As[p * ld + v] = o01;
-                        As[q * ld + u] = o10;
-                        As[q * ld + v] = o11;
-                    } else if (q < n) {  // column pair has the dummy index
-                        const float b0 = As[p * ld + u], b1 = As[q * ld + u];
-                        As[p * ld + u] = cr * b0 - sr * b1;
-                        As[q * ld + u] = sr * b0 + cr * b1;
-                    } else {  // row pair has the dummy index
-                        const float b0 = As[p * ld + u], b1 = As[p * ld + v];
-                        As[p * ld + u] = cc * b0 - sc * b1;
-                        As[p * ld + v] = sc * b0 + cc * b1;
+                if (lane < half) {
+                    const int4 cu = pqo[lane];
+                    const float2 cc = csf[lane];
+#pragma unroll 4
+                    for (int kr = wg; kr < half; kr += NWG) {
+                        const int4 ru = pqo[kr];
+                        const float2 rc = csf[kr];
+                        const float b00 = As[ru.z + cu.x], b01 = As[ru.z + cu.y];
+                        const float b10 = As[ru.w + cu.x], b11 = As[ru.w + cu.y];
+                        // rows: [c -s; s c] from the left, columns: [c s; -s c] from the right
+                        const float r00 = rc.x * b00 - rc.y * b10, r01 = rc.x * b01 - rc.y * b11;
+                        const float r10 = rc.y * b00 + rc.x * b10, r11 = rc.y * b01 + rc.x * b11;
+                        const bool own = kr == lane;  // the annihilated pair
+                        As[ru.z + cu.x] = cc.x * r00 - cc.y * r01;
+                        As[ru.z + cu.y] = own ? 0.f : cc.y * r00 + cc.x * r01;
+                        As[ru.w + cu.x] = own ? 0.f : cc.x * r10 - cc.y * r11;
+                        As[ru.w + cu.y] = cc.y * r10 + cc.x * r11;
+                    }
+                    // V := V J: warps = rows of V, lane = column pair.
+#pragma unroll 4
+                    for (int i = wg; i < n; i += NWG) {
+                        const float vp = Vs[i * ld + cu.x], vq = Vs[i * ld + cu.y];
+                        Vs[i * ld + cu.x] = cc.x * vp - cc.y * vq;
+                        Vs[i * ld + cu.y] = cc.y * vp + cc.x * vq;
                     }
                 }
-                // V := V J: warp = rows of V, lane = column pair.
-                if (colok && v < n)
-                    for (int i = wg; i < n; i += NWG) {
-                        const float vp = Vs[i * ld + u], vq = Vs[i * ld + v];
-                        Vs[i * ld + u] = cc * vp - sc * vq;
-                        Vs[i * ld + v] = sc * vp + cc * vq;
-                    }
             }
             group_sync<G>();
         }
@@ -219,16 +202,15 @@ __global__ void __launch_bounds__(NT) syevj_batched_kernel(BatchedSyevjArgs args
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NG = NT / G;
     const int g = threadIdx.x / G, gt = threadIdx.x - g * G;
-    const int ld = nmax | 1;
+    const int ld = syevj_ld(nmax), mmax = syevj_even(nmax), hmax = mmax / 2 + 1;
     const int per_group = syevj_group_floats(nmax);
     float *base = reinterpret_cast<float *>(smem_raw) + (size_t)g * ((per_group + 3) & ~3);
     float *As = base;
-    float *Vs = As + nmax * ld;
-    double *cs =
-        reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(Vs + nmax * ld) + 7) & ~uintptr_t(7));
-    int *pq = reinterpret_cast<int *>(cs + 2 * (nmax / 2 + 1));
-    double *red = reinterpret_cast<double *>(
-        (reinterpret_cast<uintptr_t>(pq + 2 * (nmax / 2 + 1)) + 7) & ~uintptr_t(7));
+    float *Vs = As + mmax * ld;
+    // 16-byte aligned tables after A and V.
+    int4 *pqo = reinterpret_cast<int4 *>((reinterpret_cast<uintptr_t>(Vs + mmax * ld) + 15) & ~uintptr_t(15));
+    float2 *csf = reinterpret_cast<float2 *>(pqo + hmax);
+    double *red = reinterpret_cast<double *>(csf + hmax);
     __shared__ int s_item[NG];
     for (;;) {
         if (gt == 0) s_item[g] = atomicAdd(counter, 1);
@@ -236,7 +218,7 @@ __global__ void __launch_bounds__(NT) syevj_batched_kernel(BatchedSyevjArgs args
         const int item = begin + s_item[g];
         group_sync<G>();
         if (item >= end) break;
-        syevj_one<G>(args, args.order[item], As, Vs, cs, pq, red, gt);
+        syevj_one<G>(args, args.order[item], As, Vs, csf, pqo, red, gt, ld);
     }
 }
 
