@@ -71,7 +71,10 @@ NMX_API int nmx_version(void);
  *   "ir.trsv_ctas"  CTAs of the persistent triangular solves of the IR loop
  *   "ir.tc_min"     smallest inner GEMM dimension the mixed-precision LU
  *                   sends to the tensor cores (-1 = 256; thinner updates
- *                   run in FP32) */
+ *                   run in FP32)
+ *   "lu.tournament" FP32 panels by tournament pivoting (a stable LU with
+ *                   other pivots than numax's): -1 = in the mixed-precision
+ *                   LU only, 0 = never, 1 = also in nmx_getrf_f32 */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
 NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
 

@@ -119,6 +119,7 @@ static int64_t *tune_slot(nmx_ctx ctx, const char *key) {
     if (!std::strcmp(key, "lu.cluster")) return &ctx->tune_lu_cluster;
     if (!std::strcmp(key, "ir.tc_min")) return &ctx->tune_ir_tc_min;
     if (!std::strcmp(key, "lu.leaf_w")) return &ctx->tune_lu_leaf_w;
+    if (!std::strcmp(key, "lu.tournament")) return &ctx->tune_lu_tournament;
     return nullptr;
 }
 

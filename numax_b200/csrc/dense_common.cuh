@@ -168,9 +168,12 @@ int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
                int c1);
 
 // Recursive LU with partial pivoting of the n x n row-major A (dense_lu.cu),
-// trailing updates through `gs`.  ipiv/info as nmx_getrf_*.
+// trailing updates through `gs`.  ipiv/info as nmx_getrf_*.  `tournament`
+// (FP32 only) picks each leaf's pivots by tournament pivoting instead: a
+// stable LU with other pivots than numax's, for the factorization that
+// iterative refinement corrects.
 template <typename T>
 int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
-              int32_t *info);
+              int32_t *info, bool tournament = false);
 
 }  // namespace nmx

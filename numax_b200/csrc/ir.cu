@@ -558,7 +558,7 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     scale_to_f32_kernel<<<(unsigned)ceil_div((int64_t)n * n, threads), threads, 0, st>>>(
         A, lda, n, R.rs, R.cs, R.W, R.ldw);
     NMX_CUDA_TRY(cudaGetLastError());
-    rc = getrf_run<float>(ctx, gs, n, R.W, R.ldw, ipiv, info_d);
+    rc = getrf_run<float>(ctx, gs, n, R.W, R.ldw, ipiv, info_d, ctx->tune_lu_tournament != 0);
     if (rc) return rc;
     // Inverses of the diagonal blocks of L and U for the triangular solves.
     {

@@ -69,6 +69,7 @@ struct nmx_context {
     int64_t tune_lu_cluster = -1;     // cap on the LU cluster leaf's CTAs (-1: none, 0: off)
     int64_t tune_lu_leaf_w = 0;       // widest LU leaf panel (0: 32; multiple of 8, <= 64)
     int64_t tune_ir_tc_min = -1;      // smallest GEMM inner dimension on the tensor cores (-1: 256)
+    int64_t tune_lu_tournament = -1;  // tournament-pivoting FP32 leaves (-1: IR only, 0: never, 1: also nmx_getrf_f32)
     // Grow-only named device buffers, one per use, kept for the context's life.
     static constexpr int kSlots = 8;
     void *slot_ptr[kSlots] = {};
@@ -80,7 +81,7 @@ struct nmx_context {
 };
 
 namespace nmx {
-enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5 };
+enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5, kWsCalu = 6 };
 }
 
 namespace nmx {

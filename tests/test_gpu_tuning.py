@@ -9,7 +9,8 @@ torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-KEYS = [b"lu.leaf_ctas", b"lu.cluster", b"lu.leaf_w", b"ir.trsv_ctas", b"ir.tc_min"]
+KEYS = [b"lu.leaf_ctas", b"lu.cluster", b"lu.leaf_w", b"ir.trsv_ctas", b"ir.tc_min",
+        b"lu.tournament"]
 
 
 def test_tune_keys_round_trip_and_errors():
