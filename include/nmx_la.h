@@ -74,7 +74,9 @@ NMX_API int nmx_version(void);
  *                   run in FP32)
  *   "lu.tournament" FP32 panels by tournament pivoting (a stable LU with
  *                   other pivots than numax's): -1 = in the mixed-precision
- *                   LU only, 0 = never, 1 = also in nmx_getrf_f32 */
+ *                   LU only, 0 = never, 1 = also in nmx_getrf_f32
+ *   "lu.lookahead"  panel width of the tournament-pivoting LU's look-ahead
+ *                   (-1 = 512, 0 = unblocked recursion; 64..1024) */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
 NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
 

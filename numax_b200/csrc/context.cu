@@ -18,6 +18,39 @@ void set_error(const char *fmt, ...) {
 
 void clear_error() { g_last_error[0] = 0; }
 
+// The second handle (same settings) for work that runs concurrently with the
+// first handle's.
+int ctx_cublas_aux(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out) {
+    if (!ctx->cublas_aux) {
+        cublasHandle_t h;
+        cublasStatus_t s = cublasCreate(&h);
+        if (s != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasCreate failed (%d)", (int)s);
+            return NMX_ERR_CUDA;
+        }
+        cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+        ctx->cublas_aux = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas_aux);
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) {
+        set_error("cublasSetStream failed");
+        return NMX_ERR_CUDA;
+    }
+    *out = h;
+    return 0;
+}
+
+int ctx_lookahead_streams(nmx_ctx ctx) {
+    if (ctx->la_stream[0]) return 0;
+    int least = 0, greatest = 0;
+    NMX_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    NMX_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[0], cudaStreamNonBlocking, greatest));
+    NMX_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[1], cudaStreamNonBlocking, least));
+    for (int i = 0; i < 2; ++i)
+        NMX_CUDA_TRY(cudaEventCreateWithFlags(&ctx->la_event[i], cudaEventDisableTiming));
+    return 0;
+}
+
 int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out) {
     if (!ctx->cublas) {
         cublasHandle_t h;
@@ -120,6 +153,7 @@ static int64_t *tune_slot(nmx_ctx ctx, const char *key) {
     if (!std::strcmp(key, "ir.tc_min")) return &ctx->tune_ir_tc_min;
     if (!std::strcmp(key, "lu.leaf_w")) return &ctx->tune_lu_leaf_w;
     if (!std::strcmp(key, "lu.tournament")) return &ctx->tune_lu_tournament;
+    if (!std::strcmp(key, "lu.lookahead")) return &ctx->tune_lu_lookahead;
     return nullptr;
 }
 
@@ -149,6 +183,11 @@ int nmx_destroy(nmx_ctx ctx) {
         for (int i = 0; i < nmx_context::kSlots; ++i)
             if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
         if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
+        if (ctx->cublas_aux) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas_aux));
+        for (int i = 0; i < 2; ++i) {
+            if (ctx->la_stream[i]) cudaStreamDestroy(ctx->la_stream[i]);
+            if (ctx->la_event[i]) cudaEventDestroy(ctx->la_event[i]);
+        }
     }
     delete ctx;
     return 0;

@@ -112,12 +112,16 @@ inline cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int
 
 // The context's cuBLAS handle bound to `st` (created on first use).
 int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
+// A second cuBLAS handle bound to `st`, for work concurrent with the first's.
+int ctx_cublas_aux(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
+// Creates the context's look-ahead streams and events on first use.
+int ctx_lookahead_streams(nmx_ctx ctx);
 
 // Tensor-core update (gemm_tc.cu): C -= round16(A) round16(B), fp32 operands.
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
                     int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
                     size_t ws_bytes);
-size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K);
+size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision);
 
 // The trailing-update product of the recursive factorizations and solves:
 // C[m x n] -= A[m x k] B[k x n], row-major.  precision 0 keeps the operands'

@@ -23,7 +23,9 @@
 
 #include <algorithm>
 
+#include "calu.cuh"
 #include "dense_common.cuh"
+#include "gemm_tc.cuh"
 
 namespace nmx {
 
@@ -393,378 +395,6 @@ __global__ void __launch_bounds__(kClusterLeafThreads)
     }
 }
 
-// ---- tournament-pivoting leaf (FP32: the mixed-precision factorization) ----
-//
-// The FP32 factorization inside iterative refinement (ir.cu) needs a stable
-// LU, not numax's exact pivot sequence: refinement in FP64 makes the solution
-// independent of which stable pivots the factors used.  Its leaves use
-// tournament pivoting (CALU; Grigori, Demmel & Xiang, SIAM J. Matrix Anal.
-// Appl. 32(4), 2011) over a reduction tree of at most three levels:
-//   1. every CTA holds 512 rows of the panel, one row per thread in
-//      registers, runs partial pivoting on them and publishes the (up to) w
-//      rows it picked;
-//   2. the last CTA of each group of 16 to finish (an arrival counter; no CTA
-//      waits for another) stacks the group's 16 x w candidates -- their
-//      original values, re-read from A -- and keeps the w rows partial
-//      pivoting picks among them;
-//   3. the last group to finish does the same over the groups' candidates,
-//      keeping the multipliers: the rows it picks, in pick order, are the
-//      pivot rows and hold L11\U11.  It writes them, the LAPACK-style
-//      interchanges and the list of rows that change place.
-// A second kernel solves every other row against U11 (l = a U11^-1, rows
-// independent) and moves rows to their final positions across the whole
-// width.  The pivot search costs one CTA barrier per column instead of one
-// grid- or cluster-wide exchange.  A zero U11 diagonal is floored to 1e-30
-// and the first one reported in info; a column without a nonzero candidate
-// picks the lowest row.
-constexpr int kCaluRows = 512;                          // rows per CTA, one per thread
-constexpr int kCaluW = 32;                              // widest leaf
-constexpr int kCaluWarps = kCaluRows / 32;
-constexpr int kCaluGroup = kCaluRows / kCaluW;          // candidate sets one CTA stacks
-constexpr int kCaluMaxCtas = kCaluGroup * kCaluGroup;   // panels of up to 131072 rows
-constexpr int kCaluApplyThreads = 256;
-
-struct CaluScratch {
-    int *cand;        // [kCaluMaxCtas][kCaluW] first-level picks (global rows, -1: none)
-    int *gcand;       // [kCaluGroup][kCaluW] second-level picks
-    unsigned *count;  // [kCaluGroup + 1] arrival counters, zero between leaves
-    float *lu;        // [kCaluW][kCaluW] L11\U11 of the pivot rows, pivot order
-    int *gp;          // [kCaluW] pivot rows in pivot order (-1 past the panel)
-    int *moves;       // [2 kCaluW][2] (from, to) of every row that changes place
-    int *nmoves;      // 1
-    static size_t bytes() {
-        return sizeof(int) * ((size_t)kCaluMaxCtas * kCaluW + kCaluGroup * kCaluW + kCaluGroup +
-                              1 + kCaluW + 4 * kCaluW + 1) +
-               sizeof(float) * kCaluW * kCaluW + 256;
-    }
-    void carve(void *base) {
-        float *f = static_cast<float *>(base);
-        lu = f;
-        int *i = reinterpret_cast<int *>(f + kCaluW * kCaluW);
-        cand = i;
-        gcand = cand + kCaluMaxCtas * kCaluW;
-        gp = gcand + kCaluGroup * kCaluW;
-        moves = gp + kCaluW;
-        nmoves = moves + 4 * kCaluW;
-        count = reinterpret_cast<unsigned *>(nmoves + 1);
-    }
-};
-
-struct CaluShared {
-    unsigned long long key[2][kCaluWarps];   // each warp's best candidate, by column parity
-    __align__(16) float row[2][kCaluWarps][kCaluW];  // that candidate's row
-    int sel[kCaluW];
-    int last;
-};
-
-// Order of a live row as a pivot candidate: |v| above zero/NaN, then the
-// lower row; 0 is reserved for "no candidate".
-__device__ __forceinline__ unsigned long long calu_key(float v, int row) {
-    const float m = fabsf(v);
-    const unsigned hi = m > 0.f ? __float_as_uint(m) + 2u : 1u;
-    return ((unsigned long long)hi << 32) | (unsigned)(~(unsigned)row);
-}
-
-__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
-    return a > b ? a : b;
-}
-
-// The first w columns of row `row` from column c into a[] (zeros past w or
-// for a dead row); vec: rows start on 16-byte boundaries.
-__device__ __forceinline__ void calu_load_row(float (&a)[kCaluW], const float *A, int64_t lda,
-                                              int row, int c, int w, bool live, bool vec) {
-    const float *src = A + (int64_t)(live ? row : 0) * lda + c;
-#pragma unroll
-    for (int q = 0; q < kCaluW / 4; ++q) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (live) {
-            if (vec && 4 * q + 4 <= w) {
-                v = *reinterpret_cast<const float4 *>(src + 4 * q);
-            } else if (4 * q + 4 <= w) {
-                v.x = src[4 * q];
-                v.y = src[4 * q + 1];
-                v.z = src[4 * q + 2];
-                v.w = src[4 * q + 3];
-            } else if (4 * q < w) {
-                v.x = src[4 * q];
-                if (4 * q + 1 < w) v.y = src[4 * q + 1];
-                if (4 * q + 2 < w) v.z = src[4 * q + 2];
-            }
-        }
-        a[4 * q] = v.x;
-        a[4 * q + 1] = v.y;
-        a[4 * q + 2] = v.z;
-        a[4 * q + 3] = v.w;
-    }
-}
-
-// Partial pivoting over the CTA's rows (one per thread: a[] its first w
-// columns, `row` its global index, dead threads live = false).  Picks up to w
-// rows, their global indices in pick order into sh.sel, and returns how many.
-// KEEP_L keeps the multipliers, so a picked row ends as its L\U row;
-// picked_at = the column at which this thread's row was picked, else -1.
-template <bool KEEP_L>
-__device__ int calu_gepp(float (&a)[kCaluW], int row, bool live, int w, CaluShared &sh,
-                         int &picked_at) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int np = 0;
-    picked_at = -1;
-#pragma unroll
-    for (int j = 0; j < kCaluW; ++j) {
-        if (j >= w) break;
-        const int b = j & 1;
-        const unsigned long long k = live ? calu_key(a[j], row) : 0ull;
-        unsigned long long best = k;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) best = umax64(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if (lane == 0) sh.key[b][warp] = best;
-        if (k != 0ull && k == best) {
-            float4 *dst = reinterpret_cast<float4 *>(sh.row[b][warp]);
-#pragma unroll
-            for (int q = 0; q < kCaluW / 4; ++q)
-                if (4 * q + 3 >= j)
-                    dst[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
-        }
-        __syncthreads();
-        const unsigned long long mine = lane < kCaluWarps ? sh.key[b][lane] : 0ull;
-        unsigned long long g = mine;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) g = umax64(g, __shfl_xor_sync(0xffffffffu, g, o));
-        if (g == 0ull) break;  // no candidate left in the CTA (uniform)
-        const int p = (int)(~(unsigned)(g & 0xffffffffull));
-        const int ww = __ffs(__ballot_sync(0xffffffffu, mine == g)) - 1;
-        const float *prow = sh.row[b][ww];
-        float pv = prow[j];
-        if (pv == 0.f) pv = pivot_floor<float>::value;
-        const float rp = __frcp_rn(pv);
-        if (live && row == p) {
-            live = false;
-            picked_at = j;
-        }
-        if (live) {
-            const float l = a[j] * rp;
-            if (KEEP_L) a[j] = l;
-#pragma unroll
-            for (int q = 0; q < kCaluW / 4; ++q) {
-                if (4 * q + 3 > j) {
-                    const float4 u = reinterpret_cast<const float4 *>(prow)[q];
-                    if (4 * q > j) a[4 * q] = fmaf(-l, u.x, a[4 * q]);
-                    if (4 * q + 1 > j) a[4 * q + 1] = fmaf(-l, u.y, a[4 * q + 1]);
-                    if (4 * q + 2 > j) a[4 * q + 2] = fmaf(-l, u.z, a[4 * q + 2]);
-                    a[4 * q + 3] = fmaf(-l, u.w, a[4 * q + 3]);
-                }
-            }
-        }
-        if (tid == 0) sh.sel[j] = p;
-        np = j + 1;
-    }
-    __syncthreads();
-    return np;
-}
-
-// Every thread's writes before, one arrival on *count after; true in the
-// CTA whose arrival completes `members`.
-__device__ __forceinline__ bool calu_arrive(unsigned *count, int members, CaluShared &sh) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) sh.last = atomicAdd(count, 1u) == (unsigned)(members - 1);
-    __syncthreads();
-    const bool last = sh.last != 0;
-    if (last) __threadfence();
-    return last;
-}
-
-// The final CTA: the pivot rows' L11\U11, the interchanges, the moves, info,
-// and the counters back to zero.
-__device__ void calu_finish(const float (&a)[kCaluW], int row, int picked, int np, int c, int w,
-                            CaluScratch s, int32_t *ipiv, int32_t *info, CaluShared &sh) {
-    const int tid = threadIdx.x, lane = tid & 31;
-    // The row buffers are free after the last pivot search: 32 x 32 floats.
-    float(*lus)[kCaluW] = reinterpret_cast<float(*)[kCaluW]>(&sh.row[0][0][0]);
-    if (picked >= 0) {
-        float4 *g = reinterpret_cast<float4 *>(s.lu + picked * kCaluW);
-        float4 *l = reinterpret_cast<float4 *>(lus[picked]);
-#pragma unroll
-        for (int q = 0; q < kCaluW / 4; ++q) {
-            const float4 v = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
-            g[q] = v;
-            l[q] = v;
-        }
-    }
-    if (tid <= kCaluGroup) s.count[tid] = 0u;
-    __syncthreads();
-    if (tid >= 32) return;
-    // LAPACK-style interchanges: step j swaps position c + j with the current
-    // position of pivot j.  Lane k tracks position c + k and, from step k on,
-    // possibly one more position outside [c, c + 32); untracked positions hold
-    // their own rows.
-    const unsigned full = 0xffffffffu;
-    int pos0 = c + lane, row0 = c + lane, pos1 = -1, row1 = -1;
-    for (int j = 0; j < np; ++j) {
-        const int g = sh.sel[j], cj = c + j;
-        int where = row0 == g ? pos0 : (row1 == g ? pos1 : -1);
-        unsigned m = __ballot_sync(full, where >= 0);
-        const int pos = m ? __shfl_sync(full, where, __ffs(m) - 1) : g;
-        int here = pos0 == cj ? row0 : (pos1 == cj ? row1 : -1);
-        m = __ballot_sync(full, here >= 0);
-        const int at_cj = m ? __shfl_sync(full, here, __ffs(m) - 1) : cj;
-        const bool tracked = __any_sync(full, pos0 == pos || pos1 == pos);
-        if (pos0 == cj) row0 = g;
-        else if (pos0 == pos) row0 = at_cj;
-        if (pos1 == cj) row1 = g;
-        else if (pos1 == pos) row1 = at_cj;
-        if (!tracked && lane == j) {
-            pos1 = pos;
-            row1 = at_cj;
-        }
-        if (lane == 0) ipiv[cj] = pos;
-    }
-    const bool mv0 = row0 != pos0, mv1 = pos1 >= 0 && row1 != pos1;
-    const unsigned b0 = __ballot_sync(full, mv0), b1 = __ballot_sync(full, mv1);
-    const unsigned lt = (1u << lane) - 1u;
-    if (mv0) {
-        const int i = __popc(b0 & lt);
-        s.moves[2 * i] = row0;
-        s.moves[2 * i + 1] = pos0;
-    }
-    if (mv1) {
-        const int i = __popc(b0) + __popc(b1 & lt);
-        s.moves[2 * i] = row1;
-        s.moves[2 * i + 1] = pos1;
-    }
-    s.gp[lane] = lane < np ? sh.sel[lane] : -1;
-    const unsigned zero = __ballot_sync(full, lane < np && lus[lane][lane] == 0.f);
-    if (lane == 0) {
-        *s.nmoves = __popc(b0) + __popc(b1);
-        if (zero && *info == 0) *info = c + __ffs(zero);
-    }
-}
-
-// Pivot search of the leaf at column c (w <= 32 columns, rows [c, n)) over
-// nctas CTAs of 512 rows.
-__global__ void __launch_bounds__(kCaluRows)
-    calu_pick_kernel(const float *A, int64_t lda, int n, int c, int w, int nctas, bool vec,
-                     CaluScratch s, int32_t *ipiv, int32_t *info) {
-    __shared__ CaluShared sh;
-    const int tid = threadIdx.x;
-    const int ngroups = (nctas + kCaluGroup - 1) / kCaluGroup;
-    float a[kCaluW];
-    int picked = -1;
-    int row = c + blockIdx.x * kCaluRows + tid;
-    bool live = row < n;
-    calu_load_row(a, A, lda, row, c, w, live, vec);
-    if (nctas == 1) {
-        const int np = calu_gepp<true>(a, row, live, w, sh, picked);
-        calu_finish(a, row, picked, np, c, w, s, ipiv, info, sh);
-        return;
-    }
-    int np = calu_gepp<false>(a, row, live, w, sh, picked);
-    if (tid < kCaluW) s.cand[blockIdx.x * kCaluW + tid] = tid < np ? sh.sel[tid] : -1;
-    const int grp = blockIdx.x / kCaluGroup;
-    const int members = min(kCaluGroup, nctas - grp * kCaluGroup);
-    if (!calu_arrive(&s.count[grp], members, sh)) return;
-    // Second level: the group's candidates, original values.
-    row = tid < members * kCaluW ? __ldcg(&s.cand[grp * kCaluGroup * kCaluW + tid]) : -1;
-    live = row >= 0;
-    calu_load_row(a, A, lda, row, c, w, live, vec);
-    if (ngroups == 1) {
-        np = calu_gepp<true>(a, row, live, w, sh, picked);
-        calu_finish(a, row, picked, np, c, w, s, ipiv, info, sh);
-        return;
-    }
-    np = calu_gepp<false>(a, row, live, w, sh, picked);
-    if (tid < kCaluW) s.gcand[grp * kCaluW + tid] = tid < np ? sh.sel[tid] : -1;
-    if (!calu_arrive(&s.count[kCaluGroup], ngroups, sh)) return;
-    // Third level: every group's candidates.
-    row = tid < ngroups * kCaluW ? __ldcg(&s.gcand[tid]) : -1;
-    live = row >= 0;
-    calu_load_row(a, A, lda, row, c, w, live, vec);
-    np = calu_gepp<true>(a, row, live, w, sh, picked);
-    calu_finish(a, row, picked, np, c, w, s, ipiv, info, sh);
-}
-
-// After the pivot search: CTAs [0, panel_ctas) take the panel's rows, one
-// per thread -- a pivot row's place c + j gets L11\U11 row j, every other
-// row becomes l = a U11^-1 at its final position; the CTAs after them move
-// the rows that change place in every column outside the panel (all reads
-// of a column before its writes).  No row is read by one thread and written
-// by another: displaced rows land on the pivots' old places, which their
-// own threads leave alone.
-__global__ void __launch_bounds__(kCaluApplyThreads)
-    calu_apply_kernel(float *A, int64_t lda, int n, int c, int w, int panel_ctas, bool vec,
-                      CaluScratch s) {
-    __shared__ __align__(16) float U[kCaluW][kCaluW];
-    __shared__ float rd[kCaluW];
-    __shared__ int gp[kCaluW];
-    __shared__ int mv[4 * kCaluW];
-    __shared__ int nmv;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kCaluW * kCaluW; e += kCaluApplyThreads) (&U[0][0])[e] = s.lu[e];
-    for (int e = tid; e < 4 * kCaluW; e += kCaluApplyThreads) mv[e] = s.moves[e];
-    if (tid < kCaluW) gp[tid] = s.gp[tid];
-    if (tid == 0) nmv = *s.nmoves;
-    __syncthreads();
-    if (tid < kCaluW) {
-        float d = U[tid][tid];
-        if (d == 0.f) d = pivot_floor<float>::value;
-        rd[tid] = __frcp_rn(d);
-    }
-    __syncthreads();
-    const int nm = nmv;
-    if ((int)blockIdx.x < panel_ctas) {
-        const int row = c + blockIdx.x * kCaluApplyThreads + tid;
-        if (row >= n) return;
-        bool pivot = false;
-#pragma unroll 8
-        for (int k = 0; k < kCaluW; ++k) pivot |= gp[k] == row;
-        float x[kCaluW];
-        int dst = row;
-        if (!pivot) {
-            if (row < c + kCaluW)
-                for (int k = 0; k < nm; ++k)
-                    if (mv[2 * k] == row) dst = mv[2 * k + 1];
-            calu_load_row(x, A, lda, row, c, w, true, vec);
-#pragma unroll
-            for (int j = 0; j < kCaluW; ++j) {
-                if (j < w) {
-                    const float l = x[j] * rd[j];
-                    x[j] = l;
-#pragma unroll
-                    for (int q = 0; q < kCaluW / 4; ++q) {
-                        if (4 * q + 3 > j) {
-                            const float4 u = reinterpret_cast<const float4 *>(U[j])[q];
-                            if (4 * q > j) x[4 * q] = fmaf(-l, u.x, x[4 * q]);
-                            if (4 * q + 1 > j) x[4 * q + 1] = fmaf(-l, u.y, x[4 * q + 1]);
-                            if (4 * q + 2 > j) x[4 * q + 2] = fmaf(-l, u.z, x[4 * q + 2]);
-                            x[4 * q + 3] = fmaf(-l, u.w, x[4 * q + 3]);
-                        }
-                    }
-                }
-            }
-            float *out = A + (int64_t)dst * lda + c;
-#pragma unroll
-            for (int j = 0; j < kCaluW; ++j)
-                if (j < w) out[j] = x[j];
-        }
-        // Row c + k (k < w) ends holding pivot k's L\U row.
-        if (row < c + w) {
-            const int k = row - c;
-            float *out = A + (int64_t)row * lda + c;
-            for (int j = 0; j < w; ++j) out[j] = U[k][j];
-        }
-        return;
-    }
-    const int col = (blockIdx.x - panel_ctas) * kCaluApplyThreads + tid;
-    if (col >= n || (col >= c && col < c + w)) return;
-    float v[2 * kCaluW];
-#pragma unroll
-    for (int k = 0; k < 2 * kCaluW; ++k)
-        if (k < nm) v[k] = A[(int64_t)mv[2 * k] * lda + col];
-#pragma unroll
-    for (int k = 0; k < 2 * kCaluW; ++k)
-        if (k < nm) A[(int64_t)mv[2 * k + 1] * lda + col] = v[k];
-}
-
 // Apply interchanges ipiv[c..c+w) to the columns outside [c, c+w) of rows of
 // A (ncols wide).  One thread per column, swaps in order.
 template <typename T>
@@ -867,6 +497,12 @@ struct LuRun {
     int max_w;    // widest leaf (multiple of 8, <= kLeafMax)
     bool tournament = false;  // tournament-pivoting leaves (FP32 only)
     CaluScratch cs = {};
+    // Tournament leaves: the columns their row interchanges reach now (the
+    // look-ahead panel; [0, n) unblocked) and where they leave their row
+    // moves for the other columns.
+    int scope_lo = 0, scope_hi = 0;
+    int *lists = nullptr;
+    int nlists = 0;
 };
 
 // Shared-memory bytes the cluster leaf needs for an m-row panel of width w.
@@ -888,19 +524,32 @@ static int leaf_width(const LuRun<T> &R, int m) {
     return R.max_w;
 }
 
-// Tournament-pivoting leaf: the pivot search, then the rows into place.
+// Row moves of `nlists` leaves in columns [a0, a1) and [b0, b1).
+static int calu_swap(cudaStream_t st, float *A, int64_t lda, const int *lists, int nlists, int a0,
+                     int a1, int b0, int b1) {
+    const int cols = std::max(0, a1 - a0) + std::max(0, b1 - b0);
+    if (cols == 0 || nlists == 0) return 0;
+    calu_swap_kernel<<<(unsigned)ceil_div(cols, kCaluApplyThreads), kCaluApplyThreads, 0, st>>>(
+        A, lda, lists, nlists, a0, std::max(a0, a1), b0, std::max(b0, b1));
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Tournament-pivoting leaf: the pivot search, the panel's rows into place,
+// and the row moves across the columns in scope.
 static int calu_leaf(LuRun<float> &R, int c, int w) {
     const int m = R.n - c;
     const int nctas = (int)ceil_div(m, kCaluRows);
     const bool vec = R.lda % 4 == 0 && reinterpret_cast<uintptr_t>(R.A) % 16 == 0;
-    calu_pick_kernel<<<nctas, kCaluRows, 0, R.st>>>(R.A, R.lda, R.n, c, w, nctas, vec, R.cs,
-                                                    R.ipiv, R.info);
-    const int panel = (int)ceil_div(m, kCaluApplyThreads);
-    const int other = (int)ceil_div(R.n, kCaluApplyThreads);
-    calu_apply_kernel<<<panel + other, kCaluApplyThreads, 0, R.st>>>(R.A, R.lda, R.n, c, w, panel,
-                                                                     vec, R.cs);
+    // Unblocked, the lists are used at once and their slots recycle.
+    if (R.nlists >= kCaluMaxLists) R.nlists = 0;
+    int *ml = R.lists + (size_t)R.nlists++ * kCaluListStride;
+    calu_pick_kernel<<<nctas, kCaluThreads, 0, R.st>>>(R.A, R.lda, R.n, c, w, nctas, vec, R.cs,
+                                                    R.ipiv, R.info, ml);
+    calu_apply_kernel<<<(unsigned)ceil_div(m, kCaluApplyThreads), kCaluApplyThreads,
+                        kCaluApplySmem, R.st>>>(R.A, R.lda, R.n, c, w, R.cs, ml);
     NMX_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return calu_swap(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
 }
 
 template <typename T>
@@ -1033,6 +682,109 @@ static int getrf2(LuRun<T> &R, int c, int w) {
     return getrf2<T>(R, c + hw, w - hw);
 }
 
+// Right-looking LU over panels of nb columns with a look-ahead of one panel
+// (tournament leaves only).  Two streams: the panel stream (high priority)
+// updates the next panel's columns and factors it while the update stream
+// applies the previous panel to every other column:
+//
+//   panel stream, step i:  moves(i) + U12 + GEMM on panel i+1's columns,
+//                          then factor panel i+1 (its leaves' row moves
+//                          reach panel i+1's columns only, the rest is kept);
+//   update stream, step i: moves(i) on columns [0, i nb) and past panel
+//                          i+1, U12 and the GEMM past panel i+1.
+//
+// Step i's two halves touch disjoint columns and only read panel i.  The
+// panel stream starts step i+1 after the update stream's step i (which
+// updated panel i+2's columns); the update stream starts step i after panel
+// i is factored.  The leaves' move lists alternate between two buffers.
+static int getrf_lookahead(LuRun<float> &R, int nb) {
+    nmx_ctx ctx = R.ctx;
+    const int n = R.n;
+    int rc = ctx_lookahead_streams(ctx);
+    if (rc) return rc;
+    cudaStream_t P = ctx->la_stream[0], U = ctx->la_stream[1];
+    cudaEvent_t eP = ctx->la_event[0], eU = ctx->la_event[1];
+    GemmSub gP = R.gs, gU = R.gs;
+    gP.st = P;
+    gU.st = U;
+    rc = ctx_cublas_aux(ctx, P, &gP.h);
+    if (rc) return rc;
+    rc = ctx_cublas(ctx, U, &gU.h);
+    if (rc) return rc;
+    if (gP.precision) {
+        gP.ws_bytes = tc_gemm_workspace_bytes(n, nb, nb, gP.precision) + 4096;
+        rc = ctx->ensure_slot(kWsGemm16Panel, gP.ws_bytes, &gP.ws);
+        if (rc) return rc;
+    }
+    LuRun<float> RP = R;
+    RP.st = P;
+    RP.gs = gP;
+    int *buf[2] = {R.cs.lists, R.cs.lists + (size_t)kCaluMaxLists * kCaluListStride};
+    int cur = 0;
+    auto panel = [&](int k, int kb) {
+        RP.scope_lo = k;
+        RP.scope_hi = k + kb;
+        RP.lists = buf[cur];
+        RP.nlists = 0;
+        return getrf2<float>(RP, k, kb);
+    };
+    auto body = [&]() -> int {
+        NMX_CUDA_TRY(cudaEventRecord(eU, R.st));
+        NMX_CUDA_TRY(cudaStreamWaitEvent(P, eU, 0));
+        NMX_CUDA_TRY(cudaStreamWaitEvent(U, eU, 0));
+        int k = 0, kb = std::min(nb, n);
+        int r = panel(k, kb);
+        if (r) return r;
+        NMX_CUDA_TRY(cudaEventRecord(eP, P));
+        float *A = R.A;
+        const int64_t lda = R.lda;
+        while (k + kb < n) {
+            const int next = k + kb, kb2 = std::min(nb, n - next), rest = next + kb2;
+            const int *lst = buf[cur];
+            const int nl = RP.nlists;
+            NMX_CUDA_TRY(cudaStreamWaitEvent(U, eP, 0));
+            NMX_CUDA_TRY(cudaStreamWaitEvent(P, eU, 0));
+            // Panel stream: the next panel's columns, then the next panel.
+            r = calu_swap(P, A, lda, lst, nl, next, rest, 0, 0);
+            if (r) return r;
+            r = trsm_lower<float, true>(gP, A, lda, k, kb, A, lda, next, rest);
+            if (r) return r;
+            r = gP(n - next, kb2, kb, A + (int64_t)next * lda + k, lda, A + (int64_t)k * lda + next,
+                   lda, A + (int64_t)next * lda + next, lda);
+            if (r) return r;
+            cur ^= 1;
+            r = panel(next, kb2);
+            if (r) return r;
+            NMX_CUDA_TRY(cudaEventRecord(eP, P));
+            // Update stream: everything else.
+            r = calu_swap(U, A, lda, lst, nl, 0, k, rest, n);
+            if (r) return r;
+            if (rest < n) {
+                r = trsm_lower<float, true>(gU, A, lda, k, kb, A, lda, rest, n);
+                if (r) return r;
+                r = gU(n - next, n - rest, kb, A + (int64_t)next * lda + k, lda,
+                       A + (int64_t)k * lda + rest, lda, A + (int64_t)next * lda + rest, lda);
+                if (r) return r;
+            }
+            NMX_CUDA_TRY(cudaEventRecord(eU, U));
+            k = next;
+            kb = kb2;
+        }
+        // The last panel's moves on the columns before it.
+        NMX_CUDA_TRY(cudaStreamWaitEvent(U, eP, 0));
+        r = calu_swap(U, A, lda, buf[cur], RP.nlists, 0, k, 0, 0);
+        if (r) return r;
+        NMX_CUDA_TRY(cudaEventRecord(eU, U));
+        NMX_CUDA_TRY(cudaStreamWaitEvent(R.st, eU, 0));
+        return 0;
+    };
+    rc = body();
+    // The main handle goes back to the caller's stream whatever happened.
+    cublasHandle_t h;
+    const int rc2 = ctx_cublas(ctx, R.st, &h);
+    return rc ? rc : rc2;
+}
+
 template <typename T>
 int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
               int32_t *info, bool tournament) {
@@ -1132,6 +884,15 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
         R.cs.carve(cv);
         NMX_CUDA_TRY(cudaMemsetAsync(R.cs.count, 0, sizeof(unsigned) * (kCaluGroup + 1), st));
         R.tournament = true;
+        R.scope_lo = 0;
+        R.scope_hi = (int)n;
+        R.lists = R.cs.lists;
+        if constexpr (std::is_same<T, float>::value) {
+            // Look-ahead panel width: a multiple of 32 in [64, 1024].
+            const int64_t want = ctx->tune_lu_lookahead < 0 ? 512 : ctx->tune_lu_lookahead;
+            const int nb = (int)std::min<int64_t>(1024, want / 32 * 32);
+            if (nb >= 64 && n >= 2 * nb) return getrf_lookahead(R, nb);
+        }
     }
     return getrf2<T>(R, 0, (int)n);
 }

@@ -63,6 +63,11 @@ struct nmx_context {
     void *workspace = nullptr;
     size_t workspace_bytes = 0;
     void *cublas = nullptr;  // cublasHandle_t, created on first dense call
+    void *cublas_aux = nullptr;  // a second handle, for the look-ahead LU's panel stream
+    // The look-ahead LU's panel (high priority) and update streams and the
+    // events that order them, created on first use.
+    cudaStream_t la_stream[2] = {};
+    cudaEvent_t la_event[2] = {};
     // Tuning knobs (nmx_tune_set / nmx_tune_get); 0 means "automatic".
     int64_t tune_lu_leaf_ctas = 0;    // CTAs of the cooperative LU leaf panel
     int64_t tune_ir_trsv_ctas = 0;    // CTAs of the persistent triangular solves
@@ -70,6 +75,7 @@ struct nmx_context {
     int64_t tune_lu_leaf_w = 0;       // widest LU leaf panel (0: 32; multiple of 8, <= 64)
     int64_t tune_ir_tc_min = -1;      // smallest GEMM inner dimension on the tensor cores (-1: 256)
     int64_t tune_lu_tournament = -1;  // tournament-pivoting FP32 leaves (-1: IR only, 0: never, 1: also nmx_getrf_f32)
+    int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the tournament LU (-1: 512, 0: off)
     // Grow-only named device buffers, one per use, kept for the context's life.
     static constexpr int kSlots = 8;
     void *slot_ptr[kSlots] = {};
@@ -81,7 +87,7 @@ struct nmx_context {
 };
 
 namespace nmx {
-enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5, kWsCalu = 6 };
+enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5, kWsCalu = 6, kWsGemm16Panel = 7 };
 }
 
 namespace nmx {

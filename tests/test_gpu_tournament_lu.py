@@ -2,8 +2,9 @@
 factorization (no numax counterpart; opted into for nmx_getrf_f32 by the
 "lu.tournament" knob): P A = L U to FP32 accuracy with LAPACK-style
 interchanges, for panels that one CTA, one group of CTAs and several groups
-pick pivots for; an exactly zero column is reported in info as by partial
-pivoting; and the refinement converges with tournament pivoting on and off."""
+pick pivots for, unblocked and over look-ahead panels; an exactly zero
+column is reported in info as by partial pivoting; and the refinement
+converges with tournament pivoting on and off."""
 import numpy as np
 import pytest
 
@@ -12,15 +13,17 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-def _factor(a, tournament):
+def _factor(a, tournament, lookahead=-1):
     from numax_b200 import _lib, linalg
     lib = _lib.load()
     ctx = _lib.context(torch.cuda.current_device())
     lib.nmx_tune_set(ctx, b"lu.tournament", 1 if tournament else -1)
+    lib.nmx_tune_set(ctx, b"lu.lookahead", lookahead)
     try:
         return linalg.lu_factor(a)
     finally:
         lib.nmx_tune_set(ctx, b"lu.tournament", -1)
+        lib.nmx_tune_set(ctx, b"lu.lookahead", -1)
 
 
 def _residual(a, f):
@@ -61,6 +64,22 @@ def test_tournament_lu_reconstructs(n):
     assert same == (n <= 512)
 
 
+# Look-ahead panels (orders >= 2 panels): ragged last panels, the smallest
+# and the widest panel width, and one matrix with look-ahead off.
+@pytest.mark.parametrize("n,nb", [(700, 64), (1500, 96), (3000, 512), (5000, 1024), (3000, 0)])
+def test_tournament_lu_lookahead_panels(n, nb):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(n + nb)
+    a = torch.randn((n, n), generator=g, dtype=torch.float32, device="cuda")
+    ft = _factor(a, True, nb)
+    fp = _factor(a, False)
+    assert ft.info == 0
+    rt, lt = _residual(a, ft)
+    rp, _ = _residual(a, fp)
+    assert rt <= 10 * rp + 1e-6, (rt, rp)
+    assert lt <= 1e3, lt
+
+
 def test_tournament_lu_zero_column_and_ties():
     n = 700
     g = torch.Generator(device="cuda")
@@ -77,8 +96,8 @@ def test_tournament_lu_zero_column_and_ties():
     assert rt <= 1e-4, rt
 
 
-@pytest.mark.parametrize("tournament", [True, False])
-def test_ir_with_and_without_tournament(tournament):
+@pytest.mark.parametrize("tournament,lookahead", [(True, -1), (True, 0), (False, -1)])
+def test_ir_with_and_without_tournament(tournament, lookahead):
     from numax_b200 import _lib, linalg
     lib = _lib.load()
     ctx = _lib.context(torch.cuda.current_device())
@@ -87,11 +106,13 @@ def test_ir_with_and_without_tournament(tournament):
     a = rng.standard_normal((n, n)) / np.sqrt(n) + 2 * np.eye(n)
     b = rng.standard_normal(n)
     lib.nmx_tune_set(ctx, b"lu.tournament", -1 if tournament else 0)
+    lib.nmx_tune_set(ctx, b"lu.lookahead", lookahead)
     try:
         x, st = linalg.solve_ir(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
                                 precision="bf16x3", tol=1e-14)
     finally:
         lib.nmx_tune_set(ctx, b"lu.tournament", -1)
+        lib.nmx_tune_set(ctx, b"lu.lookahead", -1)
     x = x.cpu().numpy()
     assert st["converged"] == 1, st
     berr = np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max() + np.abs(b).max())
