@@ -76,7 +76,9 @@ NMX_API int nmx_version(void);
  *                   other pivots than numax's): -1 = in the mixed-precision
  *                   LU only, 0 = never, 1 = also in nmx_getrf_f32
  *   "lu.lookahead"  panel width of the tournament-pivoting LU's look-ahead
- *                   (-1 = 512, 0 = unblocked recursion; 64..1024) */
+ *                   (-1 = 256, 0 = unblocked recursion; 64..1024)
+ *   "lu.panel_sms"  SMs the look-ahead keeps free of the update stream's
+ *                   tensor-core GEMMs for the panel stream (-1 or 0 = none) */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);
 NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
 

@@ -154,6 +154,7 @@ static int64_t *tune_slot(nmx_ctx ctx, const char *key) {
     if (!std::strcmp(key, "lu.leaf_w")) return &ctx->tune_lu_leaf_w;
     if (!std::strcmp(key, "lu.tournament")) return &ctx->tune_lu_tournament;
     if (!std::strcmp(key, "lu.lookahead")) return &ctx->tune_lu_lookahead;
+    if (!std::strcmp(key, "lu.panel_sms")) return &ctx->tune_lu_panel_sms;
     return nullptr;
 }
 

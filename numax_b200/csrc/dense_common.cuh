@@ -6,6 +6,7 @@
 
 #include <cublas_v2.h>
 
+#include "gemm_tc.cuh"
 #include "nmx_common.cuh"
 
 namespace nmx {
@@ -117,11 +118,6 @@ int ctx_cublas_aux(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
 // Creates the context's look-ahead streams and events on first use.
 int ctx_lookahead_streams(nmx_ctx ctx);
 
-// Tensor-core update (gemm_tc.cu): C -= round16(A) round16(B), fp32 operands.
-int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
-                    int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
-                    size_t ws_bytes);
-size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision);
 
 // The trailing-update product of the recursive factorizations and solves:
 // C[m x n] -= A[m x k] B[k x n], row-major.  precision 0 keeps the operands'
@@ -134,6 +130,7 @@ struct GemmSub {
     int64_t tc_min = 256;
     void *ws = nullptr;
     size_t ws_bytes = 0;
+    int sm_limit = 0;  // > 0: tensor-core updates on at most this many SMs
     int operator()(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
                    int64_t ldb, double *C, int64_t ldc) const {
         cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
@@ -149,7 +146,8 @@ struct GemmSub {
         // the thin ones near the recursion's leaves stay FP32 (their operand
         // rounding passes and launches would cost more than they save).
         if (precision && n >= tc_min && k >= tc_min)
-            return tc_gemm_sub_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes);
+            return tc_gemm_sub_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes,
+                                   sm_limit);
         cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
         if (s != CUBLAS_STATUS_SUCCESS) {
             set_error("cublasSgemm failed (%d)", (int)s);

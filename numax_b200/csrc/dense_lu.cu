@@ -707,6 +707,11 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
     GemmSub gP = R.gs, gU = R.gs;
     gP.st = P;
     gU.st = U;
+    // Optionally the update stream's tensor-core GEMMs leave SMs to the panel
+    // stream (a static persistent GEMM on the rest).  Off by default: the
+    // hardware-scheduled GEMM already interleaves the panel's kernels.
+    const int64_t keep = ctx->tune_lu_panel_sms < 0 ? 0 : ctx->tune_lu_panel_sms;
+    gU.sm_limit = keep > 0 ? (int)std::max<int64_t>(16, ctx->sm_count - keep) : 0;
     rc = ctx_cublas_aux(ctx, P, &gP.h);
     if (rc) return rc;
     rc = ctx_cublas(ctx, U, &gU.h);
@@ -889,7 +894,7 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
         R.lists = R.cs.lists;
         if constexpr (std::is_same<T, float>::value) {
             // Look-ahead panel width: a multiple of 32 in [64, 1024].
-            const int64_t want = ctx->tune_lu_lookahead < 0 ? 512 : ctx->tune_lu_lookahead;
+            const int64_t want = ctx->tune_lu_lookahead < 0 ? 256 : ctx->tune_lu_lookahead;
             const int nb = (int)std::min<int64_t>(1024, want / 32 * 32);
             if (nb >= 64 && n >= 2 * nb) return getrf_lookahead(R, nb);
         }

@@ -33,7 +33,7 @@ using namespace cute;
 // One complete sm100 GEMM type per 16-bit input type, spelled at namespace
 // scope (the host compiler rejects the dependent carve-out inside a class
 // template).
-#define NMX_TC_GEMM(NAME, ELEM)                                                                  \
+#define NMX_TC_GEMM(NAME, ELEM, SCHED)                                                           \
     namespace NAME {                                                                             \
     using ElementA = ELEM;                                                                       \
     using ElementB = ELEM;                                                                       \
@@ -53,10 +53,10 @@ using namespace cute;
             sizeof(Epi::SharedStorage))>,                                                        \
         cutlass::gemm::collective::KernelScheduleAuto>::CollectiveOp;                            \
     using Kernel = cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Main, Epi,    \
-                                                        void>;                                   \
+                                                        SCHED>;                                  \
     using Gemm = cutlass::gemm::device::GemmUniversalAdapter<Kernel>;                            \
     inline int run(int M, int N, int K, const void *A, int64_t lda, const void *B, int64_t ldb,  \
-                   float *C, int64_t ldc, cudaStream_t st) {                                     \
+                   float *C, int64_t ldc, cudaStream_t st, int sm_count) {                       \
         Kernel::StrideA sa{};                                                                    \
         Kernel::StrideB sb{};                                                                    \
         Kernel::StrideC sc{};                                                                    \
@@ -65,11 +65,17 @@ using namespace cute;
         cute::get<1>(sb) = ldb;                                                                  \
         cute::get<0>(sc) = ldc;                                                                  \
         cute::get<0>(sd) = ldc;                                                                  \
+        cutlass::KernelHardwareInfo hw;                                                          \
+        if (sm_count > 0) {                                                                      \
+            cudaGetDevice(&hw.device_id);                                                        \
+            hw.sm_count = sm_count;                                                              \
+        }                                                                                        \
         Gemm::Arguments args{cutlass::gemm::GemmUniversalMode::kGemm,                            \
                              {M, N, K, 1},                                                       \
                              {static_cast<const ElementA *>(A), sa,                              \
                               static_cast<const ElementB *>(B), sb},                             \
-                             {{-1.0f, 1.0f}, C, sc, C, sd}};                                     \
+                             {{-1.0f, 1.0f}, C, sc, C, sd},                                      \
+                             hw};                                                                \
         Gemm g;                                                                                  \
         if (g.can_implement(args) != cutlass::Status::kSuccess) return 1;                        \
         if (Gemm::get_workspace_size(args) != 0) return 4;                                       \
@@ -78,8 +84,13 @@ using namespace cute;
     }                                                                                            \
     }
 
-NMX_TC_GEMM(bf16, cutlass::bfloat16_t)
-NMX_TC_GEMM(fp16, cutlass::half_t)
+// The default (hardware cluster-launch-control) scheduler takes every SM;
+// the static persistent one runs on at most `sm_count` SMs, leaving the rest
+// to concurrent work (the look-ahead LU's panel stream).
+NMX_TC_GEMM(bf16, cutlass::bfloat16_t, void)
+NMX_TC_GEMM(fp16, cutlass::half_t, void)
+NMX_TC_GEMM(bf16s, cutlass::bfloat16_t, cutlass::gemm::StaticPersistentScheduler)
+NMX_TC_GEMM(fp16s, cutlass::half_t, cutlass::gemm::StaticPersistentScheduler)
 #undef NMX_TC_GEMM
 
 }  // namespace tc
@@ -129,7 +140,7 @@ static inline int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
 
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
                     int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
-                    size_t ws_bytes) {
+                    size_t ws_bytes, int sm_limit) {
     if (M <= 0 || N <= 0 || K <= 0) return 0;
     const int64_t Kp = up8(K), Np = up8(N);
     const size_t need = tc_gemm_workspace_bytes(M, N, K, precision);
@@ -155,7 +166,8 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         round_block_kernel<cutlass::half_t><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N, (int)Kp,
                                                                     (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
-        rc = tc::fp16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st);
+        rc = sm_limit > 0 ? tc::fp16s::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, sm_limit)
+                          : tc::fp16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, 0);
     } else if (precision == NMX_PREC_BF16X3) {
         auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
         auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
@@ -164,7 +176,8 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         round_split_bf16_kernel<false><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N, (int)Kp,
                                                                (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
-        rc = tc::bf16::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st);
+        rc = sm_limit > 0 ? tc::bf16s::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st, sm_limit)
+                          : tc::bf16::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st, 0);
     } else {
         auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
         auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
@@ -173,7 +186,8 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         round_block_kernel<cutlass::bfloat16_t><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N,
                                                                         (int)Kp, (int)Np, b, Np);
         NMX_CUDA_TRY(cudaGetLastError());
-        rc = tc::bf16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st);
+        rc = sm_limit > 0 ? tc::bf16s::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, sm_limit)
+                          : tc::bf16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, 0);
     }
     if (rc) {
         set_error("tensor-core GEMM %lldx%lldx%lld failed at step %d", (long long)M, (long long)N,

@@ -14,10 +14,11 @@ namespace nmx {
 
 // C[M x N] -= round(A)[M x K] * round(B)[K x N], fp32 row-major operands,
 // rounded to BF16 (precision = NMX_PREC_BF16) or FP16 into `ws` first.
-// C must be 16-byte aligned with ldc % 4 == 0.
+// C must be 16-byte aligned with ldc % 4 == 0.  sm_limit > 0 keeps the GEMM
+// on at most that many SMs.
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
                     int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
-                    size_t ws_bytes);
+                    size_t ws_bytes, int sm_limit = 0);
 
 // Workspace tc_gemm_sub_f32 needs for an M x N x K update.
 size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision = NMX_PREC_BF16);

@@ -10,7 +10,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 KEYS = [b"lu.leaf_ctas", b"lu.cluster", b"lu.leaf_w", b"ir.trsv_ctas", b"ir.tc_min",
-        b"lu.tournament", b"lu.lookahead"]
+        b"lu.tournament", b"lu.lookahead", b"lu.panel_sms"]
 
 
 def test_tune_keys_round_trip_and_errors():
