@@ -471,4 +471,92 @@ __global__ void __launch_bounds__(kCaluApplyThreads)
     }
 }
 
+// X := L^-1 X for the unit lower w x w block L at (r, r) of A (w <= 256, a
+// multiple of 32) and X = rows [r, r + w) x columns [c0, c1) of B: the
+// triangular solves of the tournament LU's panels in one kernel, a CTA per
+// 32 columns with X in shared memory.  Warp b inverts the 32 x 32 diagonal
+// block b by forward substitution (lane j forms column j), so each block step
+// is two small products from shared memory: X_b := inv(L_bb) X_b, then
+// X_below -= L_below,b X_b.
+constexpr int kTrsmMaxW = 256;
+constexpr int kTrsmThreads = 256;
+constexpr int kTrsmXPitch = 33;
+constexpr int kTrsmLPitch = 36;  // 16-byte rows for float4 reads
+__host__ __device__ constexpr size_t trsm_unit_lower_smem(int w) {
+    return sizeof(float) * ((size_t)w * kTrsmXPitch * 2 + (size_t)(w - 32) * kTrsmLPitch);
+}
+
+__global__ void __launch_bounds__(kTrsmThreads)
+    trsm_unit_lower_kernel(const float *A, int64_t lda, int r, int w, float *B, int64_t ldb,
+                           int c0, int c1) {
+    extern __shared__ __align__(16) float tsm[];
+    float *X = tsm;                          // [w][33] the CTA's 32 columns of X
+    float *Li = X + w * kTrsmXPitch;         // [w/32][32][33] inverted diagonal blocks
+    float *Ls = Li + w * kTrsmXPitch;        // [w-32][36] L below the current block
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kTrsmThreads / 32;
+    const int nb = w / 32;
+    const int col = c0 + blockIdx.x * 32 + lane;
+    const bool cv = col < c1;
+    for (int i = warp; i < w; i += NW) X[i * kTrsmXPitch + lane] = cv ? B[(int64_t)(r + i) * ldb + col] : 0.f;
+    if (warp < nb) {
+        float *D = Li + warp * 32 * kTrsmXPitch;
+        const int rb = r + 32 * warp;
+        for (int i = 0; i < 32; ++i) D[i * kTrsmXPitch + lane] = A[(int64_t)(rb + i) * lda + rb + lane];
+        __syncwarp();
+        float x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            float t = 0.f;
+#pragma unroll
+            for (int p = 0; p < i; ++p) t = fmaf(D[i * kTrsmXPitch + p], x[p], t);
+            x[i] = i == lane ? 1.f : (i < lane ? 0.f : -t);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) D[i * kTrsmXPitch + lane] = x[i];
+    }
+    __syncthreads();
+    for (int b = 0; b < nb; ++b) {
+        const int rb = 32 * b, below = w - rb - 32;
+        for (int i = warp; i < below; i += NW)
+            Ls[i * kTrsmLPitch + lane] = A[(int64_t)(r + rb + 32 + i) * lda + r + rb + lane];
+        {
+            const float *D = Li + b * 32 * kTrsmXPitch;
+            float y[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+            for (int p = 0; p < 32; ++p) {
+                const float xp = X[(rb + p) * kTrsmXPitch + lane];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) y[q] = fmaf(D[(4 * warp + q) * kTrsmXPitch + p], xp, y[q]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; ++q) X[(rb + 4 * warp + q) * kTrsmXPitch + lane] = y[q];
+        }
+        __syncthreads();
+        if (below > 0) {
+            float xb[32];
+#pragma unroll
+            for (int p = 0; p < 32; ++p) xb[p] = X[(rb + p) * kTrsmXPitch + lane];
+            for (int i = warp; i < below; i += NW) {
+                const float4 *lr = reinterpret_cast<const float4 *>(Ls + i * kTrsmLPitch);
+                float t = 0.f;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float4 l = lr[q];
+                    t = fmaf(l.x, xb[4 * q], t);
+                    t = fmaf(l.y, xb[4 * q + 1], t);
+                    t = fmaf(l.z, xb[4 * q + 2], t);
+                    t = fmaf(l.w, xb[4 * q + 3], t);
+                }
+                X[(rb + 32 + i) * kTrsmXPitch + lane] -= t;
+            }
+        }
+        __syncthreads();
+    }
+    if (cv)
+        for (int i = warp; i < w; i += NW) B[(int64_t)(r + i) * ldb + col] = X[i * kTrsmXPitch + lane];
+}
+
 }  // namespace nmx

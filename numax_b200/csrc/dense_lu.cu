@@ -662,6 +662,28 @@ int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
     return trsm_upper<T, TRANS>(gs, A, lda, r, hw, B, ldb, c0, c1);
 }
 
+// X := L^-1 X (unit lower L, w x w at (r, r) of A; X rows [r, r+w) x cols
+// [c0, c1) of B) for the tournament LU: one kernel for w <= 256 in multiples
+// of 32, else the recursion.
+static int trsm_unit_lower_f32(const GemmSub &gs, const float *A, int64_t lda, int r, int w,
+                               float *B, int64_t ldb, int c0, int c1) {
+    if (w <= 0 || c1 <= c0) return 0;
+    if (w > kTrsmMaxW || w % 32 != 0) return trsm_lower<float, true>(gs, A, lda, r, w, B, ldb, c0, c1);
+    static bool attr_set[64] = {};
+    int dev = 0;
+    NMX_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr_set[dev]) {
+        NMX_CUDA_TRY(cudaFuncSetAttribute(trsm_unit_lower_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)trsm_unit_lower_smem(kTrsmMaxW)));
+        attr_set[dev] = true;
+    }
+    trsm_unit_lower_kernel<<<(unsigned)ceil_div(c1 - c0, 32), kTrsmThreads, trsm_unit_lower_smem(w),
+                             gs.st>>>(A, lda, r, w, B, ldb, c0, c1);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 template <typename T>
 static int getrf2(LuRun<T> &R, int c, int w) {
     const int lw = leaf_width<T>(R, R.n - c);
@@ -672,7 +694,14 @@ static int getrf2(LuRun<T> &R, int c, int w) {
     int rc = getrf2<T>(R, c, hw);
     if (rc) return rc;
     // U12 := L11^-1 A12 over the right half's columns.
-    rc = trsm_lower<T, true>(R.gs, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+    if constexpr (std::is_same<T, float>::value) {
+        if (R.tournament)
+            rc = trsm_unit_lower_f32(R.gs, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+        else
+            rc = trsm_lower<T, true>(R.gs, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+    } else {
+        rc = trsm_lower<T, true>(R.gs, R.A, R.lda, c, hw, R.A, R.lda, c + hw, c + w);
+    }
     if (rc) return rc;
     // A22 -= L21 U12.
     rc = R.gs(R.n - c - hw, w - hw, hw, R.A + (int64_t)(c + hw) * R.lda + c, R.lda,
@@ -752,7 +781,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
             // Panel stream: the next panel's columns, then the next panel.
             r = calu_swap(P, A, lda, lst, nl, next, rest, 0, 0);
             if (r) return r;
-            r = trsm_lower<float, true>(gP, A, lda, k, kb, A, lda, next, rest);
+            r = trsm_unit_lower_f32(gP, A, lda, k, kb, A, lda, next, rest);
             if (r) return r;
             r = gP(n - next, kb2, kb, A + (int64_t)next * lda + k, lda, A + (int64_t)k * lda + next,
                    lda, A + (int64_t)next * lda + next, lda);
@@ -765,7 +794,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
             r = calu_swap(U, A, lda, lst, nl, 0, k, rest, n);
             if (r) return r;
             if (rest < n) {
-                r = trsm_lower<float, true>(gU, A, lda, k, kb, A, lda, rest, n);
+                r = trsm_unit_lower_f32(gU, A, lda, k, kb, A, lda, rest, n);
                 if (r) return r;
                 r = gU(n - next, n - rest, kb, A + (int64_t)next * lda + k, lda,
                        A + (int64_t)k * lda + rest, lda, A + (int64_t)next * lda + rest, lda);
