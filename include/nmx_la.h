@@ -75,8 +75,10 @@ NMX_API int nmx_version(void);
  *   "lu.tournament" FP32 panels by tournament pivoting (a stable LU with
  *                   other pivots than numax's): -1 = in the mixed-precision
  *                   LU only, 0 = never, 1 = also in nmx_getrf_f32
- *   "lu.lookahead"  panel width of the tournament-pivoting LU's look-ahead
- *                   (-1 = 256, 0 = unblocked recursion; 64..1024)
+ *   "lu.lookahead"  look-ahead panel width of the LU (-1 = 256, from order
+ *                   512 with tournament pivoting, from 4096 with numax's
+ *                   pivots; 0 = unblocked recursion; 64..1024, <= 512 with
+ *                   numax's pivots)
  *   "lu.panel_sms"  SMs the look-ahead keeps free of the update stream's
  *                   tensor-core GEMMs for the panel stream (-1 or 0 = none) */
 NMX_API int nmx_tune_set(nmx_ctx ctx, const char *key, int64_t value);

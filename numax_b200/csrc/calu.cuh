@@ -439,10 +439,13 @@ __global__ void __launch_bounds__(kCaluApplyThreads)
 }
 
 // Row moves in columns [a0, a1) and [b0, b1), a column per thread: the
-// lists in order, each list's reads of a column before its writes.
+// lists in order, each list's reads of a column before its writes.  (Any
+// LU leaf's interchanges: the tournament leaves write their lists, the
+// partial-pivoting leaves get theirs from ipiv_moves_kernel.)
+template <typename T>
 __global__ void __launch_bounds__(kCaluApplyThreads)
-    calu_swap_kernel(float *__restrict__ A, int64_t lda, const int *lists, int nlists, int a0,
-                     int a1, int b0, int b1) {
+    calu_swap_kernel(T *__restrict__ A, int64_t lda, const int *lists, int nlists, int a0, int a1,
+                     int b0, int b1) {
     __shared__ int64_t from[2 * kCaluW], to[2 * kCaluW];
     __shared__ int nmv;
     const int tid = threadIdx.x;
@@ -461,7 +464,7 @@ __global__ void __launch_bounds__(kCaluApplyThreads)
         __syncthreads();
         if (!mine) continue;
         const int nm = nmv;
-        float v[2 * kCaluW];
+        T v[2 * kCaluW];
 #pragma unroll
         for (int k = 0; k < 2 * kCaluW; ++k)
             if (k < nm) v[k] = A[from[k] + col];
@@ -557,6 +560,48 @@ __global__ void __launch_bounds__(kTrsmThreads)
     }
     if (cv)
         for (int i = warp; i < w; i += NW) B[(int64_t)(r + i) * ldb + col] = X[i * kTrsmXPitch + lane];
+}
+
+// The row moves of LAPACK-style interchanges ipiv[c .. c+w) (w <= 32), as a
+// list: one warp replays the swaps on the positions they touch (lane k
+// tracks position c + k and, from step k on, possibly one more), then lists
+// every tracked position whose row changed.
+__global__ void ipiv_moves_kernel(const int32_t *ipiv, int c, int w, int *mlist) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int pos0 = c + lane, row0 = c + lane, pos1 = -1, row1 = -1;
+    for (int j = 0; j < w; ++j) {
+        const int cj = c + j, p = ipiv[cj];
+        int h = pos0 == cj ? row0 : (pos1 == cj ? row1 : -1);
+        unsigned m = __ballot_sync(full, h >= 0);
+        const int at_cj = m ? __shfl_sync(full, h, __ffs(m) - 1) : cj;
+        h = pos0 == p ? row0 : (pos1 == p ? row1 : -1);
+        m = __ballot_sync(full, h >= 0);
+        const int at_p = m ? __shfl_sync(full, h, __ffs(m) - 1) : p;
+        const bool tracked = __any_sync(full, pos0 == p || pos1 == p);
+        if (pos0 == cj) row0 = at_p;
+        else if (pos0 == p) row0 = at_cj;
+        if (pos1 == cj) row1 = at_p;
+        else if (pos1 == p) row1 = at_cj;
+        if (!tracked && lane == j) {
+            pos1 = p;
+            row1 = at_cj;
+        }
+    }
+    const bool mv0 = row0 != pos0, mv1 = pos1 >= 0 && row1 != pos1;
+    const unsigned b0 = __ballot_sync(full, mv0), b1 = __ballot_sync(full, mv1);
+    const unsigned lt = (1u << lane) - 1u;
+    if (mv0) {
+        const int i = __popc(b0 & lt);
+        mlist[1 + 2 * i] = row0;
+        mlist[2 + 2 * i] = pos0;
+    }
+    if (mv1) {
+        const int i = __popc(b0) + __popc(b1 & lt);
+        mlist[1 + 2 * i] = row1;
+        mlist[2 + 2 * i] = pos1;
+    }
+    if (lane == 0) mlist[0] = __popc(b0) + __popc(b1);
 }
 
 }  // namespace nmx

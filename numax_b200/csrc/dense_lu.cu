@@ -525,12 +525,39 @@ static int leaf_width(const LuRun<T> &R, int m) {
 }
 
 // Row moves of `nlists` leaves in columns [a0, a1) and [b0, b1).
-static int calu_swap(cudaStream_t st, float *A, int64_t lda, const int *lists, int nlists, int a0,
+template <typename T>
+static int calu_swap(cudaStream_t st, T *A, int64_t lda, const int *lists, int nlists, int a0,
                      int a1, int b0, int b1) {
     const int cols = std::max(0, a1 - a0) + std::max(0, b1 - b0);
     if (cols == 0 || nlists == 0) return 0;
-    calu_swap_kernel<<<(unsigned)ceil_div(cols, kCaluApplyThreads), kCaluApplyThreads, 0, st>>>(
+    calu_swap_kernel<T><<<(unsigned)ceil_div(cols, kCaluApplyThreads), kCaluApplyThreads, 0, st>>>(
         A, lda, lists, nlists, a0, std::max(a0, a1), b0, std::max(b0, b1));
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// The next slot for a leaf's row moves (unblocked, slots recycle: each list
+// is applied at once).
+template <typename T>
+static int *leaf_list(LuRun<T> &R) {
+    if (R.nlists >= kCaluMaxLists) R.nlists = 0;
+    return R.lists + (size_t)R.nlists++ * kCaluListStride;
+}
+
+// A partial-pivoting leaf's interchanges on the other columns in scope: as a
+// row-move list for leaves of <= 32 columns, else swap by swap (unblocked
+// runs only).
+template <typename T>
+static int leaf_swap(LuRun<T> &R, int c, int w) {
+    if (w <= kCaluW) {
+        int *ml = leaf_list(R);
+        ipiv_moves_kernel<<<1, 32, 0, R.st>>>(R.ipiv, c, w, ml);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return calu_swap<T>(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
+    }
+    const int threads = 256;
+    laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(R.A, R.lda, R.n, c, w,
+                                                                             R.ipiv, c, c + w);
     NMX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -541,21 +568,18 @@ static int calu_leaf(LuRun<float> &R, int c, int w) {
     const int m = R.n - c;
     const int nctas = (int)ceil_div(m, kCaluRows);
     const bool vec = R.lda % 4 == 0 && reinterpret_cast<uintptr_t>(R.A) % 16 == 0;
-    // Unblocked, the lists are used at once and their slots recycle.
-    if (R.nlists >= kCaluMaxLists) R.nlists = 0;
-    int *ml = R.lists + (size_t)R.nlists++ * kCaluListStride;
+    int *ml = leaf_list(R);
     calu_pick_kernel<<<nctas, kCaluThreads, 0, R.st>>>(R.A, R.lda, R.n, c, w, nctas, vec, R.cs,
                                                     R.ipiv, R.info, ml);
     calu_apply_kernel<<<(unsigned)ceil_div(m, kCaluApplyThreads), kCaluApplyThreads,
                         kCaluApplySmem, R.st>>>(R.A, R.lda, R.n, c, w, R.cs, ml);
     NMX_CUDA_TRY(cudaGetLastError());
-    return calu_swap(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
+    return calu_swap<float>(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
 }
 
 template <typename T>
 static int leaf(LuRun<T> &R, int c, int w) {
     const int m = R.n - c;
-    const int threads = 256;
     if constexpr (std::is_same<T, float>::value) {
         if (R.tournament) return calu_leaf(R, c, w);
     }
@@ -575,10 +599,7 @@ static int leaf(LuRun<T> &R, int c, int w) {
         cfg.numAttrs = 1;
         NMX_CUDA_TRY(cudaLaunchKernelEx(&cfg, getrf_cluster_leaf_kernel<T>, R.A, R.lda, R.n, c, w,
                                         rpc, R.ipiv, R.info));
-        laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(
-            R.A, R.lda, R.n, c, w, R.ipiv, c, c + w);
-        NMX_CUDA_TRY(cudaGetLastError());
-        return 0;
+        return leaf_swap(R, c, w);
     }
     int G = (int)std::min<int64_t>(R.max_ctas, ceil_div(m, 32));
     G = std::max(G, 1);
@@ -592,11 +613,7 @@ static int leaf(LuRun<T> &R, int c, int w) {
     void *args[] = {&R.A, &R.lda, &R.n, &c, &w, &rpc, &R.ipiv, &R.info, &R.sc};
     NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)getrf_leaf_kernel<T>, dim3(G),
                                              dim3(kLeafThreads), args, smem, R.st));
-    // The interchanges across the rest of the width.
-    laswp_kernel<T><<<(unsigned)ceil_div(R.n, threads), threads, 0, R.st>>>(R.A, R.lda, R.n, c, w,
-                                                                             R.ipiv, c, c + w);
-    NMX_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return leaf_swap(R, c, w);
 }
 
 // X := L^-1 X, L the w x w lower block at (r, r) of A, X rows [r, r+w) cols [c0, c1) of B.
@@ -726,7 +743,18 @@ static int getrf2(LuRun<T> &R, int c, int w) {
 // panel stream starts step i+1 after the update stream's step i (which
 // updated panel i+2's columns); the update stream starts step i after panel
 // i is factored.  The leaves' move lists alternate between two buffers.
-static int getrf_lookahead(LuRun<float> &R, int nb) {
+// U12 := L11^-1 A12 for the look-ahead steps.
+template <typename T>
+static int la_trsm(const GemmSub &gs, bool tournament, T *A, int64_t lda, int k, int kb, int c0,
+                   int c1) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (tournament) return trsm_unit_lower_f32(gs, A, lda, k, kb, A, lda, c0, c1);
+    }
+    return trsm_lower<T, true>(gs, A, lda, k, kb, A, lda, c0, c1);
+}
+
+template <typename T>
+static int getrf_lookahead(LuRun<T> &R, int nb) {
     nmx_ctx ctx = R.ctx;
     const int n = R.n;
     int rc = ctx_lookahead_streams(ctx);
@@ -750,7 +778,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
         rc = ctx->ensure_slot(kWsGemm16Panel, gP.ws_bytes, &gP.ws);
         if (rc) return rc;
     }
-    LuRun<float> RP = R;
+    LuRun<T> RP = R;
     RP.st = P;
     RP.gs = gP;
     int *buf[2] = {R.cs.lists, R.cs.lists + (size_t)kCaluMaxLists * kCaluListStride};
@@ -760,7 +788,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
         RP.scope_hi = k + kb;
         RP.lists = buf[cur];
         RP.nlists = 0;
-        return getrf2<float>(RP, k, kb);
+        return getrf2<T>(RP, k, kb);
     };
     auto body = [&]() -> int {
         NMX_CUDA_TRY(cudaEventRecord(eU, R.st));
@@ -770,7 +798,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
         int r = panel(k, kb);
         if (r) return r;
         NMX_CUDA_TRY(cudaEventRecord(eP, P));
-        float *A = R.A;
+        T *A = R.A;
         const int64_t lda = R.lda;
         while (k + kb < n) {
             const int next = k + kb, kb2 = std::min(nb, n - next), rest = next + kb2;
@@ -779,9 +807,9 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
             NMX_CUDA_TRY(cudaStreamWaitEvent(U, eP, 0));
             NMX_CUDA_TRY(cudaStreamWaitEvent(P, eU, 0));
             // Panel stream: the next panel's columns, then the next panel.
-            r = calu_swap(P, A, lda, lst, nl, next, rest, 0, 0);
+            r = calu_swap<T>(P, A, lda, lst, nl, next, rest, 0, 0);
             if (r) return r;
-            r = trsm_unit_lower_f32(gP, A, lda, k, kb, A, lda, next, rest);
+            r = la_trsm<T>(gP, R.tournament, A, lda, k, kb, next, rest);
             if (r) return r;
             r = gP(n - next, kb2, kb, A + (int64_t)next * lda + k, lda, A + (int64_t)k * lda + next,
                    lda, A + (int64_t)next * lda + next, lda);
@@ -791,10 +819,10 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
             if (r) return r;
             NMX_CUDA_TRY(cudaEventRecord(eP, P));
             // Update stream: everything else.
-            r = calu_swap(U, A, lda, lst, nl, 0, k, rest, n);
+            r = calu_swap<T>(U, A, lda, lst, nl, 0, k, rest, n);
             if (r) return r;
             if (rest < n) {
-                r = trsm_unit_lower_f32(gU, A, lda, k, kb, A, lda, rest, n);
+                r = la_trsm<T>(gU, R.tournament, A, lda, k, kb, rest, n);
                 if (r) return r;
                 r = gU(n - next, n - rest, kb, A + (int64_t)next * lda + k, lda,
                        A + (int64_t)k * lda + rest, lda, A + (int64_t)next * lda + rest, lda);
@@ -806,7 +834,7 @@ static int getrf_lookahead(LuRun<float> &R, int nb) {
         }
         // The last panel's moves on the columns before it.
         NMX_CUDA_TRY(cudaStreamWaitEvent(U, eP, 0));
-        r = calu_swap(U, A, lda, buf[cur], RP.nlists, 0, k, 0, 0);
+        r = calu_swap<T>(U, A, lda, buf[cur], RP.nlists, 0, k, 0, 0);
         if (r) return r;
         NMX_CUDA_TRY(cudaEventRecord(eU, U));
         NMX_CUDA_TRY(cudaStreamWaitEvent(R.st, eU, 0));
@@ -910,23 +938,33 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
                           ? (int)std::min<int64_t>(kLeafMax, ctx->tune_lu_leaf_w / 8 * 8)
                           : kLeafW;
     LuRun<T> R{ctx, st, gs, A, lda, (int)n, ipiv, info, sc, leaf_ctas, cluster, std::max(8, max_w)};
+    // Every leaf leaves its row moves in a list (applied at once, or later to
+    // the columns outside a look-ahead panel).
+    void *cv = nullptr;
+    rc = ctx->ensure_slot(kWsCalu, CaluScratch::bytes(), &cv);
+    if (rc) return rc;
+    R.cs.carve(cv);
+    R.scope_lo = 0;
+    R.scope_hi = (int)n;
+    R.lists = R.cs.lists;
     // Tournament pivoting: FP32 panels of up to 131072 rows.
     if (std::is_same<T, float>::value && tournament && n <= (int64_t)kCaluMaxCtas * kCaluRows) {
-        void *cv = nullptr;
-        rc = ctx->ensure_slot(kWsCalu, CaluScratch::bytes(), &cv);
-        if (rc) return rc;
-        R.cs.carve(cv);
         NMX_CUDA_TRY(cudaMemsetAsync(R.cs.count, 0, sizeof(unsigned) * (kCaluGroup + 1), st));
         R.tournament = true;
-        R.scope_lo = 0;
-        R.scope_hi = (int)n;
-        R.lists = R.cs.lists;
-        if constexpr (std::is_same<T, float>::value) {
-            // Look-ahead panel width: a multiple of 32 in [64, 1024].
-            const int64_t want = ctx->tune_lu_lookahead < 0 ? 256 : ctx->tune_lu_lookahead;
-            const int nb = (int)std::min<int64_t>(1024, want / 32 * 32);
-            if (nb >= 64 && n >= 2 * nb) return getrf_lookahead(R, nb);
-        }
+    }
+    // Look-ahead panel width: a multiple of 32 in [64, 1024] (tournament
+    // leaves), [64, 512] otherwise (leaves as narrow as 8 columns must fit
+    // the panel's move lists); leaves of more than 32 columns run unblocked.
+    // With numax's pivots the look-ahead starts at order 4096 by default (a
+    // tuned width applies from two panels): below that the leaves' latency
+    // is all there is to hide, and the unblocked recursion keeps its
+    // summation order.
+    {
+        const bool tuned = ctx->tune_lu_lookahead >= 0;
+        const int64_t want = tuned ? ctx->tune_lu_lookahead : 256;
+        const int nb = (int)std::min<int64_t>(R.tournament ? 1024 : 512, want / 32 * 32);
+        const int64_t from = (R.tournament || tuned) ? 2 * nb : std::max(2 * nb, 4096);
+        if (nb >= 64 && n >= from && R.max_w <= kCaluW) return getrf_lookahead(R, nb);
     }
     return getrf2<T>(R, 0, (int)n);
 }

@@ -75,7 +75,7 @@ struct nmx_context {
     int64_t tune_lu_leaf_w = 0;       // widest LU leaf panel (0: 32; multiple of 8, <= 64)
     int64_t tune_ir_tc_min = -1;      // smallest GEMM inner dimension on the tensor cores (-1: 256)
     int64_t tune_lu_tournament = -1;  // tournament-pivoting FP32 leaves (-1: IR only, 0: never, 1: also nmx_getrf_f32)
-    int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the tournament LU (-1: 256, 0: off)
+    int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the LU (-1: 256, 0: off)
     int64_t tune_lu_panel_sms = -1;   // SMs the look-ahead keeps free of the update GEMMs (-1, 0: none)
     // Grow-only named device buffers, one per use, kept for the context's life.
     static constexpr int kSlots = 8;

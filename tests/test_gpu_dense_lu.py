@@ -161,3 +161,27 @@ def test_lu_leaf_paths_match_lapack(cluster):
     np.testing.assert_array_equal(f.pivots.cpu().numpy(), piv)
     assert f.info == 0
     assert rel(f.factored.cpu().numpy(), lu) <= 1e-12
+
+
+# The look-ahead LU (panels on two streams, leaves' interchanges deferred as
+# row-move lists): numax's pivots exactly, the factors to rounding.
+@pytest.mark.parametrize("n,nb", [(700, 64), (1500, 256), (2100, 512)])
+def test_lu_lookahead_matches_lapack(n, nb):
+    import scipy.linalg as sl
+    from numax_b200 import _lib
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    rng = np.random.Generator(np.random.PCG64(4000 + n))
+    a = rng.standard_normal((n, n))
+    lib.nmx_tune_set(ctx, b"lu.lookahead", nb)
+    try:
+        f = gpu_lu(a)
+    finally:
+        lib.nmx_tune_set(ctx, b"lu.lookahead", -1)
+    lu, piv = sl.lu_factor(a)
+    np.testing.assert_array_equal(f.pivots.cpu().numpy(), piv)
+    assert rel(f.factored.cpu().numpy(), lu) <= 1e-12
+    b = rng.standard_normal((n, 4))
+    x = f.solve(torch.from_numpy(b).cuda()).cpu().numpy()
+    berr = np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max())
+    assert berr <= 1e-14, berr
