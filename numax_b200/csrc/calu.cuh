@@ -570,8 +570,9 @@ __global__ void ipiv_moves_kernel(const int32_t *ipiv, int c, int w, int *mlist)
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int pos0 = c + lane, row0 = c + lane, pos1 = -1, row1 = -1;
+    const int mine = lane < w ? ipiv[c + lane] : 0;
     for (int j = 0; j < w; ++j) {
-        const int cj = c + j, p = ipiv[cj];
+        const int cj = c + j, p = __shfl_sync(full, mine, j);
         int h = pos0 == cj ? row0 : (pos1 == cj ? row1 : -1);
         unsigned m = __ballot_sync(full, h >= 0);
         const int at_cj = m ? __shfl_sync(full, h, __ffs(m) - 1) : cj;
