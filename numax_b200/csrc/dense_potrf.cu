@@ -97,6 +97,91 @@ __global__ void trsm_right_lt_leaf_kernel(T *A, int64_t lda, int c, int w, int r
         if (j < w) row[j] = x[j];
 }
 
+// X := X L^-T in one kernel for w <= 256 (a multiple of 32): a CTA per 32
+// rows of X, held in shared memory.  Warp b first inverts the 32 x 32
+// diagonal block b of L (lane j forms column j of the inverse by forward
+// substitution), then block by block: X_b -= Y_<b L_b,<b^T (a product with
+// L's block row staged transposed in shared memory), Y_b = X_b L_bb^-T.
+constexpr int kCholTrsmMaxW = 256;
+constexpr int kCholTrsmThreads = 256;
+template <typename T>
+__host__ __device__ constexpr size_t chol_trsm_smem(int w) {
+    return sizeof(T) * ((size_t)32 * (w + 1) + (size_t)w * 33 + (size_t)w * 34);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCholTrsmThreads)
+    trsm_right_lt_small_kernel(T *A, int64_t lda, int c, int w, int r0, int r1) {
+    extern __shared__ __align__(16) unsigned char chol_smem[];
+    const int xp = w + 1;
+    T *X = reinterpret_cast<T *>(chol_smem);  // [32][w+1] the CTA's rows
+    T *Li = X + 32 * xp;                      // [w/32][32][33] inverted diagonal blocks
+    T *Lt = Li + w * 33;                      // [w][34] L's block row b, transposed
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kCholTrsmThreads / 32;
+    const int nb = w / 32;
+    const int rb = r0 + 32 * blockIdx.x, nr = min(32, r1 - rb);
+    for (int i = warp; i < 32; i += NW)
+        for (int q = lane; q < w; q += 32)
+            X[i * xp + q] = i < nr ? A[(int64_t)(rb + i) * lda + c + q] : T(0);
+    if (warp < nb) {
+        T *D = Li + warp * 32 * 33;
+        const int cb = c + 32 * warp;
+        for (int i = 0; i < 32; ++i) D[i * 33 + lane] = A[(int64_t)(cb + i) * lda + cb + lane];
+        __syncwarp();
+        const T my_rd = T(1) / D[lane * 33 + lane];
+        T x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            T t = T(0);
+#pragma unroll
+            for (int p = 0; p < i; ++p) t = fma(D[i * 33 + p], x[p], t);
+            const T rdi = __shfl_sync(0xffffffffu, my_rd, i);
+            x[i] = i == lane ? rdi : (i < lane ? T(0) : -t * rdi);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) D[i * 33 + lane] = x[i];
+    }
+    __syncthreads();
+    const int i = tid >> 3, q0 = (tid & 7) * 4;  // this thread's row and 4 columns of a block
+    for (int b = 0; b < nb; ++b) {
+        const int cb = 32 * b;
+        // L's rows [cb, cb+32) x columns [0, cb), transposed: Lt[p][q] = L[cb+q][p].
+        for (int q = warp; q < 32; q += NW)
+            for (int p = lane; p < cb; p += 32) Lt[p * 34 + q] = A[(int64_t)(c + cb + q) * lda + c + p];
+        __syncthreads();
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+        for (int p = 0; p < cb; ++p) {
+            const T xv = X[i * xp + p];
+            const T *lt = Lt + p * 34 + q0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[k] = fma(xv, lt[k], acc[k]);
+        }
+        T z[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) z[k] = X[i * xp + cb + q0 + k] - acc[k];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) X[i * xp + cb + q0 + k] = z[k];
+        __syncthreads();
+        // Y_b = Z_b Dinv^T: y_q = sum_{p <= q} z_p Dinv[q][p].
+        const T *D = Li + b * 32 * 33;
+        T y[4] = {T(0), T(0), T(0), T(0)};
+        for (int p = 0; p < 32; ++p) {
+            const T zp = X[i * xp + cb + p];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) y[k] = fma(zp, D[(q0 + k) * 33 + p], y[k]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) X[i * xp + cb + q0 + k] = y[k];
+        __syncthreads();
+    }
+    for (int r = warp; r < nr; r += NW)
+        for (int q = lane; q < w; q += 32) A[(int64_t)(rb + r) * lda + c + q] = X[r * xp + q];
+}
+
 template <typename T>
 __global__ void zero_upper_kernel(T *A, int64_t lda, int n) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -123,6 +208,21 @@ template <typename T>
 static int trsm_right_lt(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c, int w, int r0,
                          int r1) {
     if (w <= 0 || r1 <= r0) return 0;
+    if (w > kCholLeaf && w <= kCholTrsmMaxW && w % 32 == 0) {
+        static bool attr_set[64] = {};
+        int dev = 0;
+        NMX_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 64 && !attr_set[dev]) {
+            NMX_CUDA_TRY(cudaFuncSetAttribute(trsm_right_lt_small_kernel<T>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)chol_trsm_smem<T>(kCholTrsmMaxW)));
+            attr_set[dev] = true;
+        }
+        trsm_right_lt_small_kernel<T><<<(unsigned)ceil_div(r1 - r0, 32), kCholTrsmThreads,
+                                        chol_trsm_smem<T>(w), st>>>(A, lda, c, w, r0, r1);
+        NMX_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     if (w <= kCholLeaf) {
         const int threads = 128;
         trsm_right_lt_leaf_kernel<T>
