@@ -841,6 +841,15 @@ static int getrf_lookahead(LuRun<T> &R, int nb) {
         return 0;
     };
     rc = body();
+    if (rc) {
+        // On an error the caller's stream still waits for whatever both
+        // streams already hold, so nothing queued there outlives the call's
+        // ordering.
+        cudaEventRecord(eP, P);
+        cudaStreamWaitEvent(R.st, eP, 0);
+        cudaEventRecord(eU, U);
+        cudaStreamWaitEvent(R.st, eU, 0);
+    }
     // The main handle goes back to the caller's stream whatever happened.
     cublasHandle_t h;
     const int rc2 = ctx_cublas(ctx, R.st, &h);
