@@ -350,18 +350,64 @@ __global__ void __launch_bounds__(kCaluThreads)
     calu_finish(R, np, c, s, ipiv, info, mlist, sh);
 }
 
+// Row moves in columns [a0, a1) and [b0, b1), a column per thread (CTA
+// `cta` of the ones covering them): the lists in order, each list's reads of
+// a column before its writes.  (Any LU leaf's interchanges: the tournament
+// leaves write their lists, the partial-pivoting leaves get theirs from
+// ipiv_moves_kernel.)  from/to/nmv: shared scratch.
+template <typename T>
+__device__ __forceinline__ void calu_swap_cta(T *__restrict__ A, int64_t lda, const int *lists,
+                                              int nlists, int a0, int a1, int b0, int b1, int cta,
+                                              int64_t *from, int64_t *to, int *nmv) {
+    const int tid = threadIdx.x;
+    const int t = cta * kCaluApplyThreads + tid;
+    const int na = a1 - a0;
+    const int col = t < na ? a0 + t : b0 + (t - na);
+    const bool mine = t < na || col < b1;
+    for (int l = 0; l < nlists; ++l) {
+        const int *ml = lists + (size_t)l * kCaluListStride;
+        __syncthreads();
+        if (tid < 2 * kCaluW) {
+            from[tid] = (int64_t)ml[1 + 2 * tid] * lda;
+            to[tid] = (int64_t)ml[2 + 2 * tid] * lda;
+        }
+        if (tid == 0) *nmv = ml[0];
+        __syncthreads();
+        if (!mine) continue;
+        const int nm = *nmv;
+        T v[2 * kCaluW];
+#pragma unroll
+        for (int k = 0; k < 2 * kCaluW; ++k)
+            if (k < nm) v[k] = A[from[k] + col];
+#pragma unroll
+        for (int k = 0; k < 2 * kCaluW; ++k)
+            if (k < nm) A[to[k] + col] = v[k];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCaluApplyThreads)
+    calu_swap_kernel(T *__restrict__ A, int64_t lda, const int *lists, int nlists, int a0, int a1,
+                     int b0, int b1) {
+    __shared__ int64_t from[2 * kCaluW], to[2 * kCaluW];
+    __shared__ int nmv;
+    calu_swap_cta<T>(A, lda, lists, nlists, a0, a1, b0, b1, blockIdx.x, from, to, &nmv);
+}
+
 // After the pivot search: 256 rows of the panel per CTA, staged through
 // shared memory so global accesses are whole rows.  A pivot row is skipped
 // (its place c + j gets L11\U11 row j), every other row becomes
 // l = a U11^-1 at its final position.  No row is read by one CTA and written
 // by another: displaced rows land on the pivots' old places, which their own
 // CTAs leave alone, and rows c .. c+w-1 are read and written by CTA 0 alone.
+// CTAs past panel_ctas move the leaf's rows in the other columns in scope,
+// [a0, a1) and [b0, b1) (disjoint from the panel's columns).
 constexpr int kCaluApplyPitch = kCaluW + 1;
 constexpr size_t kCaluApplySmem = sizeof(float) * kCaluApplyThreads * kCaluApplyPitch;
 
 __global__ void __launch_bounds__(kCaluApplyThreads)
     calu_apply_kernel(float *A, int64_t lda, int n, int c, int w, CaluScratch s,
-                      const int *mlist) {
+                      const int *mlist, int panel_ctas, int a0, int a1, int b0, int b1) {
     __shared__ __align__(16) float U[kCaluW][kCaluW];
     __shared__ float rd[kCaluW];
     __shared__ int gp[kCaluW];
@@ -369,17 +415,33 @@ __global__ void __launch_bounds__(kCaluApplyThreads)
     __shared__ int dst[kCaluApplyThreads];
     __shared__ int nmv;
     extern __shared__ __align__(16) float tile[];  // [256][33] the CTA's rows
+    __shared__ int64_t mfrom[2 * kCaluW], mto[2 * kCaluW];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if ((int)blockIdx.x >= panel_ctas) {
+        calu_swap_cta<float>(A, lda, mlist, 1, a0, a1, b0, b1, (int)blockIdx.x - panel_ctas, mfrom,
+                             mto, &nmv);
+        return;
+    }
     for (int e = tid; e < 4 * kCaluW; e += kCaluApplyThreads) mv[e] = mlist[1 + e];
     for (int e = tid; e < kCaluW * kCaluW; e += kCaluApplyThreads) (&U[0][0])[e] = s.lu[e];
     if (tid < kCaluW) gp[tid] = s.gp[tid];
     if (tid == 0) nmv = mlist[0];
     const int r0 = c + blockIdx.x * kCaluApplyThreads;
     const int nrows = min(kCaluApplyThreads, n - r0);
-    // The CTA's rows into the tile, a warp per row, lanes over columns.
-    for (int r = warp; r < nrows; r += kCaluApplyThreads / 32)
-        tile[r * kCaluApplyPitch + lane] =
-            lane < w ? A[(int64_t)(r0 + r) * lda + c + lane] : 0.f;
+    // The CTA's rows into the tile, a warp per row, lanes over columns, eight
+    // rows' loads in flight per warp.
+    constexpr int NW = kCaluApplyThreads / 32;
+#pragma unroll
+    for (int r8 = 0; r8 < kCaluApplyThreads / NW; r8 += 8) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int r = warp + NW * (r8 + u);
+            v[u] = (r < nrows && lane < w) ? A[(int64_t)(r0 + r) * lda + c + lane] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) tile[(warp + NW * (r8 + u)) * kCaluApplyPitch + lane] = v[u];
+    }
     __syncthreads();
     if (tid < kCaluW) {
         float d = U[tid][tid];
@@ -428,50 +490,16 @@ __global__ void __launch_bounds__(kCaluApplyThreads)
         for (int j = 0; j < kCaluW; ++j) t[j] = x[j];
     }
     __syncthreads();
-    for (int r = warp; r < nrows; r += kCaluApplyThreads / 32) {
-        const int d = dst[r];
+#pragma unroll 8
+    for (int k = 0; k < kCaluApplyThreads / NW; ++k) {
+        const int r = warp + NW * k;
+        const int d = r < nrows ? dst[r] : -1;
         if (d >= 0 && lane < w) A[(int64_t)d * lda + c + lane] = tile[r * kCaluApplyPitch + lane];
     }
     // Rows c .. c+w-1: the pivots' L11\U11 (CTA 0, after its reads above).
     if (blockIdx.x == 0)
         for (int r = warp; r < w; r += kCaluApplyThreads / 32)
             if (lane < w) A[(int64_t)(c + r) * lda + c + lane] = U[r][lane];
-}
-
-// Row moves in columns [a0, a1) and [b0, b1), a column per thread: the
-// lists in order, each list's reads of a column before its writes.  (Any
-// LU leaf's interchanges: the tournament leaves write their lists, the
-// partial-pivoting leaves get theirs from ipiv_moves_kernel.)
-template <typename T>
-__global__ void __launch_bounds__(kCaluApplyThreads)
-    calu_swap_kernel(T *__restrict__ A, int64_t lda, const int *lists, int nlists, int a0, int a1,
-                     int b0, int b1) {
-    __shared__ int64_t from[2 * kCaluW], to[2 * kCaluW];
-    __shared__ int nmv;
-    const int tid = threadIdx.x;
-    const int t = blockIdx.x * kCaluApplyThreads + tid;
-    const int na = a1 - a0;
-    const int col = t < na ? a0 + t : b0 + (t - na);
-    const bool mine = t < na || col < b1;
-    for (int l = 0; l < nlists; ++l) {
-        const int *ml = lists + (size_t)l * kCaluListStride;
-        __syncthreads();
-        if (tid < 2 * kCaluW) {
-            from[tid] = (int64_t)ml[1 + 2 * tid] * lda;
-            to[tid] = (int64_t)ml[2 + 2 * tid] * lda;
-        }
-        if (tid == 0) nmv = ml[0];
-        __syncthreads();
-        if (!mine) continue;
-        const int nm = nmv;
-        T v[2 * kCaluW];
-#pragma unroll
-        for (int k = 0; k < 2 * kCaluW; ++k)
-            if (k < nm) v[k] = A[from[k] + col];
-#pragma unroll
-        for (int k = 0; k < 2 * kCaluW; ++k)
-            if (k < nm) A[to[k] + col] = v[k];
-    }
 }
 
 // X := L^-1 X for the unit lower w x w block L at (r, r) of A (w <= 256, a

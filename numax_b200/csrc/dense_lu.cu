@@ -571,10 +571,15 @@ static int calu_leaf(LuRun<float> &R, int c, int w) {
     int *ml = leaf_list(R);
     calu_pick_kernel<<<nctas, kCaluThreads, 0, R.st>>>(R.A, R.lda, R.n, c, w, nctas, vec, R.cs,
                                                     R.ipiv, R.info, ml);
-    calu_apply_kernel<<<(unsigned)ceil_div(m, kCaluApplyThreads), kCaluApplyThreads,
-                        kCaluApplySmem, R.st>>>(R.A, R.lda, R.n, c, w, R.cs, ml);
+    // The panel's rows and, in the same launch, the moves in the other
+    // columns in scope.
+    const int panel = (int)ceil_div(m, kCaluApplyThreads);
+    const int cols = (c - R.scope_lo) + (R.scope_hi - c - w);
+    calu_apply_kernel<<<(unsigned)(panel + ceil_div(cols, kCaluApplyThreads)), kCaluApplyThreads,
+                        kCaluApplySmem, R.st>>>(R.A, R.lda, R.n, c, w, R.cs, ml, panel,
+                                                R.scope_lo, c, c + w, R.scope_hi);
     NMX_CUDA_TRY(cudaGetLastError());
-    return calu_swap<float>(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
+    return 0;
 }
 
 template <typename T>
