@@ -1,4 +1,6 @@
-// Tournament-pivoting (CALU) panel kernels for the FP32 LU (dense_lu.cu).
+// LU panel kernels (dense_lu.cu): the tournament-pivoting (CALU) leaf and
+// the one-kernel panel TRSM of the FP32 factorization, and the row-move
+// kernels that carry any leaf's interchanges to the other columns.
 #pragma once
 
 #include <cstddef>
@@ -27,9 +29,10 @@ namespace nmx {
 //      pivot rows and hold L11\U11.  It writes them, the LAPACK-style
 //      interchanges and the list of rows that change place.
 // A second kernel solves every other row against U11 (l = a U11^-1, rows
-// independent) and moves rows to their final positions across the whole
-// width.  The pivot search costs one CTA barrier per column instead of one
-// grid- or cluster-wide exchange.  A zero U11 diagonal is floored to 1e-30
+// independent), puts the panel's rows in their final places and, in extra
+// CTAs, moves the same rows in the other columns in scope.  The pivot search
+// costs one CTA barrier per column instead of one grid- or cluster-wide
+// exchange.  A zero U11 diagonal is floored to 1e-30
 // and the first one reported in info; a column without a nonzero candidate
 // picks the lowest row.
 constexpr int kCaluRows = 512;                          // rows per CTA
@@ -41,7 +44,9 @@ constexpr int kCaluMaxCtas = kCaluGroup * kCaluGroup;   // panels of up to 13107
 constexpr int kCaluApplyThreads = 256;
 // A leaf's row moves: the count, then up to 2 kCaluW (from, to) row pairs.
 constexpr int kCaluListStride = 1 + 4 * kCaluW;
-constexpr int kCaluMaxLists = 64;  // leaves of one look-ahead panel (<= 2048 columns)
+// Leaves of one look-ahead panel: <= 2048 columns of tournament leaves, <= 512
+// of partial-pivoting leaves (which can be as narrow as 8 columns).
+constexpr int kCaluMaxLists = 64;
 
 struct CaluScratch {
     int *cand;        // [kCaluMaxCtas][kCaluW] first-level picks (global rows, -1: none)
