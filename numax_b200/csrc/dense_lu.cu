@@ -978,7 +978,14 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
         const int64_t want = tuned ? ctx->tune_lu_lookahead : 256;
         const int nb = (int)std::min<int64_t>(R.tournament ? 1024 : 512, want / 32 * 32);
         const int64_t from = (R.tournament || tuned) ? 2 * nb : std::max(2 * nb, 4096);
-        if (nb >= 64 && n >= from && R.max_w <= kCaluW) return getrf_lookahead(R, nb);
+        // With numax's pivots every leaf must be a cluster leaf: a cooperative
+        // grid leaf on the panel stream could not count on all its CTAs being
+        // resident beside the update stream's kernels.
+        const bool leaves_ok =
+            R.tournament ||
+            (R.cluster > 0 && cluster_leaf_smem<T>((int)n, 8, R.cluster) + 2048 <= ctx->smem_optin);
+        if (nb >= 64 && n >= from && R.max_w <= kCaluW && leaves_ok)
+            return getrf_lookahead(R, nb);
     }
     return getrf2<T>(R, 0, (int)n);
 }
