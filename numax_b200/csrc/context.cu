@@ -44,10 +44,26 @@ int ctx_lookahead_streams(nmx_ctx ctx) {
     if (ctx->la_stream[0]) return 0;
     int least = 0, greatest = 0;
     NMX_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    NMX_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[0], cudaStreamNonBlocking, greatest));
-    NMX_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[1], cudaStreamNonBlocking, least));
-    for (int i = 0; i < 2; ++i)
-        NMX_CUDA_TRY(cudaEventCreateWithFlags(&ctx->la_event[i], cudaEventDisableTiming));
+    // All four objects or none: the context keeps them only when every one
+    // was created.
+    cudaStream_t s[2] = {};
+    cudaEvent_t e[2] = {};
+    cudaError_t err = cudaStreamCreateWithPriority(&s[0], cudaStreamNonBlocking, greatest);
+    if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&s[1], cudaStreamNonBlocking, least);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e[0], cudaEventDisableTiming);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e[1], cudaEventDisableTiming);
+    if (err != cudaSuccess) {
+        for (int i = 0; i < 2; ++i) {
+            if (s[i]) cudaStreamDestroy(s[i]);
+            if (e[i]) cudaEventDestroy(e[i]);
+        }
+        set_error("look-ahead streams: %s", cudaGetErrorString(err));
+        return NMX_ERR_CUDA;
+    }
+    for (int i = 0; i < 2; ++i) {
+        ctx->la_stream[i] = s[i];
+        ctx->la_event[i] = e[i];
+    }
     return 0;
 }
 

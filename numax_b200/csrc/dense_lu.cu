@@ -503,6 +503,7 @@ struct LuRun {
     int scope_lo = 0, scope_hi = 0;
     int *lists = nullptr;
     int nlists = 0;
+    bool keep_lists = false;  // the lists are applied later (look-ahead panel)
 };
 
 // Shared-memory bytes the cluster leaf needs for an m-row panel of width w.
@@ -536,11 +537,18 @@ static int calu_swap(cudaStream_t st, T *A, int64_t lda, const int *lists, int n
     return 0;
 }
 
-// The next slot for a leaf's row moves (unblocked, slots recycle: each list
-// is applied at once).
+// The next slot for a leaf's row moves.  Unblocked the slots recycle (each
+// list is applied at once); a look-ahead panel keeps all of its leaves'
+// lists, and the panel widths are chosen so they fit -- nullptr otherwise.
 template <typename T>
 static int *leaf_list(LuRun<T> &R) {
-    if (R.nlists >= kCaluMaxLists) R.nlists = 0;
+    if (R.nlists >= kCaluMaxLists) {
+        if (R.keep_lists) {
+            set_error("LU panel needs more than %d leaf move lists", kCaluMaxLists);
+            return nullptr;
+        }
+        R.nlists = 0;
+    }
     return R.lists + (size_t)R.nlists++ * kCaluListStride;
 }
 
@@ -551,6 +559,7 @@ template <typename T>
 static int leaf_swap(LuRun<T> &R, int c, int w) {
     if (w <= kCaluW) {
         int *ml = leaf_list(R);
+        if (!ml) return NMX_ERR_INTERNAL;
         ipiv_moves_kernel<<<1, 32, 0, R.st>>>(R.ipiv, c, w, ml);
         NMX_CUDA_TRY(cudaGetLastError());
         return calu_swap<T>(R.st, R.A, R.lda, ml, 1, R.scope_lo, c, c + w, R.scope_hi);
@@ -569,6 +578,7 @@ static int calu_leaf(LuRun<float> &R, int c, int w) {
     const int nctas = (int)ceil_div(m, kCaluRows);
     const bool vec = R.lda % 4 == 0 && reinterpret_cast<uintptr_t>(R.A) % 16 == 0;
     int *ml = leaf_list(R);
+    if (!ml) return NMX_ERR_INTERNAL;
     calu_pick_kernel<<<nctas, kCaluThreads, 0, R.st>>>(R.A, R.lda, R.n, c, w, nctas, vec, R.cs,
                                                     R.ipiv, R.info, ml);
     // The panel's rows and, in the same launch, the moves in the other
@@ -786,6 +796,7 @@ static int getrf_lookahead(LuRun<T> &R, int nb) {
     LuRun<T> RP = R;
     RP.st = P;
     RP.gs = gP;
+    RP.keep_lists = true;
     int *buf[2] = {R.cs.lists, R.cs.lists + (size_t)kCaluMaxLists * kCaluListStride};
     int cur = 0;
     auto panel = [&](int k, int kb) {
