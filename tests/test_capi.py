@@ -47,3 +47,15 @@ def test_argument_errors_need_no_device(lib):
     assert "out is NULL" in _lib.last_error()
     assert lib.nmx_version() >= 100
     assert lib.nmx_batched_plan_sizes(None, None, None) == -1
+
+
+def test_tuning_keys_documented(lib):
+    """Every key nmx_tune_set accepts is documented in the public header, and
+    only those; argument errors come back without a device."""
+    src = open(os.path.join(ROOT, "numax_b200", "csrc", "context.cu")).read()
+    accepted = set(re.findall(r'strcmp\(key, "([a-z_.]+)"\)', src))
+    hdr = open(os.path.join(ROOT, "include", "nmx_la.h")).read()
+    block = hdr[hdr.index("Per-context tuning knobs"):hdr.index("NMX_API int nmx_tune_set")]
+    documented = set(re.findall(r'"([a-z_]+\.[a-z_]+)"', block))
+    assert accepted and accepted == documented, (accepted, documented)
+    assert lib.nmx_tune_set(None, b"lu.lookahead", 256) == -1
