@@ -46,6 +46,24 @@ def draw_sizes(count, seed):
     return rng.integers(NMIN, NMAX + 1, size=count).astype(np.int32)
 
 
+def shard(rank, count):
+    """Rank `rank`'s own shard (weak scaling): its matrix sizes and the seed
+    of its data."""
+    return draw_sizes(count, SEED + rank), SEED + 1000 * rank
+
+
+def max_over_ranks(x, world, device):
+    """The largest x over the job's ranks (a step takes as long as its
+    slowest rank); x itself on one rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_batch_torch(ns, nrhs, dtype, device, seed):
     """Ragged A (G G^T/n + n I per matrix) and B, generated size group by
     size group with a seeded torch generator on `device`."""
@@ -479,8 +497,8 @@ def run_ours(args):
     dtype = torch.float64 if args.dtype == "f64" else torch.float32
     esize = 8 if args.dtype == "f64" else 4
 
-    ns = draw_sizes(args.count, SEED + rank)
-    A, B = make_batch_torch(ns, NRHS, dtype, dev, SEED + 1000 * rank)
+    ns, data_seed = shard(rank, args.count)
+    A, B = make_batch_torch(ns, NRHS, dtype, dev, data_seed)
     L = torch.empty_like(A)
     X = torch.empty_like(B)
     info = torch.empty(len(ns), dtype=torch.int32, device=dev)
@@ -503,13 +521,6 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---- device-timed: inputs resident in HBM (A, L ~ 4.7 GB each >> L2) ----
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
@@ -524,7 +535,7 @@ def run_ours(args):
             ev[s][1].record(stream)
         t_end.record(stream)
         barrier()
-    total_s = max_over_ranks(t_start.elapsed_time(t_end) / 1e3)
+    total_s = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, world, dev)
     launch_s = float(np.mean([a.elapsed_time(b) for a, b in ev])) / 1e3
     value = world * len(ns) * args.steps / total_s
 
@@ -547,7 +558,7 @@ def run_ours(args):
         plan_big.run(Ab, Bb, Xb, ib, Lb)
         evb[s][1].record(stream)
     barrier()
-    big_s = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in evb])) / 1e3)
+    big_s = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in evb])) / 1e3, world, dev)
     del Ab, Bb, Lb, Xb, ib, plan_big
 
     # ---- end to end through the public API: pinned host in, host out --------
@@ -576,7 +587,7 @@ def run_ours(args):
         e2e_step()
     e1.record(stream)
     barrier()
-    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
     e2e_value = world * len(ns) * e2e_steps / e2e_s
     h2d = (hA.numel() + hB.numel()) * esize
     d2h = hX.numel() * esize + hI.numel() * 4
