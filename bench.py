@@ -64,6 +64,12 @@ def max_over_ranks(x, world, device):
     return float(t.item())
 
 
+def job_value(world, per_rank, steps, seconds):
+    """Whole-job throughput: every rank's `per_rank` units per step, over
+    `steps` steps, in the slowest rank's `seconds`."""
+    return world * per_rank * steps / seconds
+
+
 def make_batch_torch(ns, nrhs, dtype, device, seed):
     """Ragged A (G G^T/n + n I per matrix) and B, generated size group by
     size group with a seeded torch generator on `device`."""
@@ -537,7 +543,7 @@ def run_ours(args):
         barrier()
     total_s = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, world, dev)
     launch_s = float(np.mean([a.elapsed_time(b) for a, b in ev])) / 1e3
-    value = world * len(ns) * args.steps / total_s
+    value = job_value(world, len(ns), args.steps, total_s)
 
     # ---- the dominant kernel alone: the n in (96, 128] bucket -------------
     # (potrf_potrs_batched_kernel<double, 192>, about half of the step), as a
@@ -588,7 +594,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
-    e2e_value = world * len(ns) * e2e_steps / e2e_s
+    e2e_value = job_value(world, len(ns), e2e_steps, e2e_s)
     h2d = (hA.numel() + hB.numel()) * esize
     d2h = hX.numel() * esize + hI.numel() * 4
     np.testing.assert_array_equal(hI.numpy(), 0)

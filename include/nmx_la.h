@@ -158,12 +158,17 @@ NMX_API int nmx_potrf_potrs_batched_graph_f32(nmx_ctx ctx, nmx_batched_plan plan
  * kept in a fixed device array built into the library instead of a plan's
  * cudaMalloc'd buffer.  The call itself allocates nothing on the device or
  * through any library.  Same layout and results as the plan path; n_host is
- * on the host and is copied into that array on `stream`.
+ * on the host, its sizes are checked there, and it is copied into that array
+ * on `stream`.  From pageable memory the copy is staged before the call
+ * returns, so n_host may be reused at once; from pinned memory the copy is
+ * asynchronous, so keep n_host unchanged until `stream` has passed the call.
  * Limit: count <= 65536 matrices (a larger count is rejected with -2).
  * The array (about 1.5 MB) stays resident on every GPU that loads the
  * library until exit.  The first call on a device performs that device's
  * set-up (resolving the array's address), so make it before any stream
- * capture.  All calls share the one array: calls that may overlap on the GPU
+ * capture.  A call whose `stream` is being captured is refused with
+ * NMX_ERR_UNSUPPORTED, because the size checks happen on the host at call
+ * time.  All calls share the one array: calls that may overlap on the GPU
  * (different streams, or several host threads) race and must be serialized
  * by the caller. */
 NMX_API int nmx_potrf_potrs_batched_noalloc_f64(nmx_ctx ctx, int64_t count, const int32_t *n_host,

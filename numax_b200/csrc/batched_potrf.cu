@@ -1118,8 +1118,8 @@ int nmx_potrf_potrs_batched_graph_f32(nmx_ctx ctx, nmx_batched_plan plan, const 
 // ---- allocation-free entry point --------------------------------------------
 //
 // For callers that cannot allocate device memory (a host runtime whose
-// allocator owns all of HBM, code running inside another framework's memory
-// pool or a CUDA-graph-only region): the same kernel as the plan path, with
+// allocator owns all of HBM, or code running inside another framework's
+// memory pool): the same kernel as the plan path, with
 // its schedule -- matrix sizes, size-sorted order, element offsets and the
 // work counter -- held in a fixed file-scope device array instead of a plan's
 // cudaMalloc'd buffer.  The array is sized for kNoAllocMaxCount matrices
@@ -1273,10 +1273,20 @@ static int run_noalloc(nmx_ctx ctx, int64_t count, const int32_t *n_host, int nr
     }
     if (count == 0) return 0;
     DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The sizes are checked on the host and the launch is sized for them at
+    // call time, so a captured call would replay with whatever n_host holds
+    // later, unchecked.  Refuse capture instead.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    NMX_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("the allocation-free entry point checks n_host on the host at each call and "
+                  "cannot run while its stream is being captured");
+        return NMX_ERR_UNSUPPORTED;
+    }
     NoAllocDevice *d = nullptr;
     int rc = noalloc_setup<T>(ctx, &d);
     if (rc) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     NoAllocViews v = noalloc_views(d->scratch);
     NMX_CUDA_TRY(cudaMemcpyAsync(v.n, n_host, sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
     noalloc_schedule_kernel<<<1, kSchedThreads, 0, st>>>(d->scratch, (int)count, nrhs);

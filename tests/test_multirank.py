@@ -57,8 +57,10 @@ def test_two_gloo_ranks_shard_and_take_the_slowest_time():
     assert m0 == m1 == 0.75            # both ranks see the slowest rank's time
     assert s0 != s1 and seed0 != seed1  # two different shards
     assert bench.NMIN <= min(lo0, lo1) and max(hi0, hi1) <= bench.NMAX
-    # One rank's view of the job: world x its shard x steps / slowest time.
-    assert 2 * 2000 * 3 / m0 == pytest.approx(16000.0)
+    # The whole-job value bench.py reports: both ranks' shards over the
+    # slowest rank's time.
+    assert bench.job_value(2, 2000, 3, m0) == pytest.approx(16000.0)
+    assert bench.job_value(1, 2000, 3, 0.25) == pytest.approx(24000.0)
 
 
 def test_single_rank_needs_no_process_group():

@@ -70,6 +70,86 @@ def test_noalloc_matches_plan_path_twice():
         assert (info.cpu().numpy() == refI.cpu().numpy()).all()
 
 
+def _noalloc_call(lib, ctx, ns, nrhs, dA, L, dB, X, info, stream):
+    return lib.nmx_potrf_potrs_batched_noalloc_f64(
+        ctx, len(ns), ns.ctypes.data, nrhs, C.c_void_p(dA.data_ptr()), C.c_void_p(L.data_ptr()),
+        C.c_void_p(dB.data_ptr()), C.c_void_p(X.data_ptr()), C.c_void_p(info.data_ptr()),
+        C.c_void_p(stream))
+
+
+def test_noalloc_matches_oracle_at_the_limit_with_a_failing_matrix(oracle):
+    """65,536 matrices (the limit), one of them not positive definite:
+    factors and solutions against the oracle (numax's Array-tier Cholesky and
+    cholesky_solve per matrix), `info` = 4 for the failing one (numax's
+    later-block failure fixture), NaN exactly where the oracle has NaN."""
+    from numax_b200 import _lib
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.Generator(np.random.PCG64(31))
+    count, nrhs, bad_at = 65536, 2, 40000
+    ns = np.ascontiguousarray(rng.integers(1, 25, size=count), dtype=np.int32)
+    ns[bad_at] = 4
+    A, B = _batch(ns, nrhs, 32)
+    ao = np.zeros(count, dtype=np.int64)
+    ao[1:] = np.cumsum(ns.astype(np.int64) ** 2)[:-1]
+    A[ao[bad_at]:ao[bad_at] + 16] = [4.0, 1.0, 0.0, 0.0, 1.0, 4.0, 0.0, 0.0,
+                                     0.0, 0.0, 1.0, 3.0, 0.0, 0.0, 3.0, 1.0]
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    L = torch.zeros_like(dA)
+    X = torch.full_like(dB, float("nan"))
+    info = torch.full((count,), -7, dtype=torch.int32, device=dA.device)
+    assert _noalloc_call(lib, ctx, ns, nrhs, dA, L, dB, X, info, stream) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    want_info = np.zeros(count, dtype=np.int32)
+    want_info[bad_at] = 4
+    np.testing.assert_array_equal(info.cpu().numpy(), want_info)
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, nrhs)
+    gotL, gotX = L.cpu().numpy(), X.cpu().numpy()
+    np.testing.assert_array_equal(np.isnan(gotX), np.isnan(wantX))
+    ok = ~np.isnan(wantX)
+    bo = np.zeros(count, dtype=np.int64)
+    bo[1:] = np.cumsum(ns.astype(np.int64) * nrhs)[:-1]
+    worst_l = worst_x = 0.0
+    for i in range(0, count, 7):  # every 7th matrix, plus the failing one
+        n = int(ns[i])
+        if i == bad_at:
+            continue
+        g = np.tril(gotL[ao[i]:ao[i] + n * n].reshape(n, n))
+        w = np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))
+        worst_l = max(worst_l, _rel(g, w))
+        worst_x = max(worst_x, _rel(gotX[bo[i]:bo[i] + n * nrhs], wantX[bo[i]:bo[i] + n * nrhs]))
+    assert worst_l <= 1e-12, worst_l
+    assert worst_x <= 1e-12, worst_x
+    assert _rel(gotX[ok], wantX[ok]) <= 1e-12
+    bad = np.tril(gotL[ao[bad_at]:ao[bad_at] + 16].reshape(4, 4))
+    np.testing.assert_allclose(bad[:2, :2], np.tril(wantL[ao[bad_at]:ao[bad_at] + 16]
+                                                     .reshape(4, 4))[:2, :2], rtol=1e-14)
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """The sizes are checked on the host at each call, so a call made while
+    its stream is being captured is refused rather than recorded."""
+    from numax_b200 import _lib
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    ns = np.array([3, 5], dtype=np.int32)
+    A, B = _batch(ns, 1, 3)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    L, X = torch.zeros_like(dA), torch.zeros_like(dB)
+    info = torch.zeros(2, dtype=torch.int32, device="cuda")
+    # Set-up on this device happens on a first, uncaptured call.
+    assert _noalloc_call(lib, ctx, ns, 1, dA, L, dB, X, info,
+                         torch.cuda.current_stream().cuda_stream) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(g, stream=side):
+        rc = _noalloc_call(lib, ctx, ns, 1, dA, L, dB, X, info, side.cuda_stream)
+    assert rc == -1002
+    assert "captured" in _lib.last_error()
+
+
 def test_noalloc_rejects_batches_over_the_limit():
     from numax_b200 import _lib
     lib = _lib.load()
