@@ -250,13 +250,26 @@ def haar_torch(n, gen, dev):
     return q
 
 
+# Refinement modes per conditioning: (label, mode flags).  Every mode may
+# escalate (BF16/FP16 -> BF16X3 -> BF16X6 -> FP64) so that each ends at FP64
+# backward error; the final precision is reported beside the time.
+IR_MODES = {
+    1e2: [("bf16x3", "BF16X3"), ("fp16", "FP16"), ("bf16", "BF16")],
+    1e5: [("bf16x6", "BF16X6"), ("bf16x3", "BF16X3"), ("fp16", "FP16")],
+    1e8: [("bf16x6", "BF16X6"), ("fp16", "FP16")],
+}
+
+
 def run_lu_ir(n, kappas, dev, seed=SEED):
-    """FP64 LU solve vs the BF16-factor IR solve at order n, A = U diag(s) V^T
-    (U, V Haar, s geometric 1..1/kappa), b = A x_true.  Both timed on the
-    device (CUDA events), inputs resident; returns a dict per kappa."""
+    """FP64 LU solve vs the low-precision-factor IR solve at order n,
+    A = U diag(s) V^T (U, V Haar, s geometric 1..1/kappa), b = A x_true.
+    Device time (CUDA events), inputs resident.  Workspaces are reserved
+    first (nmx_gesv_ir_reserve); each mode runs twice and both times are
+    reported: "cold" (first launch of its kernels) and "warm"."""
     import ctypes as C
     import torch
     from numax_b200 import _lib
+    lib = _lib.load()
     ctx = _lib.context(dev.index)
     stream = torch.cuda.current_stream(dev)
     gen = torch.Generator(device=dev)
@@ -264,8 +277,14 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
     u = haar_torch(n, gen, dev)
     v = haar_torch(n, gen, dev)
     xt = torch.randn(n, generator=gen, dtype=torch.float64, device=dev)
+    flag = lambda p: getattr(_lib, f"NMX_IR_{p}")
+    _lib.call("nmx_gesv_ir_reserve", ctx, n, _lib.NMX_IR_BF16 | _lib.NMX_IR_ESCALATE)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lu = torch.empty((n, n), dtype=torch.float64, device=dev)
+    piv = torch.empty(n, dtype=torch.int32, device=dev)
+    info = torch.empty(1, dtype=torch.int32, device=dev)
     out = {}
-    for kappa in kappas:
+    for ki, kappa in enumerate(kappas):
         s = torch.logspace(0.0, -np.log10(kappa), n, dtype=torch.float64, device=dev)
         a = (u * s[None, :]) @ v.T
         b = a @ xt
@@ -275,60 +294,58 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
             r = b - a @ x
             return float(r.abs().max() / (norm_a * x.abs().max() + b.abs().max()))
 
-        # FP64: nmx_getrf_f64 + nmx_getrs_f64 on a copy.
-        lu = torch.empty_like(a)
-        piv = torch.empty(n, dtype=torch.int32, device=dev)
-        info = torch.empty(1, dtype=torch.int32, device=dev)
+        # FP64: nmx_getrf_f64 + nmx_getrs_f64 on a copy (the first kappa also
+        # runs it once untimed, so the timed call allocates nothing).
         x64 = torch.empty_like(b)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        lu.copy_(a)
-        x64.copy_(b)
-        torch.cuda.synchronize(dev)
-        e0.record(stream)
-        _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(),
-                  stream.cuda_stream)
-        _lib.call("nmx_getrs_f64", ctx, n, 1, lu.data_ptr(), n, piv.data_ptr(), x64.data_ptr(), 1,
-                  stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        t64 = e0.elapsed_time(e1)
-        be64 = berr(x64)
-        del lu
-        # BF16 factors + FP64 refinement (GMRES-IR when plain IR stalls).
-        res = {"fp64_lu_solve_ms": t64, "fp64_backward_error": be64}
-        # bf16: one BF16 rounding per update operand (8 significant bits);
-        # bf16x3: BF16 tensor cores on hi/lo operand splits (~16 bits);
-        # fp16: FP16 operands after power-of-two equilibration (11 bits).
-        # Plain bf16 gets fewer refinement steps: its factors are too coarse
-        # for this order, and the leg only records how far it gets.
-        for prec, mode, iters in (("bf16", _lib.NMX_IR_BF16 | _lib.NMX_IR_AUTO, 4),
-                                  ("bf16x3", _lib.NMX_IR_BF16X3 | _lib.NMX_IR_AUTO, 30),
-                                  ("fp16", _lib.NMX_IR_FP16 | _lib.NMX_IR_AUTO, 30)):
-            x = torch.empty_like(b)
-            st = _lib.IrStats()
+
+        def fp64_solve():
+            lu.copy_(a)
+            x64.copy_(b)
+            torch.cuda.synchronize(dev)
             e0.record(stream)
-            rc = _lib.load().nmx_gesv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
-                                             C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
-                                             mode, 1e-14, iters, C.byref(st),
-                                             C.c_void_p(stream.cuda_stream))
+            _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(),
+                      stream.cuda_stream)
+            _lib.call("nmx_getrs_f64", ctx, n, 1, lu.data_ptr(), n, piv.data_ptr(),
+                      x64.data_ptr(), 1, stream.cuda_stream)
             e1.record(stream)
             torch.cuda.synchronize(dev)
-            if rc != 0:
-                res[f"{prec}_ir_error"] = _lib.last_error()
+            return e0.elapsed_time(e1)
+        if ki == 0:
+            fp64_solve()
+        t64 = fp64_solve()
+        res = {"fp64_lu_solve_ms": t64, "fp64_backward_error": berr(x64)}
+        for label, prec in IR_MODES.get(kappa, IR_MODES[1e8]):
+            mode = flag(prec) | _lib.NMX_IR_AUTO | _lib.NMX_IR_ESCALATE
+            times = []
+            for rep in range(2):
+                x = torch.empty_like(b)
+                st = _lib.IrStats()
+                torch.cuda.synchronize(dev)
+                e0.record(stream)
+                rc = lib.nmx_gesv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
+                                         C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), mode,
+                                         1e-14, 60, C.byref(st), C.c_void_p(stream.cuda_stream))
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                if rc != 0:
+                    res[f"{label}_ir_error"] = _lib.last_error()
+                    break
+                times.append(e0.elapsed_time(e1))
+            if len(times) < 2:
                 continue
-            tir = e0.elapsed_time(e1)
             fe = float((x - x64).abs().max() / x64.abs().max())
-            res.update({f"{prec}_ir_solve_ms": tir, f"{prec}_ir_backward_error": berr(x),
-                        f"{prec}_ir_iterations": st.iterations,
-                        f"{prec}_gmres_iterations": st.gmres_iterations,
-                        f"{prec}_used_gmres": bool(st.used_gmres),
-                        f"{prec}_factor_ms": st.factor_ms, f"{prec}_refine_ms": st.refine_ms,
-                        f"{prec}_forward_diff_vs_fp64": fe,
-                        f"{prec}_converged": bool(st.converged),
-                        f"speedup_fp64_over_{prec}_ir": t64 / tir})
+            res[label] = {
+                "solve_ms_warm": times[1], "solve_ms_cold": times[0],
+                "backward_error": berr(x), "converged": bool(st.converged),
+                "final_precision": _lib.IR_PRECISION_NAMES.get(st.final_precision, "?"),
+                "iterations": st.iterations, "gmres_iterations": st.gmres_iterations,
+                "used_gmres": bool(st.used_gmres), "factor_ms": st.factor_ms,
+                "refine_ms": st.refine_ms, "forward_diff_vs_fp64": fe,
+                "speedup_fp64_over_ir": t64 / times[1]}
         out[f"{kappa:.0e}"] = res
         del a, b, s
         torch.cuda.empty_cache()
+    del lu
     return out
 
 
@@ -487,6 +504,20 @@ def run_eigh(count, dev, steps=3, tol=1e-7, max_sweeps=20):
             "hbm_gbs": bytes_ / (ms / 1e3) / 1e9}
 
 
+def run_lu_ir_legs(args, dev):
+    """The LU/IR comparison at every requested order; errors are reported in
+    place so that the batched line still prints."""
+    kappas = [float(k) for k in args.lu_kappas.split(",") if k]
+    legs = {"timing": "device events, inputs resident; workspaces reserved; cold = first call, "
+                      "warm = second call of each mode", "orders": {}}
+    for n in [int(v) for v in str(args.lu_n).split(",") if v and int(v) > 0]:
+        try:
+            legs["orders"][str(n)] = run_lu_ir(n, kappas, dev)
+        except Exception as exc:
+            legs["orders"][str(n)] = {"error": f"{type(exc).__name__}: {exc}"}
+    return legs
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -634,13 +665,8 @@ def run_ours(args):
             dense = {"error": f"{type(exc).__name__}: {exc}"}
 
     lu_ir = None
-    if world == 1 and args.lu_n > 0:
-        try:
-            kappas = [float(k) for k in args.lu_kappas.split(",") if k]
-            lu_ir = {"n": args.lu_n, "timing": "device events, inputs resident, one solve each",
-                     "results": run_lu_ir(args.lu_n, kappas, dev)}
-        except Exception as exc:  # report, keep the batched line
-            lu_ir = {"n": args.lu_n, "error": f"{type(exc).__name__}: {exc}"}
+    if world == 1 and args.lu_n:
+        lu_ir = run_lu_ir_legs(args, dev)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -690,11 +716,14 @@ def main():
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--lu-n", type=int, default=32768,
-                    help="order of the FP64-LU vs BF16-IR comparison (0 skips it)")
-    ap.add_argument("--lu-kappas", default="1e2",
+    ap.add_argument("--lu-n", default="16384,32768",
+                    help="comma-separated orders of the FP64-LU vs low-precision IR comparison "
+                         "(0 skips it)")
+    ap.add_argument("--lu-kappas", default="1e2,1e5,1e8",
                     help="comma-separated condition numbers for the comparison")
     ap.add_argument("--only-lu", action="store_true", help="run only the LU/IR comparison")
+    ap.add_argument("--only-dense", action="store_true",
+                    help="run only the dense LU/Cholesky/QR leg")
     ap.add_argument("--no-dense", dest="dense", action="store_false",
                     help="skip the dense LU/Cholesky/QR leg")
     ap.add_argument("--eigh-count", type=int, default=65536,
@@ -702,13 +731,17 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_dense:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        print(json.dumps({"dense": run_dense(dev)}), flush=True)
+        return 0
     if args.only_lu:
         import torch
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
         torch.cuda.set_device(dev)
-        kappas = [float(k) for k in args.lu_kappas.split(",") if k]
-        print(json.dumps({"lu_ir": {"n": args.lu_n, "results": run_lu_ir(args.lu_n, kappas, dev)}}),
-              flush=True)
+        print(json.dumps({"lu_ir": run_lu_ir_legs(args, dev)}), flush=True)
         return 0
     return run_ours(args)
 

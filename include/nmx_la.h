@@ -279,6 +279,26 @@ NMX_API int nmx_orgqr_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int
 NMX_API int nmx_orgqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
                           const double *tau, double *Q, int64_t ldq, void *stream);
 
+/* ---- the dense factorizations' GEMM ---------------------------------------
+ *
+ * C = alpha op(A) op(B) + beta C, row-major with leading dimensions, op(X) =
+ * X or X^T (trans_a / trans_b nonzero); `lower` nonzero writes only C's lower
+ * triangle (column <= row) and skips the tiles above it (the SYRK-shaped
+ * update).  beta == 0 never reads C.  FP64 runs on the DMMA pipe, FP32 on the
+ * CUDA cores, both hand-written.  The updates numax runs through MAX's
+ * linalg.matmul: numax/linalg/lu.mojo:646-673 (A22 -= L21 U12),
+ * numax/linalg/cholesky.mojo:190-225 (A22 -= L21 L21^T), the triangular
+ * solves' block products (numax/linalg/triangular.mojo:193-218) and the
+ * block-reflector products (numax/linalg/qr.mojo:262-308).  Asynchronous on
+ * `stream`.
+ */
+NMX_API int nmx_gemm_f64(nmx_ctx ctx, int trans_a, int trans_b, int64_t m, int64_t n, int64_t k,
+                         double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+                         double beta, double *C, int64_t ldc, int lower, void *stream);
+NMX_API int nmx_gemm_f32(nmx_ctx ctx, int trans_a, int trans_b, int64_t m, int64_t n, int64_t k,
+                         float alpha, const float *A, int64_t lda, const float *B, int64_t ldb,
+                         float beta, float *C, int64_t ldc, int lower, void *stream);
+
 /* ---- mixed-precision LU solve with iterative refinement -------------------
  *
  * No numax counterpart (numax's GPU path is FP32-only, without refinement);
@@ -288,23 +308,31 @@ NMX_API int nmx_orgqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, in
  *     factors are FP16, rounded to FP32 and factored by the recursive LU of
  *     nmx_getrf_f32 with its trailing updates in BF16/FP16 on the tcgen05
  *     tensor cores (FP32 accumulate), or FP32 CUDA cores (NMX_IR_FP32);
+ *     NMX_IR_FP64 factors A in FP64 (nmx_getrf_f64) and only polishes;
  *   - refinement in FP64: r = b - A x over the original A, correction from
  *     the low-precision factors; with NMX_IR_GMRES the correction is solved by
- *     restarted GMRES preconditioned by those factors (GMRES-IR); with
+ *     GMRES preconditioned by those factors (GMRES-IR, on the device); with
  *     NMX_IR_AUTO plain refinement hands over to GMRES-IR when it stops
- *     contracting.
- * Stops when ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol or
- * after max_iter refinement steps.  Synchronizes `stream` (the refinement
- * loop decides on the host).  stats (host pointer, may be NULL) receives the
- * iteration counts, the final normwise backward error and the device time of
- * the factorization and of the refinement.
+ *     contracting; with NMX_IR_ESCALATE a precision whose refinement cannot
+ *     converge is replaced by the next, more accurate one (BF16 or FP16 ->
+ *     BF16X3 -> BF16X6 -> FP64), refining on from the best iterate.
+ * x receives the iterate with the smallest backward error.  Stops when
+ * ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol or after max_iter
+ * refinement steps.  Synchronizes `stream` (the refinement loop decides on the
+ * host).  stats (host pointer, may be NULL) receives the iteration counts,
+ * the final normwise backward error, the device time of the factorizations
+ * and of the refinement, and the precision the last factorization used.
+ * Workspace is grown on first use; nmx_gesv_ir_reserve grows it ahead.
  */
 #define NMX_IR_BF16 1
 #define NMX_IR_FP16 2
 #define NMX_IR_FP32 3
 #define NMX_IR_BF16X3 4 /* BF16 tensor cores on hi/lo splits (see NMX_PREC_BF16X3) */
+#define NMX_IR_BF16X6 5 /* BF16 tensor cores on hi/mid/lo splits (see NMX_PREC_BF16X6) */
+#define NMX_IR_FP64 6   /* FP64 factors: the last escalation level */
 #define NMX_IR_GMRES 0x10
 #define NMX_IR_AUTO 0x20
+#define NMX_IR_ESCALATE 0x40
 
 typedef struct {
     int32_t iterations;       /* refinement steps taken */
@@ -312,7 +340,7 @@ typedef struct {
     int32_t converged;        /* 1 if the backward error reached tol */
     int32_t info;             /* info of the low-precision LU (first zero pivot) */
     int32_t used_gmres;       /* 1 if GMRES-IR ran */
-    int32_t reserved;
+    int32_t final_precision;  /* NMX_IR_* precision of the last factorization */
     double backward_error;    /* final normwise backward error */
     double factor_ms;         /* device time: scaling + low-precision LU */
     double refine_ms;         /* device time: the refinement loop */
@@ -324,7 +352,9 @@ typedef struct {
  * the products accumulated in FP32 on the tcgen05 tensor cores.  Precision 3
  * (BF16X3) splits each operand into BF16 hi + lo (lo = the rounding
  * residual) and forms hi*hi + hi*lo + lo*hi as one BF16 GEMM over 3K: about
- * 16 significant bits per operand instead of 8.  C must be
+ * 16 significant bits per operand instead of 8; precision 4 (BF16X6) splits
+ * into hi + mid + lo and forms the six products hi*hi, hi*mid, mid*hi,
+ * hi*lo, mid*mid, lo*hi over 6K: FP32's 24 bits.  C must be
  * 16-byte aligned with ldc a multiple of 4 and ldc >= N rounded up to 8: the
  * update runs on N (and K) rounded up to 8 with zero padding, so C's columns
  * N .. round8(N)-1 are read and written back unchanged.  No numax
@@ -332,6 +362,7 @@ typedef struct {
 #define NMX_PREC_BF16 1
 #define NMX_PREC_FP16 2
 #define NMX_PREC_BF16X3 3
+#define NMX_PREC_BF16X6 4
 NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64_t K, const float *A,
                              int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc,
                              int precision, void *stream);
@@ -339,6 +370,10 @@ NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64_t K, const
 NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, const double *b,
                             double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
                             void *stream);
+/* Grow the context's workspace for nmx_gesv_ir_f64 at order n and `mode`
+ * (with NMX_IR_ESCALATE, for every level it may reach) so that the solve
+ * itself allocates nothing.  No numax counterpart. */
+NMX_API int nmx_gesv_ir_reserve(nmx_ctx ctx, int64_t n, int mode);
 
 #ifdef __cplusplus
 }

@@ -64,21 +64,31 @@ SIGNATURES = {
     "nmx_orgqr_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
     "nmx_gesv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
     "nmx_gemm_sub_f32": (ci, [vp, i64, i64, i64, vp, i64, vp, i64, vp, i64, ci, vp]),
+    "nmx_gesv_ir_reserve": (ci, [vp, i64, ci]),
+    "nmx_gemm_f64": (ci, [vp, ci, ci, i64, i64, i64, C.c_double, vp, i64, vp, i64, C.c_double,
+                          vp, i64, ci, vp]),
+    "nmx_gemm_f32": (ci, [vp, ci, ci, i64, i64, i64, C.c_float, vp, i64, vp, i64, C.c_float,
+                          vp, i64, ci, vp]),
 }
 
 NMX_IR_BF16 = 1
 NMX_IR_FP16 = 2
 NMX_IR_FP32 = 3
 NMX_IR_BF16X3 = 4
+NMX_IR_BF16X6 = 5
+NMX_IR_FP64 = 6
 NMX_IR_GMRES = 0x10
 NMX_IR_AUTO = 0x20
+NMX_IR_ESCALATE = 0x40
+IR_PRECISION_NAMES = {NMX_IR_BF16: "bf16", NMX_IR_FP16: "fp16", NMX_IR_FP32: "fp32",
+                      NMX_IR_BF16X3: "bf16x3", NMX_IR_BF16X6: "bf16x6", NMX_IR_FP64: "fp64"}
 
 
 class IrStats(C.Structure):
     """nmx_ir_stats (include/nmx_la.h)."""
     _fields_ = [("iterations", C.c_int32), ("gmres_iterations", C.c_int32),
                 ("converged", C.c_int32), ("info", C.c_int32), ("used_gmres", C.c_int32),
-                ("reserved", C.c_int32), ("backward_error", C.c_double),
+                ("final_precision", C.c_int32), ("backward_error", C.c_double),
                 ("factor_ms", C.c_double), ("refine_ms", C.c_double)]
 
 

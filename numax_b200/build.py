@@ -79,7 +79,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lcublas"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -1,6 +1,4 @@
 // Context lifecycle and error reporting for libnmxla.so.
-#include <cublas_v2.h>
-
 #include <cstring>
 
 #include "nmx_common.cuh"
@@ -17,28 +15,6 @@ void set_error(const char *fmt, ...) {
 }
 
 void clear_error() { g_last_error[0] = 0; }
-
-// The second handle (same settings) for work that runs concurrently with the
-// first handle's.
-int ctx_cublas_aux(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out) {
-    if (!ctx->cublas_aux) {
-        cublasHandle_t h;
-        cublasStatus_t s = cublasCreate(&h);
-        if (s != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasCreate failed (%d)", (int)s);
-            return NMX_ERR_CUDA;
-        }
-        cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
-        ctx->cublas_aux = h;
-    }
-    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas_aux);
-    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) {
-        set_error("cublasSetStream failed");
-        return NMX_ERR_CUDA;
-    }
-    *out = h;
-    return 0;
-}
 
 int ctx_lookahead_streams(nmx_ctx ctx) {
     if (ctx->la_stream[0]) return 0;
@@ -64,28 +40,6 @@ int ctx_lookahead_streams(nmx_ctx ctx) {
         ctx->la_stream[i] = s[i];
         ctx->la_event[i] = e[i];
     }
-    return 0;
-}
-
-int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out) {
-    if (!ctx->cublas) {
-        cublasHandle_t h;
-        cublasStatus_t s = cublasCreate(&h);
-        if (s != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasCreate failed (%d)", (int)s);
-            return NMX_ERR_CUDA;
-        }
-        // Default math: FP64/FP32 products stay in their own precision (no
-        // TF32 tensor-op substitution, which needs CUBLAS_TF32_TENSOR_OP_MATH).
-        cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
-        ctx->cublas = h;
-    }
-    cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
-    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) {
-        set_error("cublasSetStream failed");
-        return NMX_ERR_CUDA;
-    }
-    *out = h;
     return 0;
 }
 
@@ -199,8 +153,6 @@ int nmx_destroy(nmx_ctx ctx) {
         if (ctx->workspace) cudaFree(ctx->workspace);
         for (int i = 0; i < nmx_context::kSlots; ++i)
             if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
-        if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
-        if (ctx->cublas_aux) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas_aux));
         for (int i = 0; i < 2; ++i) {
             if (ctx->la_stream[i]) cudaStreamDestroy(ctx->la_stream[i]);
             if (ctx->la_event[i]) cudaEventDestroy(ctx->la_event[i]);

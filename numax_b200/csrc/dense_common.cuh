@@ -4,8 +4,7 @@
 // with a leading dimension throughout, as numax's Tensor tiles are.
 #pragma once
 
-#include <cublas_v2.h>
-
+#include "gemm_cc.cuh"
 #include "gemm_tc.cuh"
 #include "nmx_common.cuh"
 
@@ -49,82 +48,40 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned gen, unsign
     return *s_flag != 0;
 }
 
-// C[m x n] -= A[m x k] * B[k x n], all row-major with leading dimensions.
-// Plain FP64/FP32 products go to cuBLAS (column-major: C^T -= B^T A^T).
-inline cublasStatus_t gemm_sub(cublasHandle_t h, int64_t m, int64_t n, int64_t k, const double *A,
-                               int64_t lda, const double *B, int64_t ldb, double *C, int64_t ldc) {
-    if (m <= 0 || n <= 0 || k <= 0) return CUBLAS_STATUS_SUCCESS;
-    const double minus = -1.0, one = 1.0;
-    return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)m, (int)k, &minus, B, (int)ldb, A,
-                       (int)lda, &one, C, (int)ldc);
-}
-inline cublasStatus_t gemm_sub(cublasHandle_t h, int64_t m, int64_t n, int64_t k, const float *A,
-                               int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc) {
-    if (m <= 0 || n <= 0 || k <= 0) return CUBLAS_STATUS_SUCCESS;
-    const float minus = -1.0f, one = 1.0f;
-    return cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)m, (int)k, &minus, B, (int)ldb, A,
-                       (int)lda, &one, C, (int)ldc);
+// C[m x n] -= A[m x k] * B[k x n], all row-major with leading dimensions,
+// on the library's own FP64 (DMMA) / FP32 (FFMA) GEMM.
+template <typename T>
+inline int gemm_sub(cudaStream_t st, int64_t m, int64_t n, int64_t k, const T *A, int64_t lda,
+                    const T *B, int64_t ldb, T *C, int64_t ldc) {
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    return gemm_cc<T>(st, false, false, m, n, k, T(-1), A, lda, B, ldb, T(1), C, ldc);
 }
 
-// C[m x n] -= A[m x k] * B[n x k]^T (row-major), the SYRK-shaped update.
-inline cublasStatus_t gemm_sub_bt(cublasHandle_t h, int64_t m, int64_t n, int64_t k,
-                                  const double *A, int64_t lda, const double *B, int64_t ldb,
-                                  double *C, int64_t ldc) {
-    if (m <= 0 || n <= 0 || k <= 0) return CUBLAS_STATUS_SUCCESS;
-    const double minus = -1.0, one = 1.0;
-    return cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)n, (int)m, (int)k, &minus, B, (int)ldb, A,
-                       (int)lda, &one, C, (int)ldc);
-}
-inline cublasStatus_t gemm_sub_bt(cublasHandle_t h, int64_t m, int64_t n, int64_t k,
-                                  const float *A, int64_t lda, const float *B, int64_t ldb,
-                                  float *C, int64_t ldc) {
-    if (m <= 0 || n <= 0 || k <= 0) return CUBLAS_STATUS_SUCCESS;
-    const float minus = -1.0f, one = 1.0f;
-    return cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)n, (int)m, (int)k, &minus, B, (int)ldb, A,
-                       (int)lda, &one, C, (int)ldc);
+// C[m x n] -= A[m x k] * B[n x k]^T (row-major).  `lower`: only C's lower
+// triangle (the SYRK-shaped update with B = A).
+template <typename T>
+inline int gemm_sub_bt(cudaStream_t st, int64_t m, int64_t n, int64_t k, const T *A, int64_t lda,
+                       const T *B, int64_t ldb, T *C, int64_t ldc, bool lower = false) {
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    return gemm_cc<T>(st, false, true, m, n, k, T(-1), A, lda, B, ldb, T(1), C, ldc, lower);
 }
 
-// General row-major GEMM: C[m x n] = alpha op(A)[m x k] op(B)[k x n] + beta C,
-// op(X) = X or X^T (X stored row-major with its leading dimension).
-inline cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
-                              double alpha, const double *A, int64_t lda, const double *B,
-                              int64_t ldb, double beta, double *C, int64_t ldc) {
-    if (m <= 0 || n <= 0) return CUBLAS_STATUS_SUCCESS;
-    return cublasDgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n,
-                       (int)m, (int)k, &alpha, B, (int)ldb, A, (int)lda, &beta, C, (int)ldc);
-}
-inline cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
-                              float alpha, const float *A, int64_t lda, const float *B, int64_t ldb,
-                              float beta, float *C, int64_t ldc) {
-    if (m <= 0 || n <= 0) return CUBLAS_STATUS_SUCCESS;
-    return cublasSgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n,
-                       (int)m, (int)k, &alpha, B, (int)ldb, A, (int)lda, &beta, C, (int)ldc);
-}
-
-#define NMX_CUBLAS_TRY(expr)                                                                 \
-    do {                                                                                     \
-        cublasStatus_t _s = (expr);                                                          \
-        if (_s != CUBLAS_STATUS_SUCCESS) {                                                   \
-            ::nmx::set_error("%s:%d: %s -> cublas status %d", __FILE__, __LINE__, #expr,     \
-                             (int)_s);                                                       \
-            return NMX_ERR_CUDA;                                                             \
-        }                                                                                    \
+#define NMX_TRY(expr)           \
+    do {                        \
+        const int _rc = (expr); \
+        if (_rc) return _rc;    \
     } while (0)
 
-// The context's cuBLAS handle bound to `st` (created on first use).
-int ctx_cublas(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
-// A second cuBLAS handle bound to `st`, for work concurrent with the first's.
-int ctx_cublas_aux(nmx_ctx ctx, cudaStream_t st, cublasHandle_t *out);
 // Creates the context's look-ahead streams and events on first use.
 int ctx_lookahead_streams(nmx_ctx ctx);
 
 
 // The trailing-update product of the recursive factorizations and solves:
 // C[m x n] -= A[m x k] B[k x n], row-major.  precision 0 keeps the operands'
-// own precision (cuBLAS FP64/FP32 GEMM); NMX_PREC_BF16 / NMX_PREC_FP16 (fp32
-// data only) round the operands to 16 bits and run the tcgen05 kernel.
+// own precision (the DMMA / FFMA GEMM of gemm_cc.cu); NMX_PREC_BF16 /
+// NMX_PREC_FP16 / NMX_PREC_BF16X3 (fp32 data only) round or split the
+// operands to 16 bits and run the tcgen05 kernel.
 struct GemmSub {
-    cublasHandle_t h = nullptr;
     cudaStream_t st = nullptr;
     int precision = 0;
     int64_t tc_min = 256;
@@ -133,12 +90,7 @@ struct GemmSub {
     int sm_limit = 0;  // > 0: tensor-core updates on at most this many SMs
     int operator()(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
                    int64_t ldb, double *C, int64_t ldc) const {
-        cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
-        if (s != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasDgemm failed (%d)", (int)s);
-            return NMX_ERR_CUDA;
-        }
-        return 0;
+        return gemm_sub<double>(st, m, n, k, A, lda, B, ldb, C, ldc);
     }
     int operator()(int64_t m, int64_t n, int64_t k, const float *A, int64_t lda, const float *B,
                    int64_t ldb, float *C, int64_t ldc) const {
@@ -148,12 +100,7 @@ struct GemmSub {
         if (precision && n >= tc_min && k >= tc_min)
             return tc_gemm_sub_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes,
                                    sm_limit);
-        cublasStatus_t s = gemm_sub(h, m, n, k, A, lda, B, ldb, C, ldc);
-        if (s != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasSgemm failed (%d)", (int)s);
-            return NMX_ERR_CUDA;
-        }
-        return 0;
+        return gemm_sub<float>(st, m, n, k, A, lda, B, ldb, C, ldc);
     }
 };
 
@@ -177,5 +124,8 @@ int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
 template <typename T>
 int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
               int32_t *info, bool tournament = false);
+
+// The tallest panel the tournament-pivoting leaf takes (dense_lu.cu).
+int64_t tournament_max_rows();
 
 }  // namespace nmx

@@ -658,7 +658,6 @@ template <typename T, bool TRANS>
 int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
                int c1) {
     cudaStream_t st = gs.st;
-    cublasHandle_t h = gs.h;
     if (w <= 0 || c1 <= c0) return 0;
     if (w <= kTrsmLeaf) {
         int threads = 128;
@@ -670,22 +669,13 @@ int trsm_upper(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
     int hw = (w / 2 + kTrsmLeaf - 1) / kTrsmLeaf * kTrsmLeaf;
     int rc = trsm_upper<T, TRANS>(gs, A, lda, r + hw, w - hw, B, ldb, c0, c1);
     if (rc) return rc;
-    // B_top -= U_top,bot X_bot   (TRANS: U_top,bot = (L_bot,top)^T)
+    // B_top -= U_top,bot X_bot   (TRANS: U_top,bot = (L_bot,top)^T, the
+    // (w - hw) x hw block below the diagonal read transposed).
     if (TRANS) {
-        const T minus = T(-1), one = T(1);
-        // row-major C[hw x nc] -= (L[bot x top])^T X[bot x nc]; column-major: C^T -= X^T L
-        cublasStatus_t s;
-        if (sizeof(T) == 8)
-            s = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, c1 - c0, hw, w - hw, (const double *)&minus,
-                            (const double *)(B + (int64_t)(r + hw) * ldb + c0), (int)ldb,
-                            (const double *)(A + (int64_t)(r + hw) * lda + r), (int)lda,
-                            (const double *)&one, (double *)(B + (int64_t)r * ldb + c0), (int)ldb);
-        else
-            s = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, c1 - c0, hw, w - hw, (const float *)&minus,
-                            (const float *)(B + (int64_t)(r + hw) * ldb + c0), (int)ldb,
-                            (const float *)(A + (int64_t)(r + hw) * lda + r), (int)lda,
-                            (const float *)&one, (float *)(B + (int64_t)r * ldb + c0), (int)ldb);
-        NMX_CUBLAS_TRY(s);
+        rc = gemm_cc<T>(st, true, false, hw, c1 - c0, w - hw, T(-1),
+                        A + (int64_t)(r + hw) * lda + r, lda, B + (int64_t)(r + hw) * ldb + c0, ldb,
+                        T(1), B + (int64_t)r * ldb + c0, ldb);
+        if (rc) return rc;
     } else {
         rc = gs(hw, c1 - c0, w - hw, A + (int64_t)r * lda + r + hw, lda,
                 B + (int64_t)(r + hw) * ldb + c0, ldb, B + (int64_t)r * ldb + c0, ldb);
@@ -784,10 +774,6 @@ static int getrf_lookahead(LuRun<T> &R, int nb) {
     // hardware-scheduled GEMM already interleaves the panel's kernels.
     const int64_t keep = ctx->tune_lu_panel_sms < 0 ? 0 : ctx->tune_lu_panel_sms;
     gU.sm_limit = keep > 0 ? (int)std::max<int64_t>(16, ctx->sm_count - keep) : 0;
-    rc = ctx_cublas_aux(ctx, P, &gP.h);
-    if (rc) return rc;
-    rc = ctx_cublas(ctx, U, &gU.h);
-    if (rc) return rc;
     if (gP.precision) {
         gP.ws_bytes = tc_gemm_workspace_bytes(n, nb, nb, gP.precision) + 4096;
         rc = ctx->ensure_slot(kWsGemm16Panel, gP.ws_bytes, &gP.ws);
@@ -866,11 +852,10 @@ static int getrf_lookahead(LuRun<T> &R, int nb) {
         cudaEventRecord(eU, U);
         cudaStreamWaitEvent(R.st, eU, 0);
     }
-    // The main handle goes back to the caller's stream whatever happened.
-    cublasHandle_t h;
-    const int rc2 = ctx_cublas(ctx, R.st, &h);
-    return rc ? rc : rc2;
+    return rc;
 }
+
+int64_t tournament_max_rows() { return (int64_t)kCaluMaxCtas * kCaluRows; }
 
 template <typename T>
 int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
@@ -1018,8 +1003,6 @@ static int getrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *ipiv, int32
     DeviceGuard g(ctx->device);
     GemmSub gs;
     gs.st = static_cast<cudaStream_t>(stream);
-    int rc = ctx_cublas(ctx, gs.st, &gs.h);
-    if (rc) return rc;
     return getrf_run<T>(ctx, gs, n, A, lda, ipiv, info, ctx->tune_lu_tournament == 1);
 }
 
@@ -1039,8 +1022,7 @@ static int getrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *LU, int64_t lda,
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     GemmSub gs;
     gs.st = st;
-    int rc = ctx_cublas(ctx, st, &gs.h);
-    if (rc) return rc;
+    int rc = 0;
     int threads = 128;
     laswp_kernel<T><<<(unsigned)ceil_div(nrhs, threads), threads, 0, st>>>(B, ldb, (int)nrhs, 0,
                                                                            (int)n, ipiv, 0, 0);

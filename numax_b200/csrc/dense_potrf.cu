@@ -190,22 +190,9 @@ __global__ void zero_upper_kernel(T *A, int64_t lda, int n) {
     if (j > i) A[(int64_t)i * lda + j] = T(0);
 }
 
-inline cublasStatus_t syrk_sub(cublasHandle_t h, int64_t n, int64_t k, const double *A, int64_t lda,
-                               double *C, int64_t ldc) {
-    const double minus = -1.0, one = 1.0;
-    return cublasDsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)n, (int)k, &minus, A, (int)lda,
-                       &one, C, (int)ldc);
-}
-inline cublasStatus_t syrk_sub(cublasHandle_t h, int64_t n, int64_t k, const float *A, int64_t lda,
-                               float *C, int64_t ldc) {
-    const float minus = -1.0f, one = 1.0f;
-    return cublasSsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)n, (int)k, &minus, A, (int)lda,
-                       &one, C, (int)ldc);
-}
-
 // X := X L^-T, X = rows [r0, r1) x cols [c, c+w), L the lower block at (c, c).
 template <typename T>
-static int trsm_right_lt(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c, int w, int r0,
+static int trsm_right_lt(cudaStream_t st, T *A, int64_t lda, int c, int w, int r0,
                          int r1) {
     if (w <= 0 || r1 <= r0) return 0;
     if (w > kCholLeaf && w <= kCholTrsmMaxW && w % 32 == 0) {
@@ -231,17 +218,17 @@ static int trsm_right_lt(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, i
         return 0;
     }
     const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
-    int rc = trsm_right_lt<T>(h, st, A, lda, c, hw, r0, r1);
+    int rc = trsm_right_lt<T>(st, A, lda, c, hw, r0, r1);
     if (rc) return rc;
     // X_b -= X_a L_ba^T, L_ba = rows [c+hw, c+w) x cols [c, c+hw).
-    NMX_CUBLAS_TRY(gemm_sub_bt(h, r1 - r0, w - hw, hw, A + (int64_t)r0 * lda + c, lda,
-                               A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)r0 * lda + c + hw,
-                               lda));
-    return trsm_right_lt<T>(h, st, A, lda, c + hw, w - hw, r0, r1);
+    NMX_TRY(gemm_sub_bt<T>(st, r1 - r0, w - hw, hw, A + (int64_t)r0 * lda + c, lda,
+                           A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)r0 * lda + c + hw,
+                           lda));
+    return trsm_right_lt<T>(st, A, lda, c + hw, w - hw, r0, r1);
 }
 
 template <typename T>
-static int potrf_rec(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c, int w,
+static int potrf_rec(cudaStream_t st, T *A, int64_t lda, int c, int w,
                      int32_t *info) {
     if (w <= kCholLeaf) {
         potrf_leaf_kernel<T><<<1, 32, 0, st>>>(A, lda, c, w, info);
@@ -249,14 +236,15 @@ static int potrf_rec(cublasHandle_t h, cudaStream_t st, T *A, int64_t lda, int c
         return 0;
     }
     const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
-    int rc = potrf_rec<T>(h, st, A, lda, c, hw, info);
+    int rc = potrf_rec<T>(st, A, lda, c, hw, info);
     if (rc) return rc;
-    rc = trsm_right_lt<T>(h, st, A, lda, c, hw, c + hw, c + w);
+    rc = trsm_right_lt<T>(st, A, lda, c, hw, c + hw, c + w);
     if (rc) return rc;
-    // A22 -= L21 L21^T on the lower triangle (column-major upper).
-    NMX_CUBLAS_TRY(syrk_sub(h, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
-                            A + (int64_t)(c + hw) * lda + c + hw, lda));
-    return potrf_rec<T>(h, st, A, lda, c + hw, w - hw, info);
+    // A22 -= L21 L21^T on the lower triangle.
+    NMX_TRY(gemm_sub_bt<T>(st, w - hw, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
+                           A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)(c + hw) * lda + c + hw,
+                           lda, true));
+    return potrf_rec<T>(st, A, lda, c + hw, w - hw, info);
 }
 
 template <typename T>
@@ -270,10 +258,7 @@ static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     if (n == 0) return 0;
-    cublasHandle_t h;
-    int rc = ctx_cublas(ctx, st, &h);
-    if (rc) return rc;
-    rc = potrf_rec<T>(h, st, A, lda, 0, (int)n, info);
+    int rc = potrf_rec<T>(st, A, lda, 0, (int)n, info);
     if (rc) return rc;
     const int threads = 256;
     zero_upper_kernel<T><<<(unsigned)ceil_div(n * n, threads), threads, 0, st>>>(A, lda, (int)n);
@@ -296,9 +281,7 @@ static int potrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *L, int64_t lda, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     GemmSub gs;
     gs.st = st;
-    int rc = ctx_cublas(ctx, st, &gs.h);
-    if (rc) return rc;
-    rc = trsm_lower<T, false>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
+    int rc = trsm_lower<T, false>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
     if (rc) return rc;
     return trsm_upper<T, true>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
 }

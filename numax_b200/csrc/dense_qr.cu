@@ -187,15 +187,95 @@ __global__ void larft_kernel(const T *gram_part, int G, const T *tau, int k, int
     }
 }
 
+// W = V^T C over the rows of a tall panel, split by rows: CTA (g, b) forms
+// the partial product of row chunk g with columns [256 b, 256 b + 256) of C
+// -- one thread per column, kQrW accumulators, V's rows staged through
+// shared memory -- and leaves it at part[g] (kQrW x nc).  Reads C once.
+constexpr int kVtcRows = 64;
+constexpr int kVtcMaxChunks = 512;
+template <typename T>
+__global__ void __launch_bounds__(256) vtc_partial_kernel(const T *V, const T *C, int64_t ldc,
+                                                          int mk, int nc, int rows_per, T *part) {
+    __shared__ T vs[kVtcRows][kQrW];
+    const int g = blockIdx.x;
+    const int c = blockIdx.y * 256 + threadIdx.x;
+    const int r0 = g * rows_per, r1 = min(mk, r0 + rows_per);
+    T acc[kQrW];
+#pragma unroll
+    for (int j = 0; j < kQrW; ++j) acc[j] = T(0);
+    for (int rb = r0; rb < r1; rb += kVtcRows) {
+        const int nr = min(kVtcRows, r1 - rb);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kVtcRows * kQrW; e += 256) {
+            const int i = e / kQrW, j = e - i * kQrW;
+            vs[i][j] = i < nr ? V[(int64_t)(rb + i) * kQrW + j] : T(0);
+        }
+        __syncthreads();
+        if (c < nc) {
+            const T *col = C + (int64_t)rb * ldc + c;
+#pragma unroll 4
+            for (int i = 0; i < nr; ++i) {
+                const T x = col[(int64_t)i * ldc];
+#pragma unroll
+                for (int j = 0; j < kQrW; ++j) acc[j] += vs[i][j] * x;
+            }
+        }
+    }
+    if (c < nc)
+#pragma unroll
+        for (int j = 0; j < kQrW; ++j) part[((int64_t)g * kQrW + j) * nc + c] = acc[j];
+}
+
+// W = sum over the G partials (in chunk order, so every run sums alike), then
+// Y = Tm W (kQrW x kQrW times kQrW x nc), or Y = W when Tm is null.  A CTA per
+// 16 columns, thread (j, c).
+template <typename T>
+__global__ void __launch_bounds__(kQrW * 16) vtc_reduce_kernel(const T *part, int G, int nc,
+                                                              const T *Tm, T *Y) {
+    __shared__ T w[kQrW][17];
+    const int j = threadIdx.x / 16, cc = threadIdx.x % 16, c = blockIdx.x * 16 + cc;
+    T s = T(0);
+    if (c < nc) {
+#pragma unroll 8
+        for (int g = 0; g < G; ++g) s += part[((int64_t)g * kQrW + j) * nc + c];
+    }
+    w[j][cc] = s;
+    __syncthreads();
+    if (c >= nc) return;
+    if (Tm) {
+        T y = T(0);
+#pragma unroll
+        for (int p = 0; p < kQrW; ++p) y += Tm[j * kQrW + p] * w[p][cc];
+        Y[(int64_t)j * nc + c] = y;
+    } else {
+        Y[(int64_t)j * nc + c] = s;
+    }
+}
+
 template <typename T>
 struct QrRun {
     nmx_ctx ctx;
     cudaStream_t st;
-    cublasHandle_t h;
     int m;
-    T *Vd, *Tm, *Wk, *Yk;  // V (m x 16), T (16 x 16), W and Y (16 x n)
+    T *Vd, *Tm, *Yk;  // V (m x 16), T (16 x 16), Y (16 x n)
+    T *part;          // kVtcMaxChunks x 16 x n partial products
     QrScratch<T> sc;
 };
+
+// Y = Tm V^T C (Tm null: Y = V^T C) for the mk x nc block C.
+template <typename T>
+static int vtc(QrRun<T> &R, int mk, const T *C, int64_t ldc, int nc, const T *Tm, T *Y) {
+    const int cb = (int)ceil_div(nc, 256);
+    int G = (int)std::min<int64_t>({ceil_div(mk, 256), (int64_t)kVtcMaxChunks,
+                                    std::max<int64_t>(1, 4 * (int64_t)R.ctx->sm_count / cb)});
+    G = std::max(G, 1);
+    const int rows_per = (int)ceil_div(mk, G);
+    G = (int)ceil_div(mk, rows_per);
+    vtc_partial_kernel<T><<<dim3(G, cb), 256, 0, R.st>>>(R.Vd, C, ldc, mk, nc, rows_per, R.part);
+    vtc_reduce_kernel<T><<<(unsigned)ceil_div(nc, 16), kQrW * 16, 0, R.st>>>(R.part, G, nc, Tm, Y);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
 
 // Factor the panel at column k (width w) and record V and T' for it.
 template <typename T>
@@ -226,34 +306,30 @@ static int apply_reflector(QrRun<T> &R, int k, T *Cm, int64_t ldc, int c0, int c
     const int nc = c1 - c0, mk = R.m - k;
     if (nc <= 0) return 0;
     T *C = Cm + (int64_t)k * ldc + c0;
-    NMX_CUBLAS_TRY(gemm_rm(R.h, true, false, kQrW, nc, mk, T(1), R.Vd, kQrW, C, ldc, T(0), R.Wk, nc));
-    NMX_CUBLAS_TRY(gemm_rm(R.h, false, false, kQrW, nc, kQrW, T(1), R.Tm, kQrW, R.Wk, nc, T(0), R.Yk,
-                           nc));
-    NMX_CUBLAS_TRY(gemm_rm(R.h, false, false, mk, nc, kQrW, T(-1), R.Vd, kQrW, R.Yk, nc, T(1), C, ldc));
-    return 0;
+    // Y = T' (V^T C), then C -= V Y.
+    NMX_TRY(vtc<T>(R, mk, C, ldc, nc, R.Tm, R.Yk));
+    return gemm_cc<T>(R.st, false, false, mk, nc, kQrW, T(-1), R.Vd, kQrW, R.Yk, nc, T(1), C, ldc);
 }
 
 template <typename T>
 static int qr_setup(nmx_ctx ctx, cudaStream_t st, int64_t m, int64_t n, QrRun<T> &R) {
-    cublasHandle_t h;
-    int rc = ctx_cublas(ctx, st, &h);
-    if (rc) return rc;
     const int G = ctx->sm_count;
-    size_t elems = (size_t)m * kQrW + kQrW * kQrW + 2 * (size_t)kQrW * std::max<int64_t>(n, 1) +
-                   2 * (size_t)G * (kQrW + 1) + 2 + (size_t)G * kQrW * kQrW + 64;
+    const size_t nn = (size_t)std::max<int64_t>(n, kQrW);
+    size_t elems = (size_t)m * kQrW + kQrW * kQrW + (size_t)kQrW * nn +
+                   (size_t)kVtcMaxChunks * kQrW * nn + 2 * (size_t)G * (kQrW + 1) + 2 +
+                   (size_t)G * kQrW * kQrW + 64;
     void *wsv = nullptr;
-    rc = ctx->ensure_slot(kWsWork, sizeof(T) * elems + 64, &wsv);
+    int rc = ctx->ensure_slot(kWsWork, sizeof(T) * elems + 64, &wsv);
     if (rc) return rc;
     T *ws = static_cast<T *>(wsv);
     R.ctx = ctx;
     R.st = st;
-    R.h = h;
     R.m = (int)m;
     R.Vd = ws;
     R.Tm = R.Vd + (size_t)m * kQrW;
-    R.Wk = R.Tm + kQrW * kQrW;
-    R.Yk = R.Wk + (size_t)kQrW * std::max<int64_t>(n, 1);
-    R.sc.part = R.Yk + (size_t)kQrW * std::max<int64_t>(n, 1);
+    R.Yk = R.Tm + kQrW * kQrW;
+    R.part = R.Yk + (size_t)kQrW * nn;
+    R.sc.part = R.part + (size_t)kVtcMaxChunks * kQrW * nn;
     R.sc.alpha = R.sc.part + 2 * (size_t)G * (kQrW + 1);
     R.sc.gram_part = R.sc.alpha + 2;
     R.sc.bar = reinterpret_cast<unsigned *>(R.sc.gram_part + (size_t)G * kQrW * kQrW);
@@ -337,8 +413,7 @@ static int orgqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, con
                                                                              R.Vd, nullptr);
         NMX_CUDA_TRY(cudaGetLastError());
         // Gram matrix of V for T (one partial), then T.
-        NMX_CUBLAS_TRY(gemm_rm(R.h, true, false, kQrW, kQrW, mk, T(1), R.Vd, kQrW, R.Vd, kQrW, T(0),
-                               R.sc.gram_part, kQrW));
+        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, nullptr, R.sc.gram_part));
         larft_kernel<T><<<1, 256, 0, st>>>(R.sc.gram_part, 1, tau, k, w, R.Tm, 0);
         NMX_CUDA_TRY(cudaGetLastError());
         rc = apply_reflector<T>(R, k, Q, ldq, k, (int)n);

@@ -132,6 +132,43 @@ __global__ void round_split_bf16_kernel(const float *src, int64_t lds, int rows,
     }
 }
 
+// BF16X6 operands: x = h + m + l with h = bf16(x), m = bf16(x - h),
+// l = bf16(x - h - m) (24 significant bits, FP32's), and the six products
+// with i + j <= 2 as one GEMM over 6 K:
+//   A' = [h | h | m | h | m | l],  B' = [h; m; h; l; m; h]
+// i.e. hh + hm + mh + hl + mm + lh.  The dropped terms are below FP32's
+// rounding of the FP32 accumulation.  Zero past rows x cols.
+template <bool IS_A>
+__global__ void round_split6_bf16_kernel(const float *src, int64_t lds, int rows, int cols,
+                                         int rows_p, int cols_p, cutlass::bfloat16_t *dst,
+                                         int64_t ldd) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)rows_p * cols_p) return;
+    const int r = (int)(e / cols_p), c = (int)(e - (int64_t)r * cols_p);
+    const float v = (r < rows && c < cols) ? src[(int64_t)r * lds + c] : 0.0f;
+    const cutlass::bfloat16_t h(v);
+    const float r1 = v - float(h);
+    const cutlass::bfloat16_t m(r1);
+    const cutlass::bfloat16_t l(r1 - float(m));
+    if (IS_A) {
+        cutlass::bfloat16_t *d = dst + (int64_t)r * ldd;
+        d[c] = h;
+        d[cols_p + c] = h;
+        d[2 * cols_p + c] = m;
+        d[3 * cols_p + c] = h;
+        d[4 * cols_p + c] = m;
+        d[5 * cols_p + c] = l;
+    } else {
+        const cutlass::bfloat16_t seg[6] = {h, m, h, l, m, h};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) dst[(int64_t)(q * rows_p + r) * ldd + c] = seg[q];
+    }
+}
+
+static inline int split_factor(int precision) {
+    return precision == NMX_PREC_BF16X3 ? 3 : precision == NMX_PREC_BF16X6 ? 6 : 1;
+}
+
 // The GEMM runs on K and N rounded up to multiples of 8 (the 16-byte TMA and
 // epilogue granularity): the padded rows/columns of the 16-bit operands are
 // zero, so the extra columns of C (up to N rounded to 8) get C - 0 and are
@@ -152,7 +189,7 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         set_error("tensor-core update: C must be 16-byte aligned, ldc %% 4 == 0, ldc >= N rounded to 8");
         return NMX_ERR_INTERNAL;
     }
-    const int64_t Kw = precision == NMX_PREC_BF16X3 ? 3 * Kp : Kp;  // K of the 16-bit GEMM
+    const int64_t Kw = split_factor(precision) * Kp;  // K of the 16-bit GEMM
     auto *a16 = static_cast<unsigned char *>(ws);
     auto *b16 = a16 + ((2 * (size_t)M * Kw + 255) & ~size_t(255));
     const int threads = 256;
@@ -168,13 +205,20 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
         NMX_CUDA_TRY(cudaGetLastError());
         rc = sm_limit > 0 ? tc::fp16s::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, sm_limit)
                           : tc::fp16::run((int)M, (int)Np, (int)Kp, a, Kp, b, Np, C, ldc, st, 0);
-    } else if (precision == NMX_PREC_BF16X3) {
+    } else if (precision == NMX_PREC_BF16X3 || precision == NMX_PREC_BF16X6) {
         auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
         auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
-        round_split_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
-                                                              (int)Kp, a, Kw);
-        round_split_bf16_kernel<false><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N, (int)Kp,
-                                                               (int)Np, b, Np);
+        if (precision == NMX_PREC_BF16X3) {
+            round_split_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                  (int)Kp, a, Kw);
+            round_split_bf16_kernel<false><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N,
+                                                                   (int)Kp, (int)Np, b, Np);
+        } else {
+            round_split6_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                   (int)Kp, a, Kw);
+            round_split6_bf16_kernel<false><<<gb, threads, 0, st>>>(B, ldb, (int)K, (int)N,
+                                                                    (int)Kp, (int)Np, b, Np);
+        }
         NMX_CUDA_TRY(cudaGetLastError());
         rc = sm_limit > 0 ? tc::bf16s::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st, sm_limit)
                           : tc::bf16::run((int)M, (int)Np, (int)Kw, a, Kw, b, Np, C, ldc, st, 0);
@@ -199,7 +243,7 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
 }
 
 size_t tc_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int precision) {
-    const int64_t Kp = up8(K) * (precision == NMX_PREC_BF16X3 ? 3 : 1), Np = up8(N);
+    const int64_t Kp = up8(K) * split_factor(precision), Np = up8(N);
     return ((2 * (size_t)M * Kp + 255) & ~size_t(255)) + 2 * (size_t)Kp * Np + 512;
 }
 
@@ -219,8 +263,9 @@ extern "C" NMX_API int nmx_gemm_sub_f32(nmx_ctx ctx, int64_t M, int64_t N, int64
     NMX_ARG_CHECK(C != nullptr || M * N == 0, 9, "C is NULL");
     NMX_ARG_CHECK(ldc >= std::max<int64_t>(1, N), 10, "ldc < N");
     NMX_ARG_CHECK(precision == NMX_PREC_BF16 || precision == NMX_PREC_FP16 ||
-                      precision == NMX_PREC_BF16X3,
-                  11, "precision must be NMX_PREC_BF16, NMX_PREC_FP16 or NMX_PREC_BF16X3");
+                      precision == NMX_PREC_BF16X3 || precision == NMX_PREC_BF16X6,
+                  11, "precision must be NMX_PREC_BF16, NMX_PREC_FP16, NMX_PREC_BF16X3 or "
+                      "NMX_PREC_BF16X6");
     if (M == 0 || N == 0 || K == 0) return 0;
     DeviceGuard g(ctx->device);
     void *ws = nullptr;

@@ -8,12 +8,14 @@
 #define NMX_PREC_BF16 1
 #define NMX_PREC_FP16 2
 #define NMX_PREC_BF16X3 3
+#define NMX_PREC_BF16X6 4
 #endif
 
 namespace nmx {
 
 // C[M x N] -= round(A)[M x K] * round(B)[K x N], fp32 row-major operands,
-// rounded to BF16 (precision = NMX_PREC_BF16) or FP16 into `ws` first.
+// rounded to BF16 (precision = NMX_PREC_BF16) or FP16, or split into 2 / 3
+// BF16 pieces (NMX_PREC_BF16X3 / NMX_PREC_BF16X6), into `ws` first.
 // C must be 16-byte aligned with ldc % 4 == 0.  sm_limit > 0 keeps the GEMM
 // on at most that many SMs.
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,

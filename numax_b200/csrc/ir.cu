@@ -4,20 +4,36 @@
 // north-star addition for the large solve.  A (FP64, row-major) is factored
 // once in low precision and the solution is refined in FP64:
 //
-//   W = (float) R A C        R, C power-of-two row/column scalings (exact)
-//   P W = L U                the recursive LU of dense_lu.cu with its trailing
-//                            updates on the tensor cores (BF16 or FP16 in,
-//                            FP32 accumulate) or FP32 CUDA cores
+//   W = (float) R A C        R, C power-of-two row/column scalings (exact;
+//                            FP16 factors only, which need the range)
+//   P W = L U                the LU of dense_lu.cu (tournament pivoting,
+//                            look-ahead) with its trailing updates on the
+//                            tensor cores: BF16 or FP16 operands, or BF16
+//                            hi/lo splits (BF16X3, ~16 bits) or hi/mid/lo
+//                            splits (BF16X6, FP32's 24 bits), FP32 accumulate
 //   x = 0, r = b
-//   repeat: d = C U^-1 L^-1 P R r   (triangular solves read the FP32 factors,
+//   repeat: d = C U^-1 L^-1 P R r   (triangular solves read the factors,
 //                                    arithmetic in FP64)
 //           x += d; r = b - A x (FP64 GEMV over the original A)
 //   until ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol
 //
-// GMRES-IR (Carson & Higham) replaces the correction solve by restarted
-// GMRES on the left-preconditioned system (U^-1 L^-1 P R A C) y = U^-1 L^-1 P R r,
-// all Krylov arithmetic in FP64 with A applied in FP64, for conditioning
-// beyond what plain refinement with 16-bit factors converges on.
+// GMRES-IR (Carson & Higham, SIAM J. Sci. Comput. 40(2), 2018) replaces the
+// correction solve by GMRES on the left-preconditioned system
+// (C U^-1 L^-1 P R A) d = C U^-1 L^-1 P R r, in FP64 with A applied in FP64.
+// The whole Arnoldi step stays on the device: the matrix-vector product and
+// the two triangular solves, classical Gram-Schmidt twice (CGS2) as per-CTA
+// partial dot products reduced in a fixed order, the norm, the Givens
+// rotation of the new Hessenberg column and the convergence test run as
+// kernels that read and write a device-resident state; a step whose state
+// says "done" returns at once, so the host launches steps in chunks and
+// reads the state once per chunk.
+//
+// A refinement that cannot converge at its precision (the backward error
+// stops halving, or GMRES stops reducing its residual) hands over, with
+// NMX_IR_AUTO, from plain refinement to GMRES-IR, and with NMX_IR_ESCALATE
+// refactors one level up (BF16 or FP16 -> BF16X3 -> BF16X6 -> FP64) and
+// refines on from the best iterate so far.  The iterate with the smallest
+// backward error is the one returned.
 //
 // The single-right-hand-side triangular solves are one persistent kernel
 // each: CTAs take 64-row blocks in order from an atomic counter, stream the
@@ -27,6 +43,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dense_common.cuh"
@@ -37,8 +54,11 @@ namespace nmx {
 constexpr int kTrsvRB = 64;
 constexpr int kTrsvThreads = 256;
 constexpr int kTrsvPitch = kTrsvRB + 4;
-constexpr size_t kTrsvSmem = (sizeof(double) + sizeof(float)) * kTrsvRB * kTrsvPitch;
 constexpr long long kTrsvSpin = 1ll << 25;
+template <typename TF>
+constexpr size_t trsv_smem() {
+    return (sizeof(double) + sizeof(TF)) * kTrsvRB * kTrsvPitch;
+}
 
 __device__ __forceinline__ int ld_acquire_i32(const int *p) {
     int v;
@@ -50,13 +70,13 @@ __device__ __forceinline__ void st_release_i32(int *p, int v) {
 }
 
 // Inverse of every 64 x 64 diagonal block of the unit-lower (UPPER = false)
-// or upper (UPPER = true) triangle of the FP32 factor, in FP64: one CTA per
-// block, thread j forms column j of the inverse by substitution.  Computed
-// once per factorization; it turns each block's serial substitution in the
-// triangular solves into a 64 x 64 matrix-vector product.
-template <bool UPPER>
+// or upper (UPPER = true) triangle of the factor F (FP32 or FP64), in FP64:
+// one CTA per block, thread j forms column j of the inverse by substitution.
+// Computed once per factorization; it turns each block's serial substitution
+// in the triangular solves into a 64 x 64 matrix-vector product.
+template <typename TF, bool UPPER>
 __global__ void __launch_bounds__(kTrsvRB)
-    diag_inverse_kernel(const float *F, int64_t ldf, int n, double *Inv) {
+    diag_inverse_kernel(const TF *F, int64_t ldf, int n, double *Inv) {
     __shared__ double D[kTrsvRB][kTrsvRB + 1];
     const int b = blockIdx.x, r0 = b * kTrsvRB, rows = min(kTrsvRB, n - r0);
     const int j = threadIdx.x;
@@ -95,10 +115,35 @@ __global__ void __launch_bounds__(kTrsvRB)
     for (int i = 0; i < kTrsvRB; ++i) out[i * kTrsvRB + j] = (j < rows && i < rows) ? x[i] : 0.0;
 }
 
+__device__ __forceinline__ void cp_async_n(unsigned dst, const void *src, int bytes) {
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(unsigned dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all_() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <typename TF>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+
 // Solve with the unit-lower (UPPER = false) or upper (UPPER = true) triangle
-// of the FP32 factor F (n x n, ldf) in place on the FP64 vector x, using the
-// precomputed FP64 inverses Inv of its 64 x 64 diagonal blocks.
+// of the factor F (n x n, ldf; FP32 or FP64) in place on the FP64 vector x,
+// using the precomputed FP64 inverses Inv of its 64 x 64 diagonal blocks.
 // counter[0]: block ticket, counter[1]: blocks finished, counter[2]: error.
+// `stop` (may be null): when it reads nonzero at entry the kernel does
+// nothing (a finished GMRES step).  `out` (may be null): also writes
+// out[i] = cs[i] x[i] as each block finishes.
 //
 // A CTA takes 64-row blocks in solve order.  It accumulates the block's row
 // segments against the solution blocks finished so far as they appear, all
@@ -107,26 +152,21 @@ __global__ void __launch_bounds__(kTrsvRB)
 // shared memory asynchronously.  So once the adjacent block is released,
 // what remains on the chain from block to block is one 64-value read of x,
 // two 64 x 64 products out of shared memory, and the release.
-__device__ __forceinline__ void cp_async_4(unsigned dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_16(unsigned dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all_() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-template <bool UPPER>
+template <typename TF, bool UPPER>
 __global__ void __launch_bounds__(kTrsvThreads)
-    trsv_f32f64_kernel(const float *F, int64_t ldf, int n, const double *Inv, double *x,
-                       int *counter) {
+    trsv_kernel(const TF *F, int64_t ldf, int n, const double *Inv, double *x, int *counter,
+                const int *stop, const double *cs, double *out) {
+    using P2 = typename Pair<TF>::type;
     // Dynamic shared memory: Is[64][68] (Inv of this block, FP64) then
     // Ft[64][68] (the F tile against the adjacent block).  Row pitch 68 with
     // thread (i, part) reading columns part + 4m keeps both conflict-free.
-    extern __shared__ __align__(16) unsigned char trsv_smem[];
-    auto Is = reinterpret_cast<double(*)[kTrsvPitch]>(trsv_smem);
-    auto Ft = reinterpret_cast<float(*)[kTrsvPitch]>(trsv_smem + sizeof(double) * kTrsvRB * kTrsvPitch);
+    extern __shared__ __align__(16) unsigned char trsv_smem_raw[];
+    auto Is = reinterpret_cast<double(*)[kTrsvPitch]>(trsv_smem_raw);
+    auto Ft = reinterpret_cast<TF(*)[kTrsvPitch]>(trsv_smem_raw +
+                                                   sizeof(double) * kTrsvRB * kTrsvPitch);
     __shared__ double accS[kTrsvRB], xs[kTrsvRB], ys[kTrsvRB];
     __shared__ int s_blk, s_avail;
+    if (stop && *stop) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int NB = (n + kTrsvRB - 1) / kTrsvRB;
     // Column range of the finished blocks with solve-order indices [d0, d1).
@@ -191,8 +231,8 @@ __global__ void __launch_bounds__(kTrsvThreads)
             const int nd = min(avail, ticket - 1);
             int c0, c1;
             cols(done, nd, c0, c1);
-            // Two columns per lane (float2 / double2 loads: c0 is a multiple
-            // of 64, rows are 32-byte aligned, x 16-byte aligned), the 8 rows
+            // Two columns per lane (pair loads: c0 is a multiple of 64, rows
+            // start on 8-element boundaries, x 16-byte aligned), the 8 rows
             // and 2 iterations in flight: this stream must keep ahead of the
             // chain of blocks, so it needs memory-level parallelism.
             int c = c0 + 2 * lane;
@@ -202,7 +242,7 @@ __global__ void __launch_bounds__(kTrsvThreads)
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int i = min(8 * warp + q, rows - 1);
-                    const float2 f = *reinterpret_cast<const float2 *>(F + (int64_t)(r0 + i) * ldf + c);
+                    const P2 f = *reinterpret_cast<const P2 *>(F + (int64_t)(r0 + i) * ldf + c);
                     acc[q] += (double)f.x * xv.x + (double)f.y * xv.y;
                 }
             }
@@ -230,10 +270,10 @@ __global__ void __launch_bounds__(kTrsvThreads)
             for (int e = tid; e < kTrsvRB * kTrsvRB; e += kTrsvThreads) {
                 const int i = e >> 6, c = e & 63;
                 if (i < rows && a0 + c < a1)
-                    cp_async_4(ft0 + (unsigned)(i * kTrsvPitch + c) * 4u,
-                               F + (int64_t)(r0 + i) * ldf + a0 + c);
+                    cp_async_n(ft0 + (unsigned)(i * kTrsvPitch + c) * (unsigned)sizeof(TF),
+                               F + (int64_t)(r0 + i) * ldf + a0 + c, (int)sizeof(TF));
                 else
-                    Ft[i][c] = 0.0f;
+                    Ft[i][c] = TF(0);
             }
         }
         if (ticket > 0) {
@@ -264,7 +304,10 @@ __global__ void __launch_bounds__(kTrsvThreads)
             for (int m = 0; m < 16; ++m) s += Is[i][part + 4 * m] * ys[part + 4 * m];
             s += __shfl_xor_sync(0xffffffffu, s, 1);
             s += __shfl_xor_sync(0xffffffffu, s, 2);
-            if (part == 0 && i < rows) x[r0 + i] = s;
+            if (part == 0 && i < rows) {
+                x[r0 + i] = s;
+                if (out) out[r0 + i] = cs[r0 + i] * s;
+            }
         }
         __threadfence();
         __syncthreads();
@@ -272,23 +315,28 @@ __global__ void __launch_bounds__(kTrsvThreads)
     }
 }
 
+// One row of A times v (FP64), a warp per row; the lanes' sum on lane 0.
+__device__ __forceinline__ double row_dot(const double *row, const double *v, int n, int lane) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int c = lane;
+    for (; c + 96 < n; c += 128) {
+        s0 += row[c] * v[c];
+        s1 += row[c + 32] * v[c + 32];
+        s2 += row[c + 64] * v[c + 64];
+        s3 += row[c + 96] * v[c + 96];
+    }
+    for (; c < n; c += 32) s0 += row[c] * v[c];
+    double s = (s0 + s1) + (s2 + s3);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
 // r = b - A x (FP64), one warp per row; rmax <- max |r_i| (as ordered bits).
 __global__ void residual_kernel(const double *A, int64_t lda, int n, const double *x,
                                 const double *b, double *r, unsigned long long *rmax) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n) return;
-    const double *row = A + (int64_t)warp * lda;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    int c = lane;
-    for (; c + 96 < n; c += 128) {
-        s0 += row[c] * x[c];
-        s1 += row[c + 32] * x[c + 32];
-        s2 += row[c + 64] * x[c + 64];
-        s3 += row[c + 96] * x[c + 96];
-    }
-    for (; c < n; c += 32) s0 += row[c] * x[c];
-    double s = (s0 + s1) + (s2 + s3);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double s = row_dot(A + (int64_t)warp * lda, x, n, lane);
     if (lane == 0) {
         const double v = b[warp] - s;
         r[warp] = v;
@@ -296,7 +344,7 @@ __global__ void residual_kernel(const double *A, int64_t lda, int n, const doubl
     }
 }
 
-// max_i sum_j |A_ij| (||A||_inf) and optional per-row max |A_ij|.
+// max_i sum_j |A_ij| (||A||_inf) and per-row max |A_ij|.
 __global__ void row_norms_kernel(const double *A, int64_t lda, int n, unsigned long long *norm_inf,
                                  double *rowmax) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -314,7 +362,7 @@ __global__ void row_norms_kernel(const double *A, int64_t lda, int n, unsigned l
     }
     if (lane == 0) {
         atomicMax(norm_inf, (unsigned long long)__double_as_longlong(s));
-        if (rowmax) rowmax[warp] = m;
+        rowmax[warp] = m;
     }
 }
 
@@ -367,13 +415,14 @@ __global__ void col_scale_kernel(const unsigned long long *cmax, int n, double *
     if (j < n) cs[j] = enabled ? pow2_inv(__longlong_as_double((long long)cmax[j])) : 1.0;
 }
 
-// W = (float)(R A C).
-__global__ void scale_to_f32_kernel(const double *A, int64_t lda, int n, const double *rs,
-                                    const double *cs, float *W, int64_t ldw) {
+// W = (TW)(R A C), W row-major with ldw.
+template <typename TW>
+__global__ void scale_copy_kernel(const double *A, int64_t lda, int n, const double *rs,
+                                  const double *cs, TW *W, int64_t ldw) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)n * n) return;
     const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
-    W[(int64_t)i * ldw + j] = (float)(A[(int64_t)i * lda + j] * rs[i] * cs[j]);
+    W[(int64_t)i * ldw + j] = (TW)(A[(int64_t)i * lda + j] * rs[i] * cs[j]);
 }
 
 // v[i] = s[perm[i]] * rs[perm[i]]  (apply P R to a vector).
@@ -383,38 +432,285 @@ __global__ void permute_scale_kernel(const double *s, const int *perm, const dou
     if (i < n) v[i] = s[perm[i]] * rs[perm[i]];
 }
 
-// x += C v  (or x = C v when assign).
-__global__ void axpy_scale_kernel(const double *v, const double *cs, int n, double *x, int assign) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x[i] = assign ? cs[i] * v[i] : x[i] + cs[i] * v[i];
-}
-
 __global__ void add_kernel(const double *v, int n, double *x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] += v[i];
 }
 
-__global__ void scale_vec_kernel(const double *v, const double *cs, int n, double *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = cs[i] * v[i];
+// ---- GMRES on the device ------------------------------------------------
+
+constexpr int kRestart = 200;    // Krylov basis size per GMRES cycle
+constexpr int kGmresChunk = 6;   // Arnoldi steps launched between host reads
+constexpr int kSlowStep = 32;    // step at which a slow cycle is abandoned
+constexpr int kCgsThreads = 256;
+
+// flag: 0 running, 1 converged, 2 breakdown (the Krylov space is invariant:
+// the least-squares solution is exact), 3 basis full, 4 too slow (after
+// kSlowStep steps the residual has not dropped tenfold).
+struct GmresState {
+    int flag;
+    int k;        // Arnoldi steps completed (basis vectors V_0 .. V_k)
+    int ky;       // length of y after the solve
+    int slow_at;  // step of the "too slow" test (0: none)
+    double beta, tol, inv_hn, pad2;
+    double H[(kRestart + 1) * kRestart];  // H[j * kRestart + k]
+    double cs[kRestart], sn[kRestart], g[kRestart + 1], y[kRestart], hcur[kRestart + 1];
+};
+
+// out[pinv[i]] = rs[i] (A V_k)[i]: P R A v with v the newest basis vector.
+__global__ void gmres_matvec_kernel(const double *A, int64_t lda, int n, const double *V,
+                                    const GmresState *st, const double *rs, const int *pinv,
+                                    double *out) {
+    if (st->flag) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double *v = V + (size_t)st->k * n;
+    const double s = row_dot(A + (int64_t)warp * lda, v, n, lane);
+    if (lane == 0) out[pinv[warp]] = rs[warp] * s;
+}
+
+// Stage rows [r0, r1) of w in shared memory.  part[g][j] = V_j[chunk] . w[chunk]
+// for j <= k, a warp per j.
+__device__ __forceinline__ void chunk_dots(const double *V, int n, const double *wsm, int r0,
+                                           int len, int kc, double *part_row) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = wp; j < kc; j += nw) {
+        const double *vj = V + (size_t)j * n + r0;
+        double s = 0.0;
+        for (int i = lane; i < len; i += 32) s += vj[i] * wsm[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) part_row[j] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kCgsThreads)
+    cgs_dots_kernel(const double *V, int n, const double *w, int rows_per, const GmresState *st,
+                    double *part) {
+    if (st->flag) return;
+    extern __shared__ double wsm[];
+    const int g = blockIdx.x, r0 = g * rows_per, len = min(n, r0 + rows_per) - r0;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) wsm[i] = w[r0 + i];
+    __syncthreads();
+    chunk_dots(V, n, wsm, r0, len, st->k + 1, part + (size_t)g * (kRestart + 1));
+}
+
+// h_j = sum_g part[g][j] in chunk order; pass 0: H[:, k] = h, pass 1: H[:, k] += h.
+__global__ void cgs_reduce_kernel(const double *part, int G, GmresState *st, int pass) {
+    if (st->flag) return;
+    const int k = st->k, j = threadIdx.x;
+    if (j > k) return;
+    double s = 0.0;
+    for (int g = 0; g < G; ++g) s += part[(size_t)g * (kRestart + 1) + j];
+    st->hcur[j] = s;
+    st->H[j * kRestart + k] = pass ? st->H[j * kRestart + k] + s : s;
+}
+
+// w -= V h over the chunk.  mode 0: part[g][j] = V_j . w (the second pass's
+// projections); mode 1: the new vector goes to V_{k+1} and part[g][0] =
+// ||w||^2 over the chunk.
+__global__ void __launch_bounds__(kCgsThreads)
+    cgs_update_kernel(double *V, int n, double *w, int rows_per, const GmresState *st,
+                      double *part, int mode) {
+    if (st->flag) return;
+    extern __shared__ double wsm[];
+    __shared__ double h[kRestart + 1];
+    __shared__ double red[kCgsThreads / 32];
+    const int kc = st->k + 1;
+    const int g = blockIdx.x, r0 = g * rows_per, len = min(n, r0 + rows_per) - r0;
+    for (int j = threadIdx.x; j < kc; j += blockDim.x) h[j] = st->hcur[j];
+    __syncthreads();
+    double *dst = mode ? V + (size_t)kc * n : w;
+    double ss = 0.0;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        double s = w[r0 + i];
+        for (int j = 0; j < kc; ++j) s -= V[(size_t)j * n + r0 + i] * h[j];
+        wsm[i] = s;
+        dst[r0 + i] = s;
+        ss += s * s;
+    }
+    if (mode == 0) {
+        __syncthreads();
+        chunk_dots(V, n, wsm, r0, len, kc, part + (size_t)g * (kRestart + 1));
+    } else {
+        for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+            part[(size_t)g * (kRestart + 1)] = t;
+        }
+    }
+}
+
+// part[g][0] = ||v||^2 over chunk g (the first basis vector's norm).
+__global__ void __launch_bounds__(kCgsThreads)
+    chunk_norm2_kernel(const double *v, int n, int rows_per, double *part) {
+    __shared__ double red[kCgsThreads / 32];
+    const int g = blockIdx.x, r0 = g * rows_per, r1 = min(n, r0 + rows_per);
+    double ss = 0.0;
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) ss += v[i] * v[i];
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+        part[(size_t)g * (kRestart + 1)] = t;
+    }
+}
+
+// One thread: beta = ||z0||, g = beta e1, k = 0.
+__global__ void gmres_start_kernel(const double *part, int G, GmresState *st, double tol,
+                                   int slow_at) {
+    double ss = 0.0;
+    for (int g = 0; g < G; ++g) ss += part[(size_t)g * (kRestart + 1)];
+    const double beta = sqrt(ss);
+    st->beta = beta;
+    st->tol = tol;
+    st->k = 0;
+    st->ky = 0;
+    st->slow_at = slow_at;
+    st->g[0] = beta;
+    st->inv_hn = beta > 0.0 ? 1.0 / beta : 0.0;
+    st->flag = (beta > 0.0 && isfinite(beta)) ? 0 : 2;
+}
+
+// One thread: h_{k+1,k} = ||w||, the earlier rotations applied to column k of
+// H, a new rotation zeroing h_{k+1,k}, g updated, the stopping tests.
+__global__ void arnoldi_finish_kernel(const double *part, int G, GmresState *st) {
+    if (st->flag) return;
+    const int k = st->k;
+    double ss = 0.0;
+    for (int g = 0; g < G; ++g) ss += part[(size_t)g * (kRestart + 1)];
+    const double hn = sqrt(ss);
+    double *H = st->H;
+    for (int j = 0; j < k; ++j) {
+        const double a = H[j * kRestart + k], b = H[(j + 1) * kRestart + k];
+        H[j * kRestart + k] = st->cs[j] * a + st->sn[j] * b;
+        H[(j + 1) * kRestart + k] = -st->sn[j] * a + st->cs[j] * b;
+    }
+    const double a = H[k * kRestart + k];
+    const double rr = hypot(a, hn);
+    const double c = rr > 0.0 ? a / rr : 1.0, s = rr > 0.0 ? hn / rr : 0.0;
+    st->cs[k] = c;
+    st->sn[k] = s;
+    H[k * kRestart + k] = rr;
+    st->g[k + 1] = -s * st->g[k];
+    st->g[k] = c * st->g[k];
+    st->k = k + 1;
+    st->inv_hn = hn > 0.0 ? 1.0 / hn : 0.0;
+    const double res = fabs(st->g[k + 1]);
+    if (res <= st->tol * st->beta)
+        st->flag = 1;
+    else if (!(hn > 0.0) || !isfinite(hn))
+        st->flag = 2;
+    else if (k + 1 == kRestart)
+        st->flag = 3;
+    else if (k + 1 == st->slow_at && res > 0.1 * st->beta)
+        st->flag = 4;
+}
+
+// V_k *= inv_hn (k already counts the new vector).
+__global__ void scale_basis_kernel(double *V, int n, const GmresState *st) {
+    if (st->flag) return;
+    double *v = V + (size_t)st->k * n;
+    const double s = st->inv_hn;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] *= s;
+}
+
+// One thread: y = R^-1 g over the leading k x k triangle of the rotated H,
+// shortened at the first diagonal that is negligible against the largest
+// (a least-squares solution of the leading block instead of a blow-up).
+__global__ void gmres_solve_kernel(GmresState *st) {
+    const int k = st->k;
+    const double *H = st->H;
+    double hmax = 0.0;
+    for (int i = 0; i < k; ++i) hmax = fmax(hmax, fabs(H[i * kRestart + i]));
+    int kk = k;
+    for (int i = 0; i < k; ++i)
+        if (!(fabs(H[i * kRestart + i]) > 1e-14 * hmax)) {
+            kk = i;
+            break;
+        }
+    for (int i = kk - 1; i >= 0; --i) {
+        double s = st->g[i];
+        for (int j = i + 1; j < kk; ++j) s -= H[i * kRestart + j] * st->y[j];
+        st->y[i] = s / H[i * kRestart + i];
+    }
+    st->ky = kk;
+}
+
+// x += V y.
+__global__ void gmres_update_kernel(const double *V, int n, const GmresState *st, double *x) {
+    const int ky = st->ky;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < ky; ++j) s += V[(size_t)j * n + i] * st->y[j];
+        x[i] += s;
+    }
 }
 
 // ---- host side ----------------------------------------------------------
 
+// Precision levels, in escalation order.
+enum IrLevel { kLvBF16 = 0, kLvFP16, kLvBF16X3, kLvBF16X6, kLvFP32, kLvFP64 };
+
+static int level_of(int prec) {
+    switch (prec) {
+        case NMX_IR_BF16: return kLvBF16;
+        case NMX_IR_FP16: return kLvFP16;
+        case NMX_IR_BF16X3: return kLvBF16X3;
+        case NMX_IR_BF16X6: return kLvBF16X6;
+        case NMX_IR_FP32: return kLvFP32;
+        default: return kLvFP64;
+    }
+}
+static int prec_of(int level) {
+    static const int p[] = {NMX_IR_BF16, NMX_IR_FP16, NMX_IR_BF16X3, NMX_IR_BF16X6, NMX_IR_FP32,
+                            NMX_IR_FP64};
+    return p[level];
+}
+// The next, more accurate level: 8-bit and 11-bit factors go to ~16 bits,
+// then to FP32's 24 bits, then to FP64 itself.
+static int next_level(int level) {
+    switch (level) {
+        case kLvBF16:
+        case kLvFP16: return kLvBF16X3;
+        case kLvBF16X3: return kLvBF16X6;
+        default: return kLvFP64;
+    }
+}
+static int gemm_precision(int level) {
+    switch (level) {
+        case kLvBF16: return NMX_PREC_BF16;
+        case kLvFP16: return NMX_PREC_FP16;
+        case kLvBF16X3: return NMX_PREC_BF16X3;
+        case kLvBF16X6: return NMX_PREC_BF16X6;
+        default: return 0;
+    }
+}
+
 struct IrRun {
     nmx_ctx ctx;
     cudaStream_t st;
-    cublasHandle_t h;
     int n;
     const double *A;
     int64_t lda;
-    float *W;
+    int level = -1;
+    float *W = nullptr;     // FP32 factors (levels below FP64)
+    double *W64 = nullptr;  // FP64 factors
     int64_t ldw;
-    int *perm;
-    double *rs, *cs, *v, *r, *tmp, *rowmax;
+    int *perm, *pinv;
+    double *rs, *cs, *v, *r, *tmp, *w, *rowmax, *xbest;
     int *counters;  // 3 per triangular solve
     double *invL, *invU;  // inverses of the 64 x 64 diagonal blocks of L and U
-    unsigned long long *norms;  // [0] ||A||_inf, [1] ||r||, [2] ||x||, [3] ||b||, [4] scratch
+    unsigned long long *norms;  // [0] ||A||_inf, [1] ||r||, [2] ||x||, [3] ||b||
+    int32_t *ipiv, *info_d;
+    double *V = nullptr;   // Krylov basis, kRestart + 1 vectors of n
+    double *part = nullptr;
+    GmresState *gst = nullptr;
+    int G = 1, rows_per = 1;  // chunks of the Gram-Schmidt kernels
 };
 
 static double bits_to_double(unsigned long long u) {
@@ -423,25 +719,95 @@ static double bits_to_double(unsigned long long u) {
     return d;
 }
 
-// v := U^-1 L^-1 v (the FP32 factors in W, arithmetic in FP64).
-static int lu_solve_inplace(IrRun &R, double *v) {
+static size_t ir_vec_bytes(int64_t n) {
+    return sizeof(double) * (size_t)n * 9 + sizeof(int) * (size_t)n * 4 + 4096;
+}
+static size_t ir_krylov_bytes(int64_t n, int G) {
+    return sizeof(double) * ((size_t)n * (kRestart + 1) + (size_t)G * (kRestart + 1)) +
+           sizeof(GmresState) + 1024;
+}
+
+// The largest tensor-core update of the FP32 factorization: look-ahead
+// panels of nb columns (tournament leaves, order >= 2 nb; the same decision
+// getrf_run makes) bound its inner dimension at nb; otherwise the recursion's
+// largest update is about half the order.
+static size_t ir_gemm_ws_bytes(nmx_ctx ctx, int64_t n, int prec) {
+    if (!prec) return 0;
+    const bool tournament = ctx->tune_lu_tournament != 0 && n <= tournament_max_rows();
+    const int64_t want = ctx->tune_lu_lookahead >= 0 ? ctx->tune_lu_lookahead : 256;
+    const int64_t nb = std::min<int64_t>(1024, want / 32 * 32);
+    if (tournament && nb >= 64 && n >= 2 * nb)
+        return tc_gemm_workspace_bytes(n, n, nb, prec) + 4096;
+    const int64_t half = (n / 2 + 31) / 32 * 32;
+    return tc_gemm_workspace_bytes(n - half, n - half, std::max<int64_t>(half, 1), prec) + 4096;
+}
+
+// Every buffer a solve at `level` (and, when escalating, at the levels above
+// it) needs, grown now.
+static int ir_reserve(nmx_ctx ctx, int64_t n, int level, bool escalate) {
+    void *p = nullptr;
+    const int64_t ldw = (n + 7) / 8 * 8;
+    const int G = std::max(1, std::min<int>(2 * ctx->sm_count, (int)ceil_div(n, 256)));
+    NMX_TRY(ctx->ensure_slot(kWsVec, ir_vec_bytes(n), &p));
+    NMX_TRY(ctx->ensure_slot(kWsKrylov, ir_krylov_bytes(n, G), &p));
+    NMX_TRY(ctx->ensure_slot(kWsBest, sizeof(double) * (size_t)n + 256, &p));
+    const int NB = (int)ceil_div(n, kTrsvRB);
+    NMX_TRY(ctx->ensure_slot(kWsInv, sizeof(double) * (size_t)NB * kTrsvRB * kTrsvRB * 2 + 256, &p));
+    size_t gemm_ws = 0;
+    bool need32 = false, need64 = false;
+    for (int lv = level;; lv = next_level(lv)) {
+        if (lv == kLvFP64)
+            need64 = true;
+        else
+            need32 = true;
+        gemm_ws = std::max(gemm_ws, ir_gemm_ws_bytes(ctx, n, gemm_precision(lv)));
+        if (!escalate || lv == kLvFP64) break;
+    }
+    if (need32) NMX_TRY(ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * ldw + 256, &p));
+    if (need64) NMX_TRY(ctx->ensure_slot(kWsWork64, sizeof(double) * (size_t)n * ldw + 256, &p));
+    if (gemm_ws) NMX_TRY(ctx->ensure_slot(kWsGemm16, gemm_ws, &p));
+    return 0;
+}
+
+// v := U^-1 L^-1 v with the current level's factors, arithmetic in FP64;
+// with `out`, also out = C v.  `stop`: the GMRES state's flag, or null.
+static int lu_solve_inplace(IrRun &R, double *v, const int *stop, double *out) {
     const int NB = (R.n + kTrsvRB - 1) / kTrsvRB;
     const int want = R.ctx->tune_ir_trsv_ctas > 0 ? (int)R.ctx->tune_ir_trsv_ctas
                                                   : 2 * R.ctx->sm_count;
     const int grid = std::max(1, std::min(NB, want));
-    static bool attr_set[64] = {};
-    if (R.ctx->device < 64 && !attr_set[R.ctx->device]) {
-        NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_f32f64_kernel<false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
-        NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_f32f64_kernel<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
-        attr_set[R.ctx->device] = true;
+    static bool attr_set[64][2] = {};
+    const int f64 = R.level == kLvFP64 ? 1 : 0;
+    if (R.ctx->device < 64 && !attr_set[R.ctx->device][f64]) {
+        if (f64) {
+            NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<double, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)trsv_smem<double>()));
+            NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<double, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)trsv_smem<double>()));
+        } else {
+            NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<float, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)trsv_smem<float>()));
+            NMX_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<float, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)trsv_smem<float>()));
+        }
+        attr_set[R.ctx->device][f64] = true;
     }
     NMX_CUDA_TRY(cudaMemsetAsync(R.counters, 0, 6 * sizeof(int), R.st));
-    trsv_f32f64_kernel<false><<<grid, kTrsvThreads, kTrsvSmem, R.st>>>(R.W, R.ldw, R.n, R.invL, v,
-                                                                       R.counters);
-    trsv_f32f64_kernel<true><<<grid, kTrsvThreads, kTrsvSmem, R.st>>>(R.W, R.ldw, R.n, R.invU, v,
-                                                                      R.counters + 3);
+    if (f64) {
+        trsv_kernel<double, false><<<grid, kTrsvThreads, trsv_smem<double>(), R.st>>>(
+            R.W64, R.ldw, R.n, R.invL, v, R.counters, stop, nullptr, nullptr);
+        trsv_kernel<double, true><<<grid, kTrsvThreads, trsv_smem<double>(), R.st>>>(
+            R.W64, R.ldw, R.n, R.invU, v, R.counters + 3, stop, R.cs, out);
+    } else {
+        trsv_kernel<float, false><<<grid, kTrsvThreads, trsv_smem<float>(), R.st>>>(
+            R.W, R.ldw, R.n, R.invL, v, R.counters, stop, nullptr, nullptr);
+        trsv_kernel<float, true><<<grid, kTrsvThreads, trsv_smem<float>(), R.st>>>(
+            R.W, R.ldw, R.n, R.invU, v, R.counters + 3, stop, R.cs, out);
+    }
     NMX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -450,18 +816,164 @@ static int lu_solve_inplace(IrRun &R, double *v) {
 static int precond_apply(IrRun &R, const double *in, double *out) {
     const int threads = 256, blocks = (int)ceil_div(R.n, threads);
     permute_scale_kernel<<<blocks, threads, 0, R.st>>>(in, R.perm, R.rs, R.n, R.tmp);
-    int rc = lu_solve_inplace(R, R.tmp);
-    if (rc) return rc;
-    scale_vec_kernel<<<blocks, threads, 0, R.st>>>(R.tmp, R.cs, R.n, out);
     NMX_CUDA_TRY(cudaGetLastError());
+    return lu_solve_inplace(R, R.tmp, nullptr, out);
+}
+
+// Factor A at `level` into R's buffers: scalings, the copy, the LU, the
+// diagonal-block inverses (then `done` is recorded, when given), and the
+// permutation (read back to the host).
+static int ir_factor(IrRun &R, int level, int32_t *hinfo, cudaEvent_t done) {
+    nmx_ctx ctx = R.ctx;
+    cudaStream_t st = R.st;
+    const int n = R.n;
+    const int threads = 256;
+    const int vb = (int)ceil_div(n, threads);
+    const int wb = (int)ceil_div((int64_t)n * 32, threads);
+    void *p = nullptr;
+    R.level = level;
+    // ||A||_inf and the row maxima (also the row scales' input).
+    NMX_CUDA_TRY(cudaMemsetAsync(R.norms, 0, sizeof(unsigned long long), st));
+    row_norms_kernel<<<wb, threads, 0, st>>>(R.A, R.lda, n, R.norms, R.rowmax);
+    const int equil = level == kLvFP16 ? 1 : 0;
+    row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
+    if (equil) {
+        // The column maxima go through R.tmp's bits (free until the solve).
+        unsigned long long *cmax = reinterpret_cast<unsigned long long *>(R.tmp);
+        NMX_CUDA_TRY(cudaMemsetAsync(cmax, 0, sizeof(double) * n, st));
+        col_max_kernel<<<dim3(vb, kColChunks), threads, 0, st>>>(R.A, R.lda, n, R.rs, cmax);
+        col_scale_kernel<<<vb, threads, 0, st>>>(cmax, n, R.cs, 1);
+    } else {
+        col_scale_kernel<<<vb, threads, 0, st>>>(nullptr, n, R.cs, 0);
+    }
+    NMX_CUDA_TRY(cudaGetLastError());
+    const unsigned cb = (unsigned)ceil_div((int64_t)n * n, threads);
+    if (level == kLvFP64) {
+        NMX_TRY(ctx->ensure_slot(kWsWork64, sizeof(double) * (size_t)n * R.ldw + 256, &p));
+        R.W64 = static_cast<double *>(p);
+        scale_copy_kernel<double><<<cb, threads, 0, st>>>(R.A, R.lda, n, R.rs, R.cs, R.W64, R.ldw);
+        NMX_CUDA_TRY(cudaGetLastError());
+        GemmSub gs;
+        gs.st = st;
+        NMX_TRY(getrf_run<double>(ctx, gs, n, R.W64, R.ldw, R.ipiv, R.info_d, false));
+    } else {
+        NMX_TRY(ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * R.ldw + 256, &p));
+        R.W = static_cast<float *>(p);
+        scale_copy_kernel<float><<<cb, threads, 0, st>>>(R.A, R.lda, n, R.rs, R.cs, R.W, R.ldw);
+        NMX_CUDA_TRY(cudaGetLastError());
+        GemmSub gs;
+        gs.st = st;
+        gs.precision = gemm_precision(level);
+        if (ctx->tune_ir_tc_min >= 0) gs.tc_min = ctx->tune_ir_tc_min;
+        if (gs.precision) {
+            gs.ws_bytes = ir_gemm_ws_bytes(ctx, n, gs.precision);
+            NMX_TRY(ctx->ensure_slot(kWsGemm16, gs.ws_bytes, &gs.ws));
+        }
+        NMX_TRY(getrf_run<float>(ctx, gs, n, R.W, R.ldw, R.ipiv, R.info_d,
+                                 ctx->tune_lu_tournament != 0));
+    }
+    // Inverses of the diagonal blocks of L and U for the triangular solves.
+    const int NB = (n + kTrsvRB - 1) / kTrsvRB;
+    NMX_TRY(ctx->ensure_slot(kWsInv, sizeof(double) * (size_t)NB * kTrsvRB * kTrsvRB * 2 + 256, &p));
+    R.invL = static_cast<double *>(p);
+    R.invU = R.invL + (size_t)NB * kTrsvRB * kTrsvRB;
+    if (level == kLvFP64) {
+        diag_inverse_kernel<double, false><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invL);
+        diag_inverse_kernel<double, true><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invU);
+    } else {
+        diag_inverse_kernel<float, false><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invL);
+        diag_inverse_kernel<float, true><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invU);
+    }
+    NMX_CUDA_TRY(cudaGetLastError());
+    if (done) NMX_CUDA_TRY(cudaEventRecord(done, st));
+    // Pivots -> permutation and its inverse on the host (the interchanges
+    // compose in order).
+    std::vector<int32_t> hp(n), perm(2 * (size_t)n);
+    NMX_CUDA_TRY(cudaMemcpyAsync(hp.data(), R.ipiv, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaMemcpyAsync(hinfo, R.info_d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int j = 0; j < n; ++j)
+        if (hp[j] != j) std::swap(perm[j], perm[hp[j]]);
+    for (int i = 0; i < n; ++i) perm[n + perm[i]] = i;
+    NMX_CUDA_TRY(cudaMemcpyAsync(R.perm, perm.data(), sizeof(int32_t) * 2 * (size_t)n,
+                                 cudaMemcpyHostToDevice, st));
+    // The copy reads pageable host memory: it is staged before the call
+    // returns, so `perm` may go out of scope.
     return 0;
 }
 
-// out = A in (FP64) via the residual kernel with b = 0 (out = -A in).
-static int apply_A(IrRun &R, const double *in, double *out, const double *zero) {
-    const int threads = 256, blocks = (int)ceil_div((int64_t)R.n * 32, threads);
-    residual_kernel<<<blocks, threads, 0, R.st>>>(R.A, R.lda, R.n, in, zero, out, R.norms + 4);
+// One GMRES cycle on M^-1 A d = M^-1 r from d = 0, then x += d.  *steps gets
+// the Arnoldi steps taken, *flag the state's final flag.  `give_up_early`:
+// end a cycle that has not cut its residual tenfold by step kSlowStep (when
+// a more accurate factorization can take over).
+static int gmres_cycle(IrRun &R, double *x, bool give_up_early, int *steps, int *flag) {
+    cudaStream_t st = R.st;
+    const int n = R.n;
+    const int threads = 256;
+    const int wb = (int)ceil_div((int64_t)n * 32, threads);
+    const size_t wsm = sizeof(double) * (size_t)R.rows_per;
+    // z0 = M^-1 r -> V_0, beta, V_0 /= beta.
+    NMX_TRY(precond_apply(R, R.r, R.V));
+    chunk_norm2_kernel<<<R.G, kCgsThreads, 0, st>>>(R.V, n, R.rows_per, R.part);
+    gmres_start_kernel<<<1, 1, 0, st>>>(R.part, R.G, R.gst, 1e-4, give_up_early ? kSlowStep : 0);
+    scale_basis_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, threads), 1024), threads, 0, st>>>(
+        R.V, n, R.gst);
     NMX_CUDA_TRY(cudaGetLastError());
+    int hstate[2] = {0, 0};
+    for (int s = 0; s < kRestart;) {
+        const int chunk = std::min(kGmresChunk, kRestart - s);
+        for (int c = 0; c < chunk; ++c) {
+            gmres_matvec_kernel<<<wb, threads, 0, st>>>(R.A, R.lda, n, R.V, R.gst, R.rs, R.pinv,
+                                                        R.tmp);
+            NMX_TRY(lu_solve_inplace(R, R.tmp, &R.gst->flag, R.w));
+            cgs_dots_kernel<<<R.G, kCgsThreads, wsm, st>>>(R.V, n, R.w, R.rows_per, R.gst, R.part);
+            cgs_reduce_kernel<<<1, kRestart + 1, 0, st>>>(R.part, R.G, R.gst, 0);
+            cgs_update_kernel<<<R.G, kCgsThreads, wsm, st>>>(R.V, n, R.w, R.rows_per, R.gst, R.part,
+                                                             0);
+            cgs_reduce_kernel<<<1, kRestart + 1, 0, st>>>(R.part, R.G, R.gst, 1);
+            cgs_update_kernel<<<R.G, kCgsThreads, wsm, st>>>(R.V, n, R.w, R.rows_per, R.gst, R.part,
+                                                             1);
+            arnoldi_finish_kernel<<<1, 1, 0, st>>>(R.part, R.G, R.gst);
+            scale_basis_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, threads), 1024), threads,
+                                 0, st>>>(R.V, n, R.gst);
+            NMX_CUDA_TRY(cudaGetLastError());
+        }
+        s += chunk;
+        NMX_CUDA_TRY(cudaMemcpyAsync(hstate, R.gst, sizeof hstate, cudaMemcpyDeviceToHost, st));
+        NMX_CUDA_TRY(cudaStreamSynchronize(st));
+        if (hstate[0]) break;
+    }
+    gmres_solve_kernel<<<1, 1, 0, st>>>(R.gst);
+    gmres_update_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, threads), 1024), threads, 0, st>>>(
+        R.V, n, R.gst, x);
+    NMX_CUDA_TRY(cudaGetLastError());
+    *steps = hstate[1];
+    *flag = hstate[0];
+    return 0;
+}
+
+// r = b - A x and the backward error (synchronizes).
+static int ir_residual(IrRun &R, const double *b, const double *x, double normA, double *berr) {
+    cudaStream_t st = R.st;
+    const int n = R.n, threads = 256;
+    const int vb = (int)ceil_div(n, threads);
+    const int wb = (int)ceil_div((int64_t)n * 32, threads);
+    NMX_CUDA_TRY(cudaMemsetAsync(R.norms + 1, 0, 2 * sizeof(unsigned long long), st));
+    residual_kernel<<<wb, threads, 0, st>>>(R.A, R.lda, n, x, b, R.r, R.norms + 1);
+    absmax_kernel<<<std::min(vb, 1024), threads, 0, st>>>(x, n, R.norms + 2);
+    NMX_CUDA_TRY(cudaGetLastError());
+    unsigned long long hn[4];
+    int terr[6] = {0, 0, 0, 0, 0, 0};
+    NMX_CUDA_TRY(cudaMemcpyAsync(hn, R.norms, sizeof hn, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaMemcpyAsync(terr, R.counters, sizeof terr, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+    const double rn = bits_to_double(hn[1]), xn = bits_to_double(hn[2]), bn = bits_to_double(hn[3]);
+    *berr = rn / (normA * xn + bn);
+    if (terr[2] || terr[5]) {
+        set_error("triangular solve: a bounded wait expired");
+        return NMX_ERR_INTERNAL;
+    }
     return 0;
 }
 
@@ -475,12 +987,14 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     NMX_ARG_CHECK(b != nullptr, 5, "b is NULL");
     NMX_ARG_CHECK(x != nullptr, 6, "x is NULL");
     const int prec = mode & 0xF;
-    const bool gmres = (mode & NMX_IR_GMRES) != 0;
-    NMX_ARG_CHECK(prec == NMX_IR_BF16 || prec == NMX_IR_FP16 || prec == NMX_IR_FP32 ||
-                      prec == NMX_IR_BF16X3,
-                  7, "mode must be NMX_IR_BF16/FP16/FP32/BF16X3, optionally | NMX_IR_GMRES");
+    NMX_ARG_CHECK(prec >= NMX_IR_BF16 && prec <= NMX_IR_FP64, 7,
+                  "mode must be NMX_IR_BF16/FP16/FP32/BF16X3/BF16X6/FP64, optionally | "
+                  "NMX_IR_GMRES / NMX_IR_AUTO / NMX_IR_ESCALATE");
     NMX_ARG_CHECK(tol >= 0.0, 8, "tol < 0");
     NMX_ARG_CHECK(max_iter >= 1 && max_iter <= 10000, 9, "max_iter must be in 1..10000");
+    const bool force_gmres = (mode & NMX_IR_GMRES) != 0;
+    const bool auto_gmres = (mode & NMX_IR_AUTO) != 0;
+    const bool escalate = (mode & NMX_IR_ESCALATE) != 0;
     const int n = (int)n64;
     DeviceGuard g(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -490,22 +1004,18 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     R.n = n;
     R.A = A;
     R.lda = lda;
-    int rc = ctx_cublas(ctx, st, &R.h);
-    if (rc) return rc;
-    // Workspace: FP32 factor, vectors, 16-bit GEMM operands.
     R.ldw = (n + 7) / 8 * 8;
-    void *wv = nullptr;
-    rc = ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * R.ldw + 256, &wv);
-    if (rc) return rc;
-    R.W = static_cast<float *>(wv);
-    const int restart = 200;
-    size_t vec_bytes = sizeof(double) * (size_t)n * 8 + sizeof(int) * (size_t)n * 2 + 4096;
-    void *vv = nullptr;
-    rc = ctx->ensure_slot(kWsVec, vec_bytes, &vv);
-    if (rc) return rc;
-    char *vp = static_cast<char *>(vv);
+    R.G = std::max(1, std::min<int>(2 * ctx->sm_count, (int)ceil_div(n, 256)));
+    R.rows_per = (int)ceil_div(n, R.G);
+    R.G = (int)ceil_div(n, R.rows_per);
+    int level = level_of(prec);
+    NMX_TRY(ir_reserve(ctx, n, level, escalate));
+    void *p = nullptr;
+    NMX_TRY(ctx->ensure_slot(kWsVec, ir_vec_bytes(n), &p));
+    char *vp = static_cast<char *>(p);
     R.norms = reinterpret_cast<unsigned long long *>(vp);
     R.counters = reinterpret_cast<int *>(vp + 256);
+    R.info_d = R.counters + 16;
     double *dv = reinterpret_cast<double *>(vp + 1024);
     R.rs = dv;
     R.cs = dv + n;
@@ -513,203 +1023,114 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     R.r = dv + 3 * (size_t)n;
     R.tmp = dv + 4 * (size_t)n;
     R.rowmax = dv + 5 * (size_t)n;
-    double *zero = dv + 6 * (size_t)n;
-    double *aux = dv + 7 * (size_t)n;
-    R.perm = reinterpret_cast<int *>(dv + 8 * (size_t)n);
-    int32_t *ipiv = R.perm + n;
-    int32_t *info_d = reinterpret_cast<int32_t *>(R.counters + 16);
-    GemmSub gs;
-    gs.h = R.h;
-    gs.st = st;
-    gs.precision = prec == NMX_IR_FP32    ? 0
-                   : prec == NMX_IR_FP16   ? NMX_PREC_FP16
-                   : prec == NMX_IR_BF16X3 ? NMX_PREC_BF16X3
-                                           : NMX_PREC_BF16;
-    if (ctx->tune_ir_tc_min >= 0) gs.tc_min = ctx->tune_ir_tc_min;
-    if (gs.precision) {
-        const int64_t half = (n / 2 + 31) / 32 * 32;
-        gs.ws_bytes = tc_gemm_workspace_bytes(n - half, n - half, half, gs.precision) + 4096;
-        rc = ctx->ensure_slot(kWsGemm16, gs.ws_bytes, &gs.ws);
-        if (rc) return rc;
-    }
+    R.w = dv + 6 * (size_t)n;
+    R.perm = reinterpret_cast<int *>(dv + 9 * (size_t)n);
+    R.pinv = R.perm + n;
+    R.ipiv = R.pinv + n;
+    NMX_TRY(ctx->ensure_slot(kWsKrylov, ir_krylov_bytes(n, R.G), &p));
+    R.V = static_cast<double *>(p);
+    R.part = R.V + (size_t)n * (kRestart + 1);
+    R.gst = reinterpret_cast<GmresState *>(R.part + (size_t)R.G * (kRestart + 1));
+    NMX_TRY(ctx->ensure_slot(kWsBest, sizeof(double) * (size_t)n + 256, &p));
+    R.xbest = static_cast<double *>(p);
     const int threads = 256;
     const int vb = (int)ceil_div(n, threads);
-    const int wb = (int)ceil_div((int64_t)n * 32, threads);
+
     cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
+    NMX_CUDA_TRY(cudaEventCreate(&e0));
+    NMX_CUDA_TRY(cudaEventCreate(&e1));
+    NMX_CUDA_TRY(cudaEventCreate(&e2));
+    struct EventsGuard {
+        cudaEvent_t *e;
+        ~EventsGuard() {
+            for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]);
+        }
+    };
+    cudaEvent_t evs[3] = {e0, e1, e2};
+    EventsGuard eg{evs};
     NMX_CUDA_TRY(cudaEventRecord(e0, st));
-    // ||A||_inf, equilibration (power-of-two scalings; FP16 factors need the range).
-    NMX_CUDA_TRY(cudaMemsetAsync(R.norms, 0, 8 * sizeof(unsigned long long), st));
-    NMX_CUDA_TRY(cudaMemsetAsync(zero, 0, sizeof(double) * n, st));
-    row_norms_kernel<<<wb, threads, 0, st>>>(A, lda, n, R.norms, R.rowmax);
-    const int equil = prec == NMX_IR_FP16 ? 1 : 0;
-    row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
-    if (equil) {
-        // The column maxima go through R.tmp's bits (free until the solve).
-        unsigned long long *cmax = reinterpret_cast<unsigned long long *>(R.tmp);
-        NMX_CUDA_TRY(cudaMemsetAsync(cmax, 0, sizeof(double) * n, st));
-        col_max_kernel<<<dim3(vb, kColChunks), threads, 0, st>>>(A, lda, n, R.rs, cmax);
-        col_scale_kernel<<<vb, threads, 0, st>>>(cmax, n, R.cs, 1);
-    } else {
-        col_scale_kernel<<<vb, threads, 0, st>>>(nullptr, n, R.cs, 0);
-    }
-    scale_to_f32_kernel<<<(unsigned)ceil_div((int64_t)n * n, threads), threads, 0, st>>>(
-        A, lda, n, R.rs, R.cs, R.W, R.ldw);
-    NMX_CUDA_TRY(cudaGetLastError());
-    rc = getrf_run<float>(ctx, gs, n, R.W, R.ldw, ipiv, info_d, ctx->tune_lu_tournament != 0);
-    if (rc) return rc;
-    // Inverses of the diagonal blocks of L and U for the triangular solves.
-    {
-        const int NB = (n + kTrsvRB - 1) / kTrsvRB;
-        void *iv = nullptr;
-        rc = ctx->ensure_slot(kWsInv, sizeof(double) * (size_t)NB * kTrsvRB * kTrsvRB * 2 + 256,
-                              &iv);
-        if (rc) return rc;
-        R.invL = static_cast<double *>(iv);
-        R.invU = R.invL + (size_t)NB * kTrsvRB * kTrsvRB;
-        diag_inverse_kernel<false><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invL);
-        diag_inverse_kernel<true><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invU);
-        NMX_CUDA_TRY(cudaGetLastError());
-    }
-    NMX_CUDA_TRY(cudaEventRecord(e1, st));
-    // Pivots -> permutation on the host (the interchanges compose in order).
-    std::vector<int32_t> hp(n), perm(n);
     int32_t hinfo = 0;
-    NMX_CUDA_TRY(cudaMemcpyAsync(hp.data(), ipiv, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
-    NMX_CUDA_TRY(cudaMemcpyAsync(&hinfo, info_d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    unsigned long long hnorm[8];
-    NMX_CUDA_TRY(cudaMemcpyAsync(hnorm, R.norms, sizeof hnorm, cudaMemcpyDeviceToHost, st));
-    NMX_CUDA_TRY(cudaStreamSynchronize(st));
-    for (int i = 0; i < n; ++i) perm[i] = i;
-    for (int j = 0; j < n; ++j)
-        if (hp[j] != j) std::swap(perm[j], perm[hp[j]]);
-    NMX_CUDA_TRY(cudaMemcpyAsync(R.perm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    const double normA = bits_to_double(hnorm[0]);
-    // ||b||_inf
+    NMX_TRY(ir_factor(R, level, &hinfo, e1));
+    unsigned long long hnorm0 = 0;
+    NMX_CUDA_TRY(cudaMemcpyAsync(&hnorm0, R.norms, sizeof hnorm0, cudaMemcpyDeviceToHost, st));
+    // ||b||_inf; x = 0, r = b.
+    NMX_CUDA_TRY(cudaMemsetAsync(R.norms + 3, 0, sizeof(unsigned long long), st));
     absmax_kernel<<<std::min(vb, 1024), threads, 0, st>>>(b, n, R.norms + 3);
-    // x = 0, r = b
     NMX_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    NMX_CUDA_TRY(cudaMemsetAsync(R.xbest, 0, sizeof(double) * n, st));
     NMX_CUDA_TRY(cudaMemcpyAsync(R.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    int it = 0, inner_total = 0;
-    double berr = INFINITY, prev = INFINITY, best_berr = INFINITY;
-    int stalled = 0;
-    bool use_gmres = gmres;
-    std::vector<double> H((size_t)(restart + 1) * restart), cs_g(restart), sn_g(restart),
-        gvec(restart + 1), y(restart);
-    void *kv = nullptr;
+    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+    const double normA = bits_to_double(hnorm0);
+
+    double factor_extra_ms = 0.0;  // refactorizations after an escalation
+    int it = 0, inner_total = 0, since_best = 0, level_steps = 0;
+    double berr = INFINITY, prev = INFINITY, best = INFINITY;
+    bool use_gmres = force_gmres, used_gmres = false;
     for (it = 1; it <= max_iter; ++it) {
+        int gflag = 0;
         if (!use_gmres) {
-            rc = precond_apply(R, R.r, R.v);  // d = M^-1 r
-            if (rc) return rc;
+            NMX_TRY(precond_apply(R, R.r, R.v));  // d = M^-1 r
             add_kernel<<<vb, threads, 0, st>>>(R.v, n, x);
             NMX_CUDA_TRY(cudaGetLastError());
         } else {
-            // Restarted GMRES on M^-1 A d = M^-1 r, M^-1 = C U^-1 L^-1 P R.
-            rc = ctx->ensure_slot(kWsKrylov, sizeof(double) * ((size_t)n * (restart + 1) + 2 * 64), &kv);
-            if (rc) return rc;
-            double *Vk = static_cast<double *>(kv);
-            double *hdev = Vk + (size_t)n * (restart + 1);
-            std::vector<double> hh(restart + 1);
-            rc = precond_apply(R, R.r, Vk);  // z0 = M^-1 r
-            if (rc) return rc;
-            double beta = 0.0;
-            NMX_CUBLAS_TRY(cublasDnrm2(R.h, n, Vk, 1, &beta));
-            NMX_CUDA_TRY(cudaStreamSynchronize(st));
-            if (!(beta > 0.0)) break;
-            const double inv = 1.0 / beta;
-            NMX_CUBLAS_TRY(cublasDscal(R.h, n, &inv, Vk, 1));
-            std::fill(gvec.begin(), gvec.end(), 0.0);
-            gvec[0] = beta;
-            int k = 0;
-            for (; k < restart; ++k) {
-                double *vk = Vk + (size_t)k * n, *w = Vk + (size_t)(k + 1) * n;
-                rc = apply_A(R, vk, aux, zero);  // aux = -A vk
-                if (rc) return rc;
-                const double minus = -1.0;
-                NMX_CUBLAS_TRY(cublasDscal(R.h, n, &minus, aux, 1));
-                rc = precond_apply(R, aux, w);
-                if (rc) return rc;
-                // Classical Gram-Schmidt, twice (CGS2): h = V^T w, w -= V h.
-                const double one = 1.0, zero_d = 0.0, mone = -1.0;
-                for (int pass = 0; pass < 2; ++pass) {
-                    NMX_CUBLAS_TRY(cublasDgemv(R.h, CUBLAS_OP_T, n, k + 1, &one, Vk, n, w, 1,
-                                               &zero_d, hdev, 1));
-                    NMX_CUBLAS_TRY(cublasDgemv(R.h, CUBLAS_OP_N, n, k + 1, &mone, Vk, n, hdev, 1,
-                                               &one, w, 1));
-                    NMX_CUDA_TRY(cudaMemcpyAsync(hh.data(), hdev, sizeof(double) * (k + 1),
-                                                 cudaMemcpyDeviceToHost, st));
-                    NMX_CUDA_TRY(cudaStreamSynchronize(st));
-                    for (int j = 0; j <= k; ++j)
-                        H[(size_t)j * restart + k] = (pass == 0 ? 0.0 : H[(size_t)j * restart + k]) + hh[j];
-                }
-                double hn = 0.0;
-                NMX_CUBLAS_TRY(cublasDnrm2(R.h, n, w, 1, &hn));
-                NMX_CUDA_TRY(cudaStreamSynchronize(st));
-                H[(size_t)(k + 1) * restart + k] = hn;
-                if (hn > 0.0) {
-                    const double ih = 1.0 / hn;
-                    NMX_CUBLAS_TRY(cublasDscal(R.h, n, &ih, w, 1));
-                }
-                // Givens rotations on column k of H.
-                for (int j = 0; j < k; ++j) {
-                    const double a = H[(size_t)j * restart + k], bb = H[(size_t)(j + 1) * restart + k];
-                    H[(size_t)j * restart + k] = cs_g[j] * a + sn_g[j] * bb;
-                    H[(size_t)(j + 1) * restart + k] = -sn_g[j] * a + cs_g[j] * bb;
-                }
-                const double a = H[(size_t)k * restart + k], bb = H[(size_t)(k + 1) * restart + k];
-                const double rr = std::hypot(a, bb);
-                cs_g[k] = rr > 0 ? a / rr : 1.0;
-                sn_g[k] = rr > 0 ? bb / rr : 0.0;
-                H[(size_t)k * restart + k] = rr;
-                H[(size_t)(k + 1) * restart + k] = 0.0;
-                gvec[k + 1] = -sn_g[k] * gvec[k];
-                gvec[k] = cs_g[k] * gvec[k];
-                ++inner_total;
-                // Inner tolerance: each GMRES solve only has to shrink the
-                // correction's residual by 1e-4; the FP64 outer loop does the rest.
-                if (std::fabs(gvec[k + 1]) <= 1e-4 * beta || hn == 0.0) {
-                    ++k;
-                    break;
-                }
-            }
-            // y = H^-1 g (upper triangular k x k), d = V y, x += d.
-            for (int i = k - 1; i >= 0; --i) {
-                double s = gvec[i];
-                for (int j = i + 1; j < k; ++j) s -= H[(size_t)i * restart + j] * y[j];
-                y[i] = s / H[(size_t)i * restart + i];
-            }
-            for (int j = 0; j < k; ++j)
-                NMX_CUBLAS_TRY(cublasDaxpy(R.h, n, &y[j], Vk + (size_t)j * n, 1, x, 1));
+            int steps = 0;
+            NMX_TRY(gmres_cycle(R, x, escalate && R.level != kLvFP64, &steps, &gflag));
+            inner_total += steps;
+            used_gmres = true;
         }
-        // r = b - A x; norms.
-        NMX_CUDA_TRY(cudaMemsetAsync(R.norms + 1, 0, 2 * sizeof(unsigned long long), st));
-        residual_kernel<<<wb, threads, 0, st>>>(A, lda, n, x, b, R.r, R.norms + 1);
-        absmax_kernel<<<std::min(vb, 1024), threads, 0, st>>>(x, n, R.norms + 2);
-        NMX_CUDA_TRY(cudaGetLastError());
-        NMX_CUDA_TRY(cudaMemcpyAsync(hnorm, R.norms, sizeof hnorm, cudaMemcpyDeviceToHost, st));
-        NMX_CUDA_TRY(cudaStreamSynchronize(st));
-        const double rn = bits_to_double(hnorm[1]), xn = bits_to_double(hnorm[2]),
-                     bn = bits_to_double(hnorm[3]);
-        berr = rn / (normA * xn + bn);
-        int terr[6] = {0, 0, 0, 0, 0, 0};
-        NMX_CUDA_TRY(cudaMemcpy(terr, R.counters, sizeof terr, cudaMemcpyDeviceToHost));
-        if (terr[2] || terr[5]) {
-            set_error("triangular solve: a bounded wait expired");
-            return NMX_ERR_INTERNAL;
-        }
-        if (berr <= tol || !std::isfinite(berr)) break;
-        // Plain refinement that stops contracting hands over to GMRES-IR when allowed.
-        if (!use_gmres && (mode & NMX_IR_AUTO) && berr > 0.5 * prev) use_gmres = true;
-        // Give up after 8 steps in a row without halving the backward error.
-        if (berr > 0.5 * best_berr) {
-            if (++stalled >= 8) break;
+        ++level_steps;
+        NMX_TRY(ir_residual(R, b, x, normA, &berr));
+        if (berr < best) {
+            if (best < INFINITY && berr > 0.5 * best)
+                ++since_best;  // an improvement, but not a halving
+            else
+                since_best = 0;
+            best = berr;
+            NMX_CUDA_TRY(cudaMemcpyAsync(R.xbest, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         } else {
-            stalled = 0;
-            best_berr = berr;
+            ++since_best;
         }
+        if (best <= tol) break;
+        // Does this precision still contract?  Plain refinement: the backward
+        // error must halve per step; a GMRES cycle must reach its own
+        // tolerance (or at least cut the backward error tenfold).
+        bool stuck;
+        if (!use_gmres)
+            stuck = level_steps >= 2 && berr > 0.5 * prev;
+        else
+            stuck = (gflag == 4 || gflag == 3) ? berr > 0.1 * prev : berr > 0.5 * prev;
+        stuck = stuck || !std::isfinite(berr);
         prev = berr;
+        if (!stuck) continue;
+        if (!use_gmres && (auto_gmres || force_gmres)) {
+            use_gmres = true;  // hand over to GMRES-IR at the same precision
+        } else if (escalate && R.level != kLvFP64) {
+            // Refactor one level up and refine on from the best iterate.
+            cudaEvent_t f0, f1;
+            NMX_CUDA_TRY(cudaEventCreate(&f0));
+            NMX_CUDA_TRY(cudaEventCreate(&f1));
+            NMX_CUDA_TRY(cudaEventRecord(f0, st));
+            int rc = ir_factor(R, next_level(R.level), &hinfo, f1);
+            if (!rc) rc = cudaEventSynchronize(f1) == cudaSuccess ? 0 : NMX_ERR_CUDA;
+            float ms = 0.f;
+            if (!rc) cudaEventElapsedTime(&ms, f0, f1);
+            cudaEventDestroy(f0);
+            cudaEventDestroy(f1);
+            if (rc) return rc;
+            factor_extra_ms += ms;
+            NMX_CUDA_TRY(cudaMemcpyAsync(x, R.xbest, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            NMX_TRY(ir_residual(R, b, x, normA, &berr));
+            prev = berr;
+            use_gmres = force_gmres;
+            level_steps = 0;
+            since_best = 0;
+        } else if (since_best >= 8) {
+            break;  // no precision left to try and no progress
+        }
+    }
+    // The best iterate is the result.
+    if (!(berr <= best)) {
+        NMX_CUDA_TRY(cudaMemcpyAsync(x, R.xbest, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     }
     NMX_CUDA_TRY(cudaEventRecord(e2, st));
     NMX_CUDA_TRY(cudaEventSynchronize(e2));
@@ -719,17 +1140,14 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
         cudaEventElapsedTime(&r_ms, e1, e2);
         stats->iterations = std::min(it, max_iter);
         stats->gmres_iterations = inner_total;
-        stats->converged = berr <= tol ? 1 : 0;
+        stats->converged = best <= tol ? 1 : 0;
         stats->info = hinfo;
-        stats->backward_error = berr;
-        stats->factor_ms = f_ms;
-        stats->refine_ms = r_ms;
-        stats->used_gmres = use_gmres ? 1 : 0;
-        stats->reserved = 0;
+        stats->backward_error = best;
+        stats->factor_ms = f_ms + factor_extra_ms;
+        stats->refine_ms = r_ms - factor_extra_ms;
+        stats->used_gmres = used_gmres ? 1 : 0;
+        stats->final_precision = prec_of(R.level);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
     return 0;
 }
 
@@ -739,4 +1157,14 @@ extern "C" NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, 
                                        const double *b, double *x, int mode, double tol,
                                        int max_iter, nmx_ir_stats *stats, void *stream) {
     return nmx::gesv_ir(ctx, n, A, lda, b, x, mode, tol, max_iter, stats, stream);
+}
+
+extern "C" NMX_API int nmx_gesv_ir_reserve(nmx_ctx ctx, int64_t n, int mode) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(n >= 1 && n <= (1 << 17), 2, "n must be in 1..131072");
+    const int prec = mode & 0xF;
+    NMX_ARG_CHECK(prec >= NMX_IR_BF16 && prec <= NMX_IR_FP64, 3,
+                  "mode must be NMX_IR_BF16/FP16/FP32/BF16X3/BF16X6/FP64 with optional flags");
+    nmx::DeviceGuard g(ctx->device);
+    return nmx::ir_reserve(ctx, n, nmx::level_of(prec), (mode & NMX_IR_ESCALATE) != 0);
 }

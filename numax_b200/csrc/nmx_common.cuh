@@ -62,8 +62,6 @@ struct nmx_context {
     size_t smem_optin = 0;
     void *workspace = nullptr;
     size_t workspace_bytes = 0;
-    void *cublas = nullptr;  // cublasHandle_t, created on first dense call
-    void *cublas_aux = nullptr;  // a second handle, for the look-ahead LU's panel stream
     // The look-ahead LU's panel (high priority) and update streams and the
     // events that order them, created on first use.
     cudaStream_t la_stream[2] = {};
@@ -78,7 +76,7 @@ struct nmx_context {
     int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the LU (-1: 256, 0: off)
     int64_t tune_lu_panel_sms = -1;   // SMs the look-ahead keeps free of the update GEMMs (-1, 0: none)
     // Grow-only named device buffers, one per use, kept for the context's life.
-    static constexpr int kSlots = 8;
+    static constexpr int kSlots = 10;
     void *slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Returns a device buffer of at least `bytes`, reusing the context's.
@@ -88,7 +86,18 @@ struct nmx_context {
 };
 
 namespace nmx {
-enum WsSlot { kWsLeaf = 0, kWsGemm16 = 1, kWsWork = 2, kWsVec = 3, kWsKrylov = 4, kWsInv = 5, kWsCalu = 6, kWsGemm16Panel = 7 };
+enum WsSlot {
+    kWsLeaf = 0,
+    kWsGemm16 = 1,
+    kWsWork = 2,
+    kWsVec = 3,
+    kWsKrylov = 4,
+    kWsInv = 5,
+    kWsCalu = 6,
+    kWsGemm16Panel = 7,
+    kWsWork64 = 8,  // FP64 factors of the refinement's last precision level
+    kWsBest = 9     // the refinement's best iterate
+};
 }
 
 namespace nmx {

@@ -209,18 +209,22 @@ def qr_factor(a) -> QR:
     return QR(f, tau)
 
 
-_IR_MODES = {"bf16": _lib.NMX_IR_BF16, "fp16": _lib.NMX_IR_FP16, "fp32": _lib.NMX_IR_FP32,
-             "bf16x3": _lib.NMX_IR_BF16X3}
+_IR_MODES = {name: code for code, name in _lib.IR_PRECISION_NAMES.items()}
 
 
 def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: float = 1e-14,
-             max_iter: int = 50):
+             max_iter: int = 50, escalate: bool = False):
     """x with a x = b for float64 a, b: low-precision LU (BF16/FP16 tensor-core
-    trailing updates, or FP32) refined in FP64 to backward error <= tol, with
-    GMRES-IR when `gmres` is True (or "auto": when plain refinement stalls).
+    trailing updates, BF16 splits with ~16 ("bf16x3") or 24 ("bf16x6") bits,
+    FP32, or FP64) refined in FP64 to backward error <= tol, with GMRES-IR
+    when `gmres` is True (or "auto": when plain refinement stalls); with
+    `escalate`, a precision whose refinement cannot converge is replaced by
+    the next more accurate one.  x is the iterate with the smallest backward
+    error.
 
     Returns (x, stats) with stats a dict: iterations, gmres_iterations,
-    converged, info, used_gmres, backward_error, factor_ms, refine_ms."""
+    converged, info, used_gmres, final_precision (name), backward_error,
+    factor_ms, refine_ms."""
     _check_matrix("a", a)
     if a.dtype != torch.float64:
         raise TypeError("solve_ir needs float64 a and b")
@@ -234,9 +238,12 @@ def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: flo
         mode |= _lib.NMX_IR_GMRES
     elif gmres == "auto":
         mode |= _lib.NMX_IR_AUTO
+    if escalate:
+        mode |= _lib.NMX_IR_ESCALATE
     st = _lib.IrStats()
     import ctypes as _C
     _lib.call("nmx_gesv_ir_f64", _ctx(dev), n, A.data_ptr(), A.stride(0), bb.data_ptr(),
               x.data_ptr(), mode, float(tol), int(max_iter), _C.byref(st), _stream(dev))
-    stats = {f: getattr(st, f) for f, _ in _lib.IrStats._fields_ if f != "reserved"}
+    stats = {f: getattr(st, f) for f, _ in _lib.IrStats._fields_}
+    stats["final_precision"] = _lib.IR_PRECISION_NAMES.get(st.final_precision, "?")
     return x.reshape(b.shape), stats

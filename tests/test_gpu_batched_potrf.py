@@ -164,3 +164,51 @@ def test_batched_autotune_and_graph_replay(oracle):
     plan.run(dA, dB, Xh, info, Lg, graph=True)
     torch.cuda.synchronize()
     assert torch.equal(Xh, X1)
+
+
+def test_batched_f32_full_config_vs_oracle_sample(oracle):
+    """float32 at the BASELINE size: 100,000 SPD matrices, n ~ U[8, 128],
+    4 right-hand sides, in one plan; every 50th matrix against the oracle
+    (numax's Array-tier cholesky + cholesky_solve) within 1e-5."""
+    import numax_b200 as nb
+    rng = np.random.Generator(np.random.PCG64(100000))
+    ns = rng.integers(8, 129, size=100_000).astype(np.int32)
+    nrhs = 4
+    sample = np.arange(0, len(ns), 50)
+    # Data on the GPU (per size group), the sample copied back for the oracle.
+    a_off = oracle.ragged_offsets(ns)
+    b_off = oracle.ragged_offsets(ns, nrhs)
+    total_a = int((ns.astype(np.int64) ** 2).sum())
+    A = torch.empty(total_a, dtype=torch.float32, device="cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    ns_t = torch.from_numpy(ns).cuda()
+    a_off_t = torch.from_numpy(a_off).cuda()
+    for n in np.unique(ns):
+        idx = torch.nonzero(ns_t == int(n)).flatten()
+        g = torch.randn((idx.numel(), int(n), int(n)), generator=gen, dtype=torch.float64,
+                        device="cuda")
+        m = g @ g.transpose(1, 2) / n + n * torch.eye(int(n), dtype=torch.float64, device="cuda")
+        pos = a_off_t[idx][:, None] + torch.arange(int(n) * int(n), device="cuda")[None, :]
+        A[pos.flatten()] = m.reshape(-1).float()
+    B = torch.randn(int(ns.astype(np.int64).sum()) * nrhs, generator=gen, dtype=torch.float32,
+                    device="cuda")
+    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float32)
+    L, X, info = plan(A.clone(), B)
+    assert int(info.abs().sum()) == 0
+    hA, hB, hL, hX = A.cpu().numpy(), B.cpu().numpy(), L.cpu().numpy(), X.cpu().numpy()
+    sub_ns = ns[sample]
+    sa = np.concatenate([hA[a_off[i]:a_off[i] + ns[i] ** 2] for i in sample])
+    sb = np.concatenate([hB[b_off[i]:b_off[i] + ns[i] * nrhs] for i in sample])
+    wantL, wantX = oracle.batched_cholesky_solve(sub_ns, sa, sb, nrhs)
+    so, sbo = oracle.ragged_offsets(sub_ns), oracle.ragged_offsets(sub_ns, nrhs)
+    worst_l = worst_x = 0.0
+    for j, i in enumerate(sample):
+        n = int(ns[i])
+        gl = np.tril(hL[a_off[i]:a_off[i] + n * n].reshape(n, n))
+        wl = np.tril(wantL[so[j]:so[j] + n * n].reshape(n, n))
+        worst_l = max(worst_l, relerr(gl, wl))
+        worst_x = max(worst_x, relerr(hX[b_off[i]:b_off[i] + n * nrhs],
+                                      wantX[sbo[j]:sbo[j] + n * nrhs]))
+    assert worst_l <= 1e-5, worst_l
+    assert worst_x <= 1e-5, worst_x

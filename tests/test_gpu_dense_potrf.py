@@ -73,3 +73,19 @@ def test_cholesky_reads_only_lower_and_reports_numax_errors():
         linalg.cholesky(torch.from_numpy(nx["not_spd_2x2"]).cuda())
     with pytest.raises(ValueError, match="index 3"):
         linalg.cholesky(torch.from_numpy(nx["later_block"]).cuda())
+
+
+def test_cholesky_config_order_8192_matches_lapack():
+    """FP64 Cholesky at a BASELINE order (SPD G G^T / n + I, n = 8192) against
+    LAPACK's factor, and the 16-right-hand-side cholesky_solve, within 1e-12."""
+    import scipy.linalg as sl
+    from numax_b200 import linalg
+    n = 8192
+    a = spd(n, 8192)
+    L = linalg.cholesky(torch.from_numpy(a).cuda())
+    want = np.linalg.cholesky(a)
+    assert rel(L.cpu().numpy(), want) <= 1e-12
+    rng = np.random.Generator(np.random.PCG64(3))
+    bm = rng.standard_normal((n, 16))
+    x = linalg.cholesky_solve(L, torch.from_numpy(bm).cuda()).cpu().numpy()
+    assert rel(x, sl.cho_solve((want, True), bm)) <= 1e-12

@@ -53,3 +53,21 @@ def test_qr_zero_column_keeps_tau_zero(oracle):
     want, tau = oracle.qr_factor(a, block=16)
     np.testing.assert_allclose(f.taus.cpu().numpy(), tau, atol=1e-15)
     assert rel(f.factored.cpu().numpy(), want) <= 1e-12
+
+
+def test_qr_config_262144x256_f32_vs_lapack():
+    """The BASELINE tall-skinny QR (262144 x 256, float32 Gaussian) against
+    LAPACK's packed geqrf of the same data in float64: R/V and tau within
+    1e-5 normwise, the thin Q orthogonal to 1e-5."""
+    import scipy.linalg as sl
+    from numax_b200 import linalg
+    m, n = 262144, 256
+    rng = np.random.Generator(np.random.PCG64(262144))
+    a = rng.standard_normal((m, n)).astype(np.float32)
+    f = linalg.qr_factor(torch.from_numpy(a).cuda())
+    (packed, tau), _ = sl.qr(a.astype(np.float64), mode="raw")
+    assert rel(f.factored.cpu().numpy().astype(np.float64), np.ascontiguousarray(packed)) <= 1e-5
+    assert rel(f.taus.cpu().numpy().astype(np.float64), tau) <= 1e-5
+    q = f.q().double()
+    eye = torch.eye(n, dtype=torch.float64, device="cuda")
+    assert float((q.T @ q - eye).abs().max()) <= 1e-5

@@ -30,24 +30,100 @@ def berr(a, x, b):
 
 # Converging cases: 16-bit factors with plain/auto refinement at kappa 1e2,
 # FP16 factors with GMRES-IR at 1e5, FP32 factors through 1e8, split-BF16
-# (bf16x3) updates through 1e5.  Single-BF16 factors at kappa >= 1e5 are
-# reported by the benchmark, not asserted here.
-@pytest.mark.parametrize("precision,gmres,kappa", [
-    ("bf16", "auto", 1e2), ("fp16", "auto", 1e2), ("fp16", True, 1e5),
-    ("fp32", "auto", 1e5), ("fp32", True, 1e8), ("bf16x3", "auto", 1e2), ("bf16x3", "auto", 1e5),
+# updates (bf16x3 through 1e5, bf16x6 through 1e8), and single-BF16 factors
+# at 1e8 when escalation may move to more accurate factors.
+@pytest.mark.parametrize("precision,gmres,kappa,escalate", [
+    ("bf16", "auto", 1e2, False), ("fp16", "auto", 1e2, False), ("fp16", True, 1e5, False),
+    ("fp32", "auto", 1e5, False), ("fp32", True, 1e8, False), ("bf16x3", "auto", 1e2, False),
+    ("bf16x3", "auto", 1e5, False), ("bf16x6", "auto", 1e5, False), ("bf16x6", True, 1e8, False),
+    ("bf16", False, 1e8, True), ("fp64", False, 1e8, False),
 ])
-def test_ir_reaches_fp64_backward_error(precision, gmres, kappa):
+def test_ir_reaches_fp64_backward_error(precision, gmres, kappa, escalate):
     from numax_b200 import linalg
     n = 1000
     a, b, xt = make_system(n, kappa, seed=int(np.log10(kappa)))
     x, st = linalg.solve_ir(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
-                            precision=precision, gmres=gmres, tol=1e-14, max_iter=60)
+                            precision=precision, gmres=gmres, tol=1e-14, max_iter=60,
+                            escalate=escalate)
     x = x.cpu().numpy()
     assert st["converged"] == 1, st
     assert berr(a, x, b) <= 1e-14, (berr(a, x, b), st)
     xr = np.linalg.solve(a, b)
     fe = np.abs(x - xr).max() / np.abs(xr).max()
     assert fe <= kappa * 1e-13, fe
+    if not escalate:
+        assert st["final_precision"] == precision
+
+
+def _haar_gpu(n, gen):
+    g = torch.randn((n, n), generator=gen, dtype=torch.float64, device="cuda")
+    q, r = torch.linalg.qr(g)
+    return q * torch.sign(torch.diagonal(r))[None, :]
+
+
+@pytest.fixture(scope="module")
+def system_8192():
+    """A = U diag(s) V^T at n = 8192 (Haar U, V on the GPU), per kappa."""
+    n = 8192
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(8192)
+    u, v = _haar_gpu(n, gen), _haar_gpu(n, gen)
+    xt = torch.randn(n, generator=gen, dtype=torch.float64, device="cuda")
+    cache = {}
+
+    def get(kappa):
+        if kappa not in cache:
+            s = torch.logspace(0.0, -np.log10(kappa), n, dtype=torch.float64, device="cuda")
+            a = (u * s[None, :]) @ v.T
+            cache.clear()
+            cache[kappa] = (a, a @ xt)
+        return cache[kappa]
+    return get
+
+
+def _berr_gpu(a, x, b):
+    r = b - a @ x
+    return float(r.abs().max() / (a.abs().sum(1).max() * x.abs().max() + b.abs().max()))
+
+
+# The BASELINE conditioning range at n = 8192: every case must end at FP64
+# backward error; with escalation the solver may move to more accurate
+# factors, and reports which it finished with.
+@pytest.mark.parametrize("kappa,precision,gmres,escalate", [
+    (1e2, "bf16x3", "auto", False), (1e2, "fp16", "auto", False), (1e2, "bf16", "auto", True),
+    (1e5, "bf16x6", "auto", False), (1e5, "bf16x3", "auto", True),
+    (1e8, "bf16x6", "auto", True), (1e8, "fp16", "auto", True),
+])
+def test_ir_8192_across_conditioning(system_8192, kappa, precision, gmres, escalate):
+    from numax_b200 import linalg
+    a, b = system_8192(kappa)
+    x, st = linalg.solve_ir(a, b, precision=precision, gmres=gmres, tol=1e-14, max_iter=80,
+                            escalate=escalate)
+    assert st["converged"] == 1, st
+    be = _berr_gpu(a, x, b)
+    assert be <= 1e-14, (be, st)
+    # Against the FP64 LU solve of the same system (cuSOLVER, for data only).
+    xr = torch.linalg.solve(a, b)
+    fe = float((x - xr).abs().max() / xr.abs().max())
+    assert fe <= kappa * 1e-12, (fe, st)
+
+
+def test_ir_returns_its_best_iterate():
+    """Single-BF16 factors at kappa 1e8 without escalation cannot converge:
+    the solver stops and returns the iterate whose backward error it reports
+    (never a later, worse one)."""
+    from numax_b200 import linalg
+    n = 1000
+    a, b, _ = make_system(n, 1e8, seed=8)
+    x, st = linalg.solve_ir(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
+                            precision="bf16", gmres=False, tol=1e-14, max_iter=12)
+    x = x.cpu().numpy()
+    assert st["converged"] == 0
+    assert np.all(np.isfinite(x))
+    got = berr(a, x, b)
+    assert got <= 1.0001 * st["backward_error"] + 1e-300, (got, st)
+    # It is no worse than x = 0 (backward error 1).
+    assert got < 1.0
 
 
 def test_ir_rejects_bad_arguments():
@@ -58,3 +134,6 @@ def test_ir_rejects_bad_arguments():
     a = torch.eye(4, dtype=torch.float64, device="cuda")
     assert lib.nmx_gesv_ir_f64(ctx, 4, a.data_ptr(), 4, a.data_ptr(), a.data_ptr(), 9, 1e-14, 10,
                                None, None) == -7
+    assert lib.nmx_gesv_ir_reserve(ctx, 0, 1) == -2
+    assert lib.nmx_gesv_ir_reserve(ctx, 64, 0) == -3
+    assert lib.nmx_gesv_ir_reserve(ctx, 64, 1 | 0x40) == 0
