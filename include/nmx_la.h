@@ -125,8 +125,9 @@ NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, cons
                                         void *stream);
 
 /* Autotuner (no numax counterpart; numax launches one problem per thread at
- * a compile-time n): times every CTA shape (64, 96, 128, 192 threads) that
- * covers each size bucket of the plan on these buffers -- the bucket's
+ * a compile-time n): times every CTA shape (64, 96, 128, 192 threads of the
+ * packed-triangle kernel, and for FP64 the 256-thread kernel on 8 x 8 DMMA
+ * tiles) that covers each size bucket of the plan on these buffers -- the bucket's
  * persistent kernel alone, best of `reps` runs, CUDA events -- and keeps the
  * fastest in the plan.  Every run computes the whole bucket, so L, X and
  * info hold a valid result afterwards.  A and B as for the run entry points
@@ -138,6 +139,12 @@ NMX_API int nmx_batched_plan_autotune(nmx_ctx ctx, nmx_batched_plan plan, const 
  * per CTA and CTAs launched; up to max_buckets entries, *nbuckets = count. */
 NMX_API int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *threads,
                                       int32_t *ctas, int max_buckets, int32_t *nbuckets);
+/* Set the CTA shape of one size bucket (bucket >= 0) or of all (-1) by hand,
+ * in place of the default or the autotuner's pick (no numax counterpart):
+ * threads 64, 96, 128 or 192 select the packed-triangle kernel, 256 the FP64
+ * kernel on 8 x 8 DMMA tiles.  Rejects a shape that cannot cover a bucket. */
+NMX_API int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket,
+                                       int threads);
 /* Run the plan through a CUDA graph (no numax counterpart): the first call
  * with a given set of buffers captures the plan's launches (counter reset +
  * one persistent kernel per bucket) on an internal stream into a graph kept

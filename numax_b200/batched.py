@@ -146,6 +146,13 @@ class CholeskySolveBatch:
                   int(reps), _stream_ptr(self.device))
         return self.schedule()
 
+    def force_shape(self, threads: int, bucket: int = -1):
+        """Fix the CTA shape of one size bucket (or all, bucket = -1): 64, 96,
+        128 or 192 threads (packed-triangle kernel) or 256 (the FP64 kernel on
+        8 x 8 DMMA tiles).  Returns the schedule."""
+        _lib.call("nmx_batched_plan_set_shape", self._ctx, self._plan, int(bucket), int(threads))
+        return self.schedule()
+
     def schedule(self):
         """Per size bucket (largest n first): n_max, threads per CTA, CTAs."""
         nmax, thr, ctas = (C.c_int32 * 8)(), (C.c_int32 * 8)(), (C.c_int32 * 8)()

@@ -705,6 +705,8 @@ __global__ void __launch_bounds__(NT, potrf_min_blocks(NT))
 
 }  // namespace nmx
 
+#include "batched_potrf_tile.cuh"
+
 // ---- plan -------------------------------------------------------------------
 
 struct nmx_batched_plan_s {
@@ -734,6 +736,17 @@ static int potrf_threads_for(int nmax) {
     return nmax <= 32 ? 64 : (nmax <= 96 ? 128 : kPotrfBigThreads);
 }
 
+// CTA shape 256 selects the 8 x 8 DMMA tile kernel (FP64 only,
+// batched_potrf_tile.cuh); the others are potrf_potrs_batched_kernel's.
+constexpr int kTileShape = kTileNW * 32;
+
+// Dynamic shared memory of a CTA shape for a bucket of matrices up to nmax.
+template <typename T>
+static size_t shape_smem(int threads, int nmax, int nrhs) {
+    if (threads == kTileShape) return sizeof(double) * (size_t)tile_smem_doubles(nmax);
+    return sizeof(T) * (size_t)potrf_smem_elems(nmax, nrhs);
+}
+
 template <typename T>
 static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s::Bucket &b,
                          int *counter, cudaStream_t st) {
@@ -748,6 +761,14 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
         NMX_CASE(128)
         NMX_CASE(192)
 #undef NMX_CASE
+        case kTileShape:
+            if constexpr (sizeof(T) == 8) {
+                potrf_tile_batched_kernel<16><<<b.grid, kTileShape, b.smem, st>>>(args, b.begin, b.end,
+                                                                              b.nmax, counter);
+                break;
+            }
+            set_error("the tile shape is FP64 only");
+            return NMX_ERR_INTERNAL;
         default:
             set_error("unsupported thread count %d", b.threads);
             return NMX_ERR_INTERNAL;
@@ -791,6 +812,13 @@ static int shape_occupancy(nmx_ctx ctx, int threads, size_t smem, int *per_sm) {
         NMX_OCC(128)
         NMX_OCC(192)
 #undef NMX_OCC
+        case kTileShape:
+            if constexpr (sizeof(T) == 8) {
+                NMX_CUDA_TRY(set_max_dynamic_smem(potrf_tile_batched_kernel<16>, ctx));
+                NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    per_sm, potrf_tile_batched_kernel<16>, kTileShape, smem));
+            }
+            break;
         default:
             break;
     }
@@ -870,10 +898,15 @@ static int autotune(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const 
     for (size_t bi = 0; bi < plan->buckets.size() && !rc; ++bi) {
         auto best = plan->buckets[bi];
         float best_ms = 3.4e38f;
-        for (int threads : {64, 96, 128, 192}) {
+        for (int threads : {64, 96, 128, 192, kTileShape}) {
             auto cand = plan->buckets[bi];
-            if (!shape_covers(threads, cand.nmax, plan->nrhs)) continue;
+            if (threads == kTileShape) {
+                if (sizeof(T) != 8) continue;
+            } else if (!shape_covers(threads, cand.nmax, plan->nrhs)) {
+                continue;
+            }
             cand.threads = threads;
+            cand.smem = shape_smem<T>(threads, cand.nmax, plan->nrhs);
             int per_sm = 0;
             rc = shape_occupancy<T>(ctx, threads, cand.smem, &per_sm);
             if (rc) break;
@@ -1099,6 +1132,44 @@ int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *thr
         if (ctas) ctas[i] = plan->buckets[i].grid;
     }
     if (nbuckets) *nbuckets = nb;
+    return 0;
+}
+
+int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket, int threads) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    NMX_ARG_CHECK(bucket >= -1 && bucket < (int)plan->buckets.size(), 3,
+                  "bucket must be -1 (all) or a bucket index");
+    NMX_ARG_CHECK(threads == 64 || threads == 96 || threads == 128 || threads == 192 ||
+                      threads == kTileShape,
+                  4, "threads must be 64, 96, 128, 192 or 256 (the FP64 tile kernel)");
+    NMX_ARG_CHECK(threads != kTileShape || plan->dtype == NMX_F64, 4,
+                  "the 256-thread tile kernel is FP64 only");
+    DeviceGuard g(ctx->device);
+    for (int bi = 0; bi < (int)plan->buckets.size(); ++bi) {
+        if (bucket >= 0 && bi != bucket) continue;
+        auto &b = plan->buckets[bi];
+        NMX_ARG_CHECK(threads == kTileShape || shape_covers(threads, b.nmax, plan->nrhs), 4,
+                      "that CTA shape cannot cover this bucket's sizes");
+        const size_t smem = plan->dtype == NMX_F64 ? shape_smem<double>(threads, b.nmax, plan->nrhs)
+                                                   : shape_smem<float>(threads, b.nmax, plan->nrhs);
+        int per_sm = 0;
+        const int rc = plan->dtype == NMX_F64 ? shape_occupancy<double>(ctx, threads, smem, &per_sm)
+                                              : shape_occupancy<float>(ctx, threads, smem, &per_sm);
+        if (rc) return rc;
+        if (per_sm < 1) {
+            set_error("that CTA shape does not fit an SM for n up to %d", b.nmax);
+            return NMX_ERR_UNSUPPORTED;
+        }
+        b.threads = threads;
+        b.smem = smem;
+        b.grid = (int)std::min<int64_t>(b.end - b.begin, (int64_t)per_sm * ctx->sm_count);
+    }
+    if (plan->graph) {  // the captured shapes are stale
+        cudaGraphExecDestroy(plan->graph);
+        plan->graph = nullptr;
+    }
     return 0;
 }
 

@@ -147,7 +147,7 @@ def test_batched_autotune_and_graph_replay(oracle):
     X = torch.empty_like(dB)
     info = torch.empty(len(ns), dtype=torch.int32, device="cuda")
     sched = plan.autotune(dA, dB, X, info, L, reps=2)
-    assert len(sched) == 4 and all(s["threads"] in (64, 96, 128, 192) and s["ctas"] >= 1
+    assert len(sched) == 4 and all(s["threads"] in (64, 96, 128, 192, 256) and s["ctas"] >= 1
                                    for s in sched)
     torch.cuda.synchronize()
     assert int(info.abs().sum()) == 0
@@ -212,3 +212,50 @@ def test_batched_f32_full_config_vs_oracle_sample(oracle):
                                       wantX[sbo[j]:sbo[j] + n * nrhs]))
     assert worst_l <= 1e-5, worst_l
     assert worst_x <= 1e-5, worst_x
+
+
+@pytest.mark.parametrize("dtype", [np.float64])
+def test_batched_tile_shape_matches_oracle(oracle, dtype):
+    """The 8 x 8 DMMA tile kernel (CTA shape 256, FP64), forced on every
+    bucket through the autotuner's schedule override, against the oracle on
+    ragged sizes around every tile edge, several right-hand-side counts, and
+    numax's later-block failure (info = 4, NaN where the oracle has NaN)."""
+    import numax_b200 as nb
+    edge = [1, 2, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65, 95, 96, 97, 120, 127, 128]
+    rng = np.random.Generator(np.random.PCG64(256))
+    for nrhs in (0, 1, 4, 8):
+        ns = np.array(edge + list(rng.integers(1, 129, size=120)), dtype=np.int32)
+        rng.shuffle(ns)
+        A, B = make_batch(ns, nrhs, dtype, seed=nrhs + 40)
+        plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float64)
+        plan.force_shape(256)
+        dA = torch.from_numpy(A.copy()).cuda()
+        dB = torch.from_numpy(B.copy()).cuda() if nrhs else None
+        gotA, gotX, info = plan(dA, dB)
+        gotA, info = gotA.cpu().numpy(), info.cpu().numpy()
+        wantL, wantX = oracle.batched_cholesky_solve(ns, A, B if nrhs else np.zeros(0), nrhs)
+        ao, bo = oracle.ragged_offsets(ns), oracle.ragged_offsets(ns, nrhs)
+        assert (info == 0).all()
+        for i, n in enumerate(ns):
+            blk = gotA[ao[i]:ao[i] + n * n].reshape(n, n)
+            assert relerr(np.tril(blk), np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= 1e-12
+            np.testing.assert_array_equal(np.triu(blk, 1),
+                                          np.triu(A[ao[i]:ao[i] + n * n].reshape(n, n), 1))
+        if nrhs:
+            gotX = gotX.cpu().numpy()
+            for i, n in enumerate(ns):
+                assert relerr(gotX[bo[i]:bo[i] + n * nrhs], wantX[bo[i]:bo[i] + n * nrhs]) <= 1e-12
+    # numax's later-block failure through the tile kernel.
+    bad = np.array([4.0, 1.0, 0.0, 0.0, 1.0, 4.0, 0.0, 0.0, 0.0, 0.0, 1.0, 3.0,
+                    0.0, 0.0, 3.0, 1.0])
+    good_ns = np.array([20, 70], dtype=np.int32)
+    goodA, goodB = make_batch(good_ns, 2, np.float64, seed=1)
+    ns = np.array([20, 4, 70], dtype=np.int32)
+    A = np.concatenate([goodA[:400], bad, goodA[400:]])
+    B = np.concatenate([goodB[:40], np.ones(8), goodB[40:]])
+    plan = nb.CholeskySolveBatch(ns, nrhs=2, dtype=torch.float64)
+    plan.force_shape(256)
+    gotA, gotX, info = plan(torch.from_numpy(A.copy()).cuda(), torch.from_numpy(B.copy()).cuda())
+    assert list(info.cpu().numpy()) == [0, 4, 0]
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, 2)
+    np.testing.assert_array_equal(np.isnan(gotX.cpu().numpy()), np.isnan(wantX))
