@@ -504,6 +504,88 @@ def run_eigh(count, dev, steps=3, tol=1e-7, max_sweeps=20):
             "hbm_gbs": bytes_ / (ms / 1e3) / 1e9}
 
 
+def run_chol_ir(n, kappas, dev, seed=SEED):
+    """FP64 Cholesky solve (nmx_potrf_f64 + nmx_potrs_f64) vs the
+    mixed-precision Cholesky with FP64 refinement (nmx_posv_ir_f64) at order
+    n, A = U diag(s) U^T (U Haar, s geometric 1..1/kappa).  Device time,
+    inputs resident, workspaces reserved, each mode run twice (cold, warm)."""
+    import ctypes as C
+    import torch
+    from numax_b200 import _lib
+    lib = _lib.load()
+    ctx = _lib.context(dev.index)
+    stream = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 91)
+    u = haar_torch(n, gen, dev)
+    xt = torch.randn(n, generator=gen, dtype=torch.float64, device=dev)
+    _lib.call("nmx_posv_ir_reserve", ctx, n, _lib.NMX_IR_BF16 | _lib.NMX_IR_ESCALATE)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    work = torch.empty((n, n), dtype=torch.float64, device=dev)
+    info = torch.empty(1, dtype=torch.int32, device=dev)
+    out = {}
+    for ki, kappa in enumerate(kappas):
+        s = torch.logspace(0.0, -np.log10(kappa), n, dtype=torch.float64, device=dev)
+        a = (u * s[None, :]) @ u.T
+        a = (a + a.T) / 2
+        b = a @ xt
+        norm_a = float(a.abs().sum(1).max())
+
+        def berr(x):
+            r = b - a @ x
+            return float(r.abs().max() / (norm_a * x.abs().max() + b.abs().max()))
+        x64 = torch.empty_like(b)
+
+        def fp64_solve():
+            work.copy_(a)
+            x64.copy_(b)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            _lib.call("nmx_potrf_f64", ctx, n, work.data_ptr(), n, info.data_ptr(),
+                      stream.cuda_stream)
+            _lib.call("nmx_potrs_f64", ctx, n, 1, work.data_ptr(), n, x64.data_ptr(), 1,
+                      stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            return e0.elapsed_time(e1)
+        if ki == 0:
+            fp64_solve()
+        t64 = fp64_solve()
+        res = {"fp64_cholesky_solve_ms": t64, "fp64_backward_error": berr(x64)}
+        for label, prec in IR_MODES.get(kappa, IR_MODES[1e8]):
+            mode = getattr(_lib, f"NMX_IR_{prec}") | _lib.NMX_IR_AUTO | _lib.NMX_IR_ESCALATE
+            times = []
+            for rep in range(2):
+                x = torch.empty_like(b)
+                st = _lib.IrStats()
+                torch.cuda.synchronize(dev)
+                e0.record(stream)
+                rc = lib.nmx_posv_ir_f64(ctx, n, C.c_void_p(a.data_ptr()), n,
+                                         C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), mode,
+                                         1e-14, 60, C.byref(st), C.c_void_p(stream.cuda_stream))
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                if rc != 0:
+                    res[f"{label}_ir_error"] = _lib.last_error()
+                    break
+                times.append(e0.elapsed_time(e1))
+            if len(times) < 2:
+                continue
+            res[label] = {
+                "solve_ms_warm": times[1], "solve_ms_cold": times[0],
+                "backward_error": berr(x), "converged": bool(st.converged),
+                "final_precision": _lib.IR_PRECISION_NAMES.get(st.final_precision, "?"),
+                "iterations": st.iterations, "gmres_iterations": st.gmres_iterations,
+                "factor_ms": st.factor_ms, "refine_ms": st.refine_ms,
+                "forward_diff_vs_fp64": float((x - x64).abs().max() / x64.abs().max()),
+                "speedup_fp64_over_ir": t64 / times[1]}
+        out[f"{kappa:.0e}"] = res
+        del a, b, s
+        torch.cuda.empty_cache()
+    del work, u
+    return out
+
+
 def run_lu_ir_legs(args, dev):
     """The LU/IR comparison at every requested order; errors are reported in
     place so that the batched line still prints."""
@@ -515,6 +597,12 @@ def run_lu_ir_legs(args, dev):
             legs["orders"][str(n)] = run_lu_ir(n, kappas, dev)
         except Exception as exc:
             legs["orders"][str(n)] = {"error": f"{type(exc).__name__}: {exc}"}
+    if args.chol_n > 0:
+        try:
+            legs["cholesky"] = {"n": args.chol_n,
+                                "results": run_chol_ir(args.chol_n, kappas, dev)}
+        except Exception as exc:
+            legs["cholesky"] = {"n": args.chol_n, "error": f"{type(exc).__name__}: {exc}"}
     return legs
 
 
@@ -721,6 +809,9 @@ def main():
                          "(0 skips it)")
     ap.add_argument("--lu-kappas", default="1e2,1e5,1e8",
                     help="comma-separated condition numbers for the comparison")
+    ap.add_argument("--chol-n", type=int, default=16384,
+                    help="order of the FP64-Cholesky vs mixed-precision Cholesky IR leg "
+                         "(0 skips it)")
     ap.add_argument("--only-lu", action="store_true", help="run only the LU/IR comparison")
     ap.add_argument("--only-dense", action="store_true",
                     help="run only the dense LU/Cholesky/QR leg")

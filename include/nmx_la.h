@@ -382,6 +382,22 @@ NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda
  * itself allocates nothing.  No numax counterpart. */
 NMX_API int nmx_gesv_ir_reserve(nmx_ctx ctx, int64_t n, int mode);
 
+/* Mixed-precision Cholesky solve with iterative refinement: nmx_gesv_ir_f64's
+ * scheme for a symmetric positive definite A.  A is scaled symmetrically by
+ * powers of two (D A D, diagonal near 1), rounded to FP32 and factored by the
+ * recursive Cholesky of nmx_potrf_f32 with its SYRK and triangular-solve
+ * products on the tcgen05 tensor cores in the mode's precision; the
+ * corrections come from D L^-T L^-1 D, the residual and every other step as
+ * in nmx_gesv_ir_f64 (GMRES-IR, escalation up to an FP64 Cholesky, the best
+ * iterate returned).  The factorization reads A's lower triangle, the FP64
+ * residual all of A: both triangles must hold the matrix.  No numax
+ * counterpart; extends numax's cholesky (numax/linalg/cholesky.mojo:59-230)
+ * to low-precision factors with FP64 accuracy. */
+NMX_API int nmx_posv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, const double *b,
+                            double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
+                            void *stream);
+NMX_API int nmx_posv_ir_reserve(nmx_ctx ctx, int64_t n, int mode);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,8 @@ SIGNATURES = {
     "nmx_gesv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
     "nmx_gemm_sub_f32": (ci, [vp, i64, i64, i64, vp, i64, vp, i64, vp, i64, ci, vp]),
     "nmx_gesv_ir_reserve": (ci, [vp, i64, ci]),
+    "nmx_posv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
+    "nmx_posv_ir_reserve": (ci, [vp, i64, ci]),
     "nmx_gemm_f64": (ci, [vp, ci, ci, i64, i64, i64, C.c_double, vp, i64, vp, i64, C.c_double,
                           vp, i64, ci, vp]),
     "nmx_gemm_f32": (ci, [vp, ci, ci, i64, i64, i64, C.c_float, vp, i64, vp, i64, C.c_float,

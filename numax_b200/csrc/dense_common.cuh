@@ -102,6 +102,19 @@ struct GemmSub {
                                    sm_limit);
         return gemm_sub<float>(st, m, n, k, A, lda, B, ldb, C, ldc);
     }
+    // C[m x n] -= A[m x k] B[n x k]^T; `lower`: only C's lower triangle is
+    // needed (the SYRK-shaped update; the tensor-core path writes all of C,
+    // so its strict upper triangle must be scratch).
+    int sub_bt(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
+               int64_t ldb, double *C, int64_t ldc, bool lower = false) const {
+        return gemm_sub_bt<double>(st, m, n, k, A, lda, B, ldb, C, ldc, lower);
+    }
+    int sub_bt(int64_t m, int64_t n, int64_t k, const float *A, int64_t lda, const float *B,
+               int64_t ldb, float *C, int64_t ldc, bool lower = false) const {
+        if (precision && n >= tc_min && k >= tc_min)
+            return tc_gemm_sub_bt_f32(st, precision, m, n, k, A, lda, B, ldb, C, ldc, ws, ws_bytes);
+        return gemm_sub_bt<float>(st, m, n, k, A, lda, B, ldb, C, ldc, lower);
+    }
 };
 
 // Blocked triangular solves, row-major (dense_lu.cu):
@@ -127,5 +140,13 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
 
 // The tallest panel the tournament-pivoting leaf takes (dense_lu.cu).
 int64_t tournament_max_rows();
+
+// Recursive lower Cholesky of the n x n row-major A in place (dense_potrf.cu),
+// numax's potrf_diag rule at the leaves, updates through `gs` (its precision
+// sends the FP32 SYRK / triangular-solve products to the tensor cores).  The
+// strict upper triangle is scratch; *info (device) gets the first failing
+// pivot.
+template <typename T>
+int potrf_run(const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *info);
 
 }  // namespace nmx

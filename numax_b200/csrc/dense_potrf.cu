@@ -192,8 +192,9 @@ __global__ void zero_upper_kernel(T *A, int64_t lda, int n) {
 
 // X := X L^-T, X = rows [r0, r1) x cols [c, c+w), L the lower block at (c, c).
 template <typename T>
-static int trsm_right_lt(cudaStream_t st, T *A, int64_t lda, int c, int w, int r0,
+static int trsm_right_lt(const GemmSub &gs, T *A, int64_t lda, int c, int w, int r0,
                          int r1) {
+    cudaStream_t st = gs.st;
     if (w <= 0 || r1 <= r0) return 0;
     if (w > kCholLeaf && w <= kCholTrsmMaxW && w % 32 == 0) {
         static bool attr_set[64] = {};
@@ -218,33 +219,32 @@ static int trsm_right_lt(cudaStream_t st, T *A, int64_t lda, int c, int w, int r
         return 0;
     }
     const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
-    int rc = trsm_right_lt<T>(st, A, lda, c, hw, r0, r1);
+    int rc = trsm_right_lt<T>(gs, A, lda, c, hw, r0, r1);
     if (rc) return rc;
     // X_b -= X_a L_ba^T, L_ba = rows [c+hw, c+w) x cols [c, c+hw).
-    NMX_TRY(gemm_sub_bt<T>(st, r1 - r0, w - hw, hw, A + (int64_t)r0 * lda + c, lda,
-                           A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)r0 * lda + c + hw,
-                           lda));
-    return trsm_right_lt<T>(st, A, lda, c + hw, w - hw, r0, r1);
+    NMX_TRY(gs.sub_bt(r1 - r0, w - hw, hw, A + (int64_t)r0 * lda + c, lda,
+                      A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)r0 * lda + c + hw, lda));
+    return trsm_right_lt<T>(gs, A, lda, c + hw, w - hw, r0, r1);
 }
 
 template <typename T>
-static int potrf_rec(cudaStream_t st, T *A, int64_t lda, int c, int w,
-                     int32_t *info) {
+static int potrf_rec(const GemmSub &gs, T *A, int64_t lda, int c, int w, int32_t *info) {
+    cudaStream_t st = gs.st;
     if (w <= kCholLeaf) {
         potrf_leaf_kernel<T><<<1, 32, 0, st>>>(A, lda, c, w, info);
         NMX_CUDA_TRY(cudaGetLastError());
         return 0;
     }
     const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
-    int rc = potrf_rec<T>(st, A, lda, c, hw, info);
+    int rc = potrf_rec<T>(gs, A, lda, c, hw, info);
     if (rc) return rc;
-    rc = trsm_right_lt<T>(st, A, lda, c, hw, c + hw, c + w);
+    rc = trsm_right_lt<T>(gs, A, lda, c, hw, c + hw, c + w);
     if (rc) return rc;
     // A22 -= L21 L21^T on the lower triangle.
-    NMX_TRY(gemm_sub_bt<T>(st, w - hw, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
-                           A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)(c + hw) * lda + c + hw,
-                           lda, true));
-    return potrf_rec<T>(st, A, lda, c + hw, w - hw, info);
+    NMX_TRY(gs.sub_bt(w - hw, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
+                      A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)(c + hw) * lda + c + hw,
+                      lda, true));
+    return potrf_rec<T>(gs, A, lda, c + hw, w - hw, info);
 }
 
 template <typename T>
@@ -258,7 +258,9 @@ static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     if (n == 0) return 0;
-    int rc = potrf_rec<T>(st, A, lda, 0, (int)n, info);
+    GemmSub gs;
+    gs.st = st;
+    int rc = potrf_rec<T>(gs, A, lda, 0, (int)n, info);
     if (rc) return rc;
     const int threads = 256;
     zero_upper_kernel<T><<<(unsigned)ceil_div(n * n, threads), threads, 0, st>>>(A, lda, (int)n);
@@ -285,6 +287,15 @@ static int potrs(nmx_ctx ctx, int64_t n, int64_t nrhs, const T *L, int64_t lda, 
     if (rc) return rc;
     return trsm_upper<T, true>(gs, L, lda, 0, (int)n, B, ldb, 0, (int)nrhs);
 }
+
+template <typename T>
+int potrf_run(const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *info) {
+    NMX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int32_t), gs.st));
+    if (n == 0) return 0;
+    return potrf_rec<T>(gs, A, lda, 0, (int)n, info);
+}
+template int potrf_run<double>(const GemmSub &, int64_t, double *, int64_t, int32_t *);
+template int potrf_run<float>(const GemmSub &, int64_t, float *, int64_t, int32_t *);
 
 }  // namespace nmx
 

@@ -33,12 +33,15 @@ using namespace cute;
 // One complete sm100 GEMM type per 16-bit input type, spelled at namespace
 // scope (the host compiler rejects the dependent carve-out inside a class
 // template).
-#define NMX_TC_GEMM(NAME, ELEM, SCHED)                                                           \
+// LAYOUTB RowMajor: B is K x N with N contiguous (C -= A B); ColumnMajor: B
+// is stored N x K with K contiguous (C -= A B^T), its leading dimension the
+// stride between its N rows.
+#define NMX_TC_GEMM(NAME, ELEM, SCHED, LAYOUTB, BSTRIDE_MODE)                                    \
     namespace NAME {                                                                             \
     using ElementA = ELEM;                                                                       \
     using ElementB = ELEM;                                                                       \
     using LayoutA = cutlass::layout::RowMajor; /* M x K, K contiguous */                         \
-    using LayoutB = cutlass::layout::RowMajor; /* K x N, N contiguous (MN-major) */              \
+    using LayoutB = LAYOUTB;                                                                     \
     using LayoutC = cutlass::layout::RowMajor;                                                   \
     using TileMNK = Shape<_128, _256, _64>;                                                      \
     using ClusterMNK = Shape<_1, _1, _1>;                                                        \
@@ -62,7 +65,7 @@ using namespace cute;
         Kernel::StrideC sc{};                                                                    \
         Kernel::StrideD sd{};                                                                    \
         cute::get<0>(sa) = lda;                                                                  \
-        cute::get<1>(sb) = ldb;                                                                  \
+        cute::get<BSTRIDE_MODE>(sb) = ldb;                                                       \
         cute::get<0>(sc) = ldc;                                                                  \
         cute::get<0>(sd) = ldc;                                                                  \
         cutlass::KernelHardwareInfo hw;                                                          \
@@ -87,10 +90,15 @@ using namespace cute;
 // The default (hardware cluster-launch-control) scheduler takes every SM;
 // the static persistent one runs on at most `sm_count` SMs, leaving the rest
 // to concurrent work (the look-ahead LU's panel stream).
-NMX_TC_GEMM(bf16, cutlass::bfloat16_t, void)
-NMX_TC_GEMM(fp16, cutlass::half_t, void)
-NMX_TC_GEMM(bf16s, cutlass::bfloat16_t, cutlass::gemm::StaticPersistentScheduler)
-NMX_TC_GEMM(fp16s, cutlass::half_t, cutlass::gemm::StaticPersistentScheduler)
+NMX_TC_GEMM(bf16, cutlass::bfloat16_t, void, cutlass::layout::RowMajor, 1)
+NMX_TC_GEMM(fp16, cutlass::half_t, void, cutlass::layout::RowMajor, 1)
+NMX_TC_GEMM(bf16s, cutlass::bfloat16_t, cutlass::gemm::StaticPersistentScheduler,
+            cutlass::layout::RowMajor, 1)
+NMX_TC_GEMM(fp16s, cutlass::half_t, cutlass::gemm::StaticPersistentScheduler,
+            cutlass::layout::RowMajor, 1)
+// B^T operands (the Cholesky's SYRK and right-side triangular-solve products).
+NMX_TC_GEMM(bf16t, cutlass::bfloat16_t, void, cutlass::layout::ColumnMajor, 0)
+NMX_TC_GEMM(fp16t, cutlass::half_t, void, cutlass::layout::ColumnMajor, 0)
 #undef NMX_TC_GEMM
 
 }  // namespace tc
@@ -169,6 +177,35 @@ static inline int split_factor(int precision) {
     return precision == NMX_PREC_BF16X3 ? 3 : precision == NMX_PREC_BF16X6 ? 6 : 1;
 }
 
+// Rows of an fp32 block (rows x cols, lds) rounded or split into 16-bit
+// pieces side by side along the row: dst[r][q cols_p + c] = piece number
+// (PAT >> 2q) & 3 of src[r][c] (0 = the rounding h, 1 = the residual's
+// rounding m, 2 = the second residual's l), for the NSEG segments.  This is
+// A's layout for every precision, and B's when B is stored N x K (K-major):
+// the segment patterns pair A's pieces with B's, e.g. BF16X3 A = [h h m],
+// B = [h m h].  Zero past rows x cols.
+template <typename Elem, int NSEG, int PAT>
+__global__ void round_rows_kernel(const float *src, int64_t lds, int rows, int cols, int rows_p,
+                                  int cols_p, Elem *dst, int64_t ldd) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)rows_p * cols_p) return;
+    const int r = (int)(e / cols_p), c = (int)(e - (int64_t)r * cols_p);
+    const float v = (r < rows && c < cols) ? src[(int64_t)r * lds + c] : 0.0f;
+    Elem piece[3];
+    piece[0] = Elem(v);
+    if (NSEG > 1) {
+        const float r1 = v - float(piece[0]);
+        piece[1] = Elem(r1);
+        piece[2] = Elem(r1 - float(piece[1]));
+    }
+    Elem *d = dst + (int64_t)r * ldd;
+#pragma unroll
+    for (int q = 0; q < NSEG; ++q) d[(int64_t)q * cols_p + c] = piece[(PAT >> (2 * q)) & 3];
+}
+constexpr int kPatX1 = 0;
+constexpr int kPatX3B = (1 << 2);                                   // [h m h]
+constexpr int kPatX6B = (1 << 2) | (2 << 6) | (1 << 8);             // [h m h l m h]
+
 // The GEMM runs on K and N rounded up to multiples of 8 (the 16-byte TMA and
 // epilogue granularity): the padded rows/columns of the 16-bit operands are
 // zero, so the extra columns of C (up to N rounded to 8) get C - 0 and are
@@ -177,8 +214,9 @@ static inline int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
 
 int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K, const float *A,
                     int64_t lda, const float *B, int64_t ldb, float *C, int64_t ldc, void *ws,
-                    size_t ws_bytes, int sm_limit) {
+                    size_t ws_bytes, int sm_limit, bool b_kmajor) {
     if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (b_kmajor) return tc_gemm_sub_bt_f32(st, precision, M, N, K, A, lda, B, ldb, C, ldc, ws, ws_bytes);
     const int64_t Kp = up8(K), Np = up8(N);
     const size_t need = tc_gemm_workspace_bytes(M, N, K, precision);
     if (need > ws_bytes) {
@@ -236,6 +274,70 @@ int tc_gemm_sub_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_
     if (rc) {
         set_error("tensor-core GEMM %lldx%lldx%lld failed at step %d", (long long)M, (long long)N,
                   (long long)K, rc);
+        return NMX_ERR_INTERNAL;
+    }
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// C -= A B^T with B stored N x K (ldb): A rounded / split as in the NN path,
+// B rounded / split along its rows (K-major) with the segment pattern that
+// pairs with A's, and the K-major-B GEMM.
+int tc_gemm_sub_bt_f32(cudaStream_t st, int precision, int64_t M, int64_t N, int64_t K,
+                       const float *A, int64_t lda, const float *B, int64_t ldb, float *C,
+                       int64_t ldc, void *ws, size_t ws_bytes) {
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    const int64_t Kp = up8(K), Np = up8(N);
+    const size_t need = tc_gemm_workspace_bytes(M, N, K, precision);
+    if (need > ws_bytes) {
+        set_error("tensor-core update needs %zu B of workspace, have %zu", need, ws_bytes);
+        return NMX_ERR_INTERNAL;
+    }
+    if ((ldc % 4) != 0 || (reinterpret_cast<uintptr_t>(C) % 16) != 0 || ldc < Np) {
+        set_error("tensor-core update: C must be 16-byte aligned, ldc %% 4 == 0, ldc >= N rounded to 8");
+        return NMX_ERR_INTERNAL;
+    }
+    const int nseg = split_factor(precision);
+    const int64_t Kw = nseg * Kp;
+    auto *a16 = static_cast<unsigned char *>(ws);
+    auto *b16 = a16 + ((2 * (size_t)M * Kw + 255) & ~size_t(255));
+    const int threads = 256;
+    const unsigned ga = (unsigned)ceil_div(M * Kp, threads), gb = (unsigned)ceil_div(Np * Kp, threads);
+    int rc;
+    if (precision == NMX_PREC_FP16) {
+        auto *a = reinterpret_cast<cutlass::half_t *>(a16);
+        auto *b = reinterpret_cast<cutlass::half_t *>(b16);
+        round_block_kernel<cutlass::half_t><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                    (int)Kp, a, Kp);
+        round_rows_kernel<cutlass::half_t, 1, kPatX1><<<gb, threads, 0, st>>>(
+            B, ldb, (int)N, (int)K, (int)Np, (int)Kp, b, Kw);
+        NMX_CUDA_TRY(cudaGetLastError());
+        rc = tc::fp16t::run((int)M, (int)Np, (int)Kw, a, Kw, b, Kw, C, ldc, st, 0);
+    } else {
+        auto *a = reinterpret_cast<cutlass::bfloat16_t *>(a16);
+        auto *b = reinterpret_cast<cutlass::bfloat16_t *>(b16);
+        if (precision == NMX_PREC_BF16X3) {
+            round_split_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                  (int)Kp, a, Kw);
+            round_rows_kernel<cutlass::bfloat16_t, 3, kPatX3B><<<gb, threads, 0, st>>>(
+                B, ldb, (int)N, (int)K, (int)Np, (int)Kp, b, Kw);
+        } else if (precision == NMX_PREC_BF16X6) {
+            round_split6_bf16_kernel<true><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K, (int)M,
+                                                                   (int)Kp, a, Kw);
+            round_rows_kernel<cutlass::bfloat16_t, 6, kPatX6B><<<gb, threads, 0, st>>>(
+                B, ldb, (int)N, (int)K, (int)Np, (int)Kp, b, Kw);
+        } else {
+            round_block_kernel<cutlass::bfloat16_t><<<ga, threads, 0, st>>>(A, lda, (int)M, (int)K,
+                                                                            (int)M, (int)Kp, a, Kp);
+            round_rows_kernel<cutlass::bfloat16_t, 1, kPatX1><<<gb, threads, 0, st>>>(
+                B, ldb, (int)N, (int)K, (int)Np, (int)Kp, b, Kw);
+        }
+        NMX_CUDA_TRY(cudaGetLastError());
+        rc = tc::bf16t::run((int)M, (int)Np, (int)Kw, a, Kw, b, Kw, C, ldc, st, 0);
+    }
+    if (rc) {
+        set_error("tensor-core GEMM (B^T) %lldx%lldx%lld failed at step %d", (long long)M,
+                  (long long)N, (long long)K, rc);
         return NMX_ERR_INTERNAL;
     }
     NMX_CUDA_TRY(cudaGetLastError());

@@ -69,12 +69,13 @@ __device__ __forceinline__ void st_release_i32(int *p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Inverse of every 64 x 64 diagonal block of the unit-lower (UPPER = false)
-// or upper (UPPER = true) triangle of the factor F (FP32 or FP64), in FP64:
+// Inverse of every 64 x 64 diagonal block of the lower (UPPER = false; unit
+// diagonal when UNIT) or upper (UPPER = true) triangle of the factor F (FP32
+// or FP64), in FP64:
 // one CTA per block, thread j forms column j of the inverse by substitution.
 // Computed once per factorization; it turns each block's serial substitution
 // in the triangular solves into a 64 x 64 matrix-vector product.
-template <typename TF, bool UPPER>
+template <typename TF, bool UPPER, bool UNIT = true>
 __global__ void __launch_bounds__(kTrsvRB)
     diag_inverse_kernel(const TF *F, int64_t ldf, int n, double *Inv) {
     __shared__ double D[kTrsvRB][kTrsvRB + 1];
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(kTrsvRB)
 #pragma unroll
                 for (int p = 0; p < kTrsvRB; ++p)
                     if (p < i) s -= D[i][p] * x[p];
-                x[i] = (i < rows) ? s : 0.0;
+                x[i] = (i < rows) ? (UNIT ? s : s / D[i][i]) : 0.0;
             }
         } else {
 #pragma unroll
@@ -425,6 +426,47 @@ __global__ void scale_copy_kernel(const double *A, int64_t lda, int n, const dou
     W[(int64_t)i * ldw + j] = (TW)(A[(int64_t)i * lda + j] * rs[i] * cs[j]);
 }
 
+// Symmetric scaling D = diag(2^-round(log2 sqrt(a_ii))) (1 for a
+// non-positive or non-finite a_ii): D A D has its diagonal in [0.5, 2).
+__global__ void sym_scale_kernel(const double *A, int64_t lda, int n, double *d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double a = A[(int64_t)i * lda + i];
+        d[i] = (a > 0.0 && isfinite(a)) ? exp2(-rint(0.5 * log2(a))) : 1.0;
+    }
+}
+
+// Copy the lower triangle of the n x n factor W into its strict upper
+// triangle transposed (upper = L^T), 32 x 32 tiles through shared memory so
+// that both the reads and the writes run along rows.  Tile (I, J), J <= I,
+// is read and written to (J, I); a diagonal tile keeps its lower half.
+template <typename T>
+__global__ void __launch_bounds__(256) mirror_lower_kernel(T *W, int64_t ldw, int n) {
+    __shared__ T t[32][33];
+    const int I = blockIdx.y, J = blockIdx.x;
+    if (J > I) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = 32 * I + ty + 8 * k, c = 32 * J + tx;
+        t[ty + 8 * k][tx] = (r < n && c < n && c <= r) ? W[(int64_t)r * ldw + c] : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = 32 * J + ty + 8 * k, c = 32 * I + tx;  // destination (r, c) = source (c, r)
+        if (r < n && c < n && c > r) W[(int64_t)r * ldw + c] = t[tx][ty + 8 * k];
+    }
+}
+
+__global__ void iota_kernel(int *p, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        p[i] = i;
+        p[n + i] = i;
+    }
+}
+
 // v[i] = s[perm[i]] * rs[perm[i]]  (apply P R to a vector).
 __global__ void permute_scale_kernel(const double *s, const int *perm, const double *rs, int n,
                                      double *v) {
@@ -694,6 +736,7 @@ static int gemm_precision(int level) {
 struct IrRun {
     nmx_ctx ctx;
     cudaStream_t st;
+    bool spd = false;  // Cholesky factors (A symmetric positive definite)
     int n;
     const double *A;
     int64_t lda;
@@ -731,8 +774,12 @@ static size_t ir_krylov_bytes(int64_t n, int G) {
 // panels of nb columns (tournament leaves, order >= 2 nb; the same decision
 // getrf_run makes) bound its inner dimension at nb; otherwise the recursion's
 // largest update is about half the order.
-static size_t ir_gemm_ws_bytes(nmx_ctx ctx, int64_t n, int prec) {
+static size_t ir_gemm_ws_bytes(nmx_ctx ctx, int64_t n, int prec, bool spd = false) {
     if (!prec) return 0;
+    if (spd) {  // the Cholesky recursion: the largest update is the first SYRK
+        const int64_t half = (n / 2 + 31) / 32 * 32;
+        return tc_gemm_workspace_bytes(n - half, n - half, std::max<int64_t>(half, 1), prec) + 4096;
+    }
     const bool tournament = ctx->tune_lu_tournament != 0 && n <= tournament_max_rows();
     const int64_t want = ctx->tune_lu_lookahead >= 0 ? ctx->tune_lu_lookahead : 256;
     const int64_t nb = std::min<int64_t>(1024, want / 32 * 32);
@@ -744,7 +791,7 @@ static size_t ir_gemm_ws_bytes(nmx_ctx ctx, int64_t n, int prec) {
 
 // Every buffer a solve at `level` (and, when escalating, at the levels above
 // it) needs, grown now.
-static int ir_reserve(nmx_ctx ctx, int64_t n, int level, bool escalate) {
+static int ir_reserve(nmx_ctx ctx, int64_t n, int level, bool escalate, bool spd) {
     void *p = nullptr;
     const int64_t ldw = (n + 7) / 8 * 8;
     const int G = std::max(1, std::min<int>(2 * ctx->sm_count, (int)ceil_div(n, 256)));
@@ -760,7 +807,7 @@ static int ir_reserve(nmx_ctx ctx, int64_t n, int level, bool escalate) {
             need64 = true;
         else
             need32 = true;
-        gemm_ws = std::max(gemm_ws, ir_gemm_ws_bytes(ctx, n, gemm_precision(lv)));
+        gemm_ws = std::max(gemm_ws, ir_gemm_ws_bytes(ctx, n, gemm_precision(lv), spd));
         if (!escalate || lv == kLvFP64) break;
     }
     if (need32) NMX_TRY(ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * ldw + 256, &p));
@@ -836,8 +883,16 @@ static int ir_factor(IrRun &R, int level, int32_t *hinfo, cudaEvent_t done) {
     NMX_CUDA_TRY(cudaMemsetAsync(R.norms, 0, sizeof(unsigned long long), st));
     row_norms_kernel<<<wb, threads, 0, st>>>(R.A, R.lda, n, R.norms, R.rowmax);
     const int equil = level == kLvFP16 ? 1 : 0;
-    row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
-    if (equil) {
+    if (R.spd) {
+        // Symmetric scaling D A D (every level: it keeps the Cholesky's
+        // pivots near 1), no permutation.
+        sym_scale_kernel<<<vb, threads, 0, st>>>(R.A, R.lda, n, R.rs);
+        NMX_CUDA_TRY(cudaMemcpyAsync(R.cs, R.rs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    } else {
+        row_scale_kernel<<<vb, threads, 0, st>>>(R.rowmax, n, R.rs, equil);
+    }
+    if (R.spd) {
+    } else if (equil) {
         // The column maxima go through R.tmp's bits (free until the solve).
         unsigned long long *cmax = reinterpret_cast<unsigned long long *>(R.tmp);
         NMX_CUDA_TRY(cudaMemsetAsync(cmax, 0, sizeof(double) * n, st));
@@ -855,7 +910,10 @@ static int ir_factor(IrRun &R, int level, int32_t *hinfo, cudaEvent_t done) {
         NMX_CUDA_TRY(cudaGetLastError());
         GemmSub gs;
         gs.st = st;
-        NMX_TRY(getrf_run<double>(ctx, gs, n, R.W64, R.ldw, R.ipiv, R.info_d, false));
+        if (R.spd)
+            NMX_TRY(potrf_run<double>(gs, n, R.W64, R.ldw, R.info_d));
+        else
+            NMX_TRY(getrf_run<double>(ctx, gs, n, R.W64, R.ldw, R.ipiv, R.info_d, false));
     } else {
         NMX_TRY(ctx->ensure_slot(kWsWork, sizeof(float) * (size_t)n * R.ldw + 256, &p));
         R.W = static_cast<float *>(p);
@@ -866,11 +924,22 @@ static int ir_factor(IrRun &R, int level, int32_t *hinfo, cudaEvent_t done) {
         gs.precision = gemm_precision(level);
         if (ctx->tune_ir_tc_min >= 0) gs.tc_min = ctx->tune_ir_tc_min;
         if (gs.precision) {
-            gs.ws_bytes = ir_gemm_ws_bytes(ctx, n, gs.precision);
+            gs.ws_bytes = ir_gemm_ws_bytes(ctx, n, gs.precision, R.spd);
             NMX_TRY(ctx->ensure_slot(kWsGemm16, gs.ws_bytes, &gs.ws));
         }
-        NMX_TRY(getrf_run<float>(ctx, gs, n, R.W, R.ldw, R.ipiv, R.info_d,
-                                 ctx->tune_lu_tournament != 0));
+        if (R.spd)
+            NMX_TRY(potrf_run<float>(gs, n, R.W, R.ldw, R.info_d));
+        else
+            NMX_TRY(getrf_run<float>(ctx, gs, n, R.W, R.ldw, R.ipiv, R.info_d,
+                                     ctx->tune_lu_tournament != 0));
+    }
+    if (R.spd) {  // upper = L^T, so that the two solves read rows
+        const dim3 mg((unsigned)ceil_div(n, 32), (unsigned)ceil_div(n, 32));
+        if (level == kLvFP64)
+            mirror_lower_kernel<double><<<mg, 256, 0, st>>>(R.W64, R.ldw, n);
+        else
+            mirror_lower_kernel<float><<<mg, 256, 0, st>>>(R.W, R.ldw, n);
+        NMX_CUDA_TRY(cudaGetLastError());
     }
     // Inverses of the diagonal blocks of L and U for the triangular solves.
     const int NB = (n + kTrsvRB - 1) / kTrsvRB;
@@ -878,14 +947,28 @@ static int ir_factor(IrRun &R, int level, int32_t *hinfo, cudaEvent_t done) {
     R.invL = static_cast<double *>(p);
     R.invU = R.invL + (size_t)NB * kTrsvRB * kTrsvRB;
     if (level == kLvFP64) {
-        diag_inverse_kernel<double, false><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invL);
+        if (R.spd)
+            diag_inverse_kernel<double, false, false><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invL);
+        else
+            diag_inverse_kernel<double, false><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invL);
         diag_inverse_kernel<double, true><<<NB, kTrsvRB, 0, st>>>(R.W64, R.ldw, n, R.invU);
     } else {
-        diag_inverse_kernel<float, false><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invL);
+        if (R.spd)
+            diag_inverse_kernel<float, false, false><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invL);
+        else
+            diag_inverse_kernel<float, false><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invL);
         diag_inverse_kernel<float, true><<<NB, kTrsvRB, 0, st>>>(R.W, R.ldw, n, R.invU);
     }
     NMX_CUDA_TRY(cudaGetLastError());
     if (done) NMX_CUDA_TRY(cudaEventRecord(done, st));
+    if (R.spd) {  // no pivoting: identity permutation
+        *hinfo = 0;
+        iota_kernel<<<(unsigned)ceil_div(n, threads), threads, 0, st>>>(R.perm, n);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_CUDA_TRY(cudaMemcpyAsync(hinfo, R.info_d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        NMX_CUDA_TRY(cudaStreamSynchronize(st));
+        return 0;
+    }
     // Pivots -> permutation and its inverse on the host (the interchanges
     // compose in order).
     std::vector<int32_t> hp(n), perm(2 * (size_t)n);
@@ -979,7 +1062,7 @@ static int ir_residual(IrRun &R, const double *b, const double *x, double normA,
 
 static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const double *b,
                    double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
-                   void *stream) {
+                   void *stream, bool spd) {
     NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
     NMX_ARG_CHECK(n64 >= 1 && n64 <= (1 << 17), 2, "n must be in 1..131072");
     NMX_ARG_CHECK(A != nullptr, 3, "A is NULL");
@@ -1001,6 +1084,7 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     IrRun R;
     R.ctx = ctx;
     R.st = st;
+    R.spd = spd;
     R.n = n;
     R.A = A;
     R.lda = lda;
@@ -1009,7 +1093,7 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
     R.rows_per = (int)ceil_div(n, R.G);
     R.G = (int)ceil_div(n, R.rows_per);
     int level = level_of(prec);
-    NMX_TRY(ir_reserve(ctx, n, level, escalate));
+    NMX_TRY(ir_reserve(ctx, n, level, escalate, spd));
     void *p = nullptr;
     NMX_TRY(ctx->ensure_slot(kWsVec, ir_vec_bytes(n), &p));
     char *vp = static_cast<char *>(p);
@@ -1156,15 +1240,29 @@ static int gesv_ir(nmx_ctx ctx, int64_t n64, const double *A, int64_t lda, const
 extern "C" NMX_API int nmx_gesv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda,
                                        const double *b, double *x, int mode, double tol,
                                        int max_iter, nmx_ir_stats *stats, void *stream) {
-    return nmx::gesv_ir(ctx, n, A, lda, b, x, mode, tol, max_iter, stats, stream);
+    return nmx::gesv_ir(ctx, n, A, lda, b, x, mode, tol, max_iter, stats, stream, false);
 }
 
-extern "C" NMX_API int nmx_gesv_ir_reserve(nmx_ctx ctx, int64_t n, int mode) {
+extern "C" NMX_API int nmx_posv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda,
+                                       const double *b, double *x, int mode, double tol,
+                                       int max_iter, nmx_ir_stats *stats, void *stream) {
+    return nmx::gesv_ir(ctx, n, A, lda, b, x, mode, tol, max_iter, stats, stream, true);
+}
+
+static int ir_reserve_entry(nmx_ctx ctx, int64_t n, int mode, bool spd) {
     NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
     NMX_ARG_CHECK(n >= 1 && n <= (1 << 17), 2, "n must be in 1..131072");
     const int prec = mode & 0xF;
     NMX_ARG_CHECK(prec >= NMX_IR_BF16 && prec <= NMX_IR_FP64, 3,
                   "mode must be NMX_IR_BF16/FP16/FP32/BF16X3/BF16X6/FP64 with optional flags");
     nmx::DeviceGuard g(ctx->device);
-    return nmx::ir_reserve(ctx, n, nmx::level_of(prec), (mode & NMX_IR_ESCALATE) != 0);
+    return nmx::ir_reserve(ctx, n, nmx::level_of(prec), (mode & NMX_IR_ESCALATE) != 0, spd);
+}
+
+extern "C" NMX_API int nmx_gesv_ir_reserve(nmx_ctx ctx, int64_t n, int mode) {
+    return ir_reserve_entry(ctx, n, mode, false);
+}
+
+extern "C" NMX_API int nmx_posv_ir_reserve(nmx_ctx ctx, int64_t n, int mode) {
+    return ir_reserve_entry(ctx, n, mode, true);
 }

@@ -213,14 +213,15 @@ _IR_MODES = {name: code for code, name in _lib.IR_PRECISION_NAMES.items()}
 
 
 def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: float = 1e-14,
-             max_iter: int = 50, escalate: bool = False):
+             max_iter: int = 50, escalate: bool = False, spd: bool = False):
     """x with a x = b for float64 a, b: low-precision LU (BF16/FP16 tensor-core
     trailing updates, BF16 splits with ~16 ("bf16x3") or 24 ("bf16x6") bits,
     FP32, or FP64) refined in FP64 to backward error <= tol, with GMRES-IR
     when `gmres` is True (or "auto": when plain refinement stalls); with
     `escalate`, a precision whose refinement cannot converge is replaced by
     the next more accurate one.  x is the iterate with the smallest backward
-    error.
+    error.  With `spd` (a symmetric positive definite, both triangles
+    holding it) the factors are Cholesky's instead of LU's.
 
     Returns (x, stats) with stats a dict: iterations, gmres_iterations,
     converged, info, used_gmres, final_precision (name), backward_error,
@@ -242,7 +243,8 @@ def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: flo
         mode |= _lib.NMX_IR_ESCALATE
     st = _lib.IrStats()
     import ctypes as _C
-    _lib.call("nmx_gesv_ir_f64", _ctx(dev), n, A.data_ptr(), A.stride(0), bb.data_ptr(),
+    _lib.call("nmx_posv_ir_f64" if spd else "nmx_gesv_ir_f64", _ctx(dev), n, A.data_ptr(),
+              A.stride(0), bb.data_ptr(),
               x.data_ptr(), mode, float(tol), int(max_iter), _C.byref(st), _stream(dev))
     stats = {f: getattr(st, f) for f, _ in _lib.IrStats._fields_}
     stats["final_precision"] = _lib.IR_PRECISION_NAMES.get(st.final_precision, "?")

@@ -137,3 +137,83 @@ def test_ir_rejects_bad_arguments():
     assert lib.nmx_gesv_ir_reserve(ctx, 0, 1) == -2
     assert lib.nmx_gesv_ir_reserve(ctx, 64, 0) == -3
     assert lib.nmx_gesv_ir_reserve(ctx, 64, 1 | 0x40) == 0
+
+
+def make_spd(n, kappa, seed):
+    """A = U diag(s) U^T (Haar U, s geometric 1 .. 1/kappa): symmetric positive
+    definite with condition number kappa."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    u = haar(n, rng)
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a = (u * s) @ u.T
+    a = (a + a.T) / 2
+    x = rng.standard_normal(n)
+    return a, a @ x
+
+
+@pytest.mark.parametrize("precision,gmres,kappa,escalate", [
+    ("bf16x3", "auto", 1e2, False), ("fp16", "auto", 1e2, False), ("bf16", "auto", 1e2, True),
+    ("bf16x6", "auto", 1e5, False), ("fp32", "auto", 1e5, False), ("bf16x6", True, 1e8, False),
+    ("bf16", False, 1e8, True), ("fp64", False, 1e8, False),
+])
+def test_spd_ir_reaches_fp64_backward_error(precision, gmres, kappa, escalate):
+    """Cholesky factors (tensor-core SYRK / triangular-solve products) with
+    FP64 refinement: FP64 backward error, forward error within the
+    conditioning, against LAPACK's FP64 solve."""
+    from numax_b200 import linalg
+    n = 1000
+    a, b = make_spd(n, kappa, seed=7 + int(np.log10(kappa)))
+    x, st = linalg.solve_ir(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
+                            precision=precision, gmres=gmres, tol=1e-14, max_iter=60,
+                            escalate=escalate, spd=True)
+    x = x.cpu().numpy()
+    assert st["converged"] == 1, st
+    assert berr(a, x, b) <= 1e-14, (berr(a, x, b), st)
+    xr = np.linalg.solve(a, b)
+    assert np.abs(x - xr).max() / np.abs(xr).max() <= kappa * 1e-13
+    if not escalate:
+        assert st["final_precision"] == precision
+
+
+@pytest.mark.parametrize("kappa,precision,escalate", [
+    (1e2, "bf16x3", False), (1e2, "fp16", False), (1e5, "bf16x6", False), (1e8, "bf16x6", True),
+])
+def test_spd_ir_8192(kappa, precision, escalate):
+    """The SPD solve at n = 8192 (U diag(s) U^T, U Haar on the GPU)."""
+    from numax_b200 import linalg
+    n = 8192
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(4096 + int(np.log10(kappa)))
+    u = _haar_gpu(n, gen)
+    s = torch.logspace(0.0, -np.log10(kappa), n, dtype=torch.float64, device="cuda")
+    a = (u * s[None, :]) @ u.T
+    a = (a + a.T) / 2
+    del u
+    xt = torch.randn(n, generator=gen, dtype=torch.float64, device="cuda")
+    b = a @ xt
+    x, st = linalg.solve_ir(a, b, precision=precision, gmres="auto", tol=1e-14, max_iter=80,
+                            escalate=escalate, spd=True)
+    assert st["converged"] == 1, st
+    assert _berr_gpu(a, x, b) <= 1e-14, st
+    xr = torch.linalg.solve(a, b)
+    assert float((x - xr).abs().max() / xr.abs().max()) <= kappa * 1e-12, st
+
+
+def test_spd_ir_gram_matrix_and_not_spd():
+    """The BASELINE SPD family G G^T / n + I solves at BF16X3; a matrix that
+    is not positive definite does not converge and reports so (it never
+    returns a blown-up x)."""
+    from numax_b200 import linalg
+    n = 2000
+    rng = np.random.Generator(np.random.PCG64(2000))
+    g = rng.standard_normal((n, n))
+    a = g @ g.T / n + np.eye(n)
+    b = rng.standard_normal(n)
+    x, st = linalg.solve_ir(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
+                            precision="bf16x3", tol=1e-14, spd=True)
+    assert st["converged"] == 1 and berr(a, x.cpu().numpy(), b) <= 1e-14, st
+    a2 = a - 3.0 * np.eye(n)  # indefinite
+    x2, st2 = linalg.solve_ir(torch.from_numpy(a2).cuda(), torch.from_numpy(b).cuda(),
+                              precision="bf16x3", tol=1e-14, spd=True, max_iter=10)
+    assert st2["converged"] == 0
+    assert np.all(np.isfinite(x2.cpu().numpy())) or st2["backward_error"] != st2["backward_error"]
