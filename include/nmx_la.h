@@ -262,6 +262,36 @@ NMX_API int nmx_potrs_f64(nmx_ctx ctx, int64_t n, int64_t nrhs, const double *L,
 NMX_API int nmx_potrs_f32(nmx_ctx ctx, int64_t n, int64_t nrhs, const float *L, int64_t lda,
                           float *B, int64_t ldb, void *stream);
 
+/* ---- what an LU gives besides solves -------------------------------------
+ *
+ * nmx_lu_slogdet_*: from nmx_getrf's packed factor and pivots, out[0] = sign,
+ * out[1] = ln|det|, out[2] = det (device pointer, 3 values; asynchronous):
+ * numax's LU.slogdet / LU.det (numax/linalg/lu.mojo:382-451) -- sign = swap
+ * parity x the signs of U's diagonal, (0, -inf) and det 0 when a diagonal
+ * entry is exactly 0, det = parity x the diagonal multiplied in index order.
+ * nmx_lu_unpack_*: numax's lu -> PLU (numax/linalg/lu.mojo:877-975): A = P L U
+ * with L unit lower, U upper and P[perm[i]][i] = 1, perm the interchanges
+ * replayed on the identity; any of P, L, U may be NULL.
+ * nmx_inverse_*: numax's inverse (numax/linalg/basic.mojo:149-192): X =
+ * A^-1 by one LU of a copy of A (ipiv: n device int32, info as nmx_getrf)
+ * and one solve against the identity; a singular A gives non-finite entries,
+ * as numax's does, with info > 0.
+ */
+NMX_API int nmx_lu_slogdet_f64(nmx_ctx ctx, int64_t n, const double *LU, int64_t lda,
+                               const int32_t *ipiv, double *out, void *stream);
+NMX_API int nmx_lu_slogdet_f32(nmx_ctx ctx, int64_t n, const float *LU, int64_t lda,
+                               const int32_t *ipiv, float *out, void *stream);
+NMX_API int nmx_lu_unpack_f64(nmx_ctx ctx, int64_t n, const double *LU, int64_t lda,
+                              const int32_t *ipiv, double *P, int64_t ldp, double *L, int64_t ldl,
+                              double *U, int64_t ldu, void *stream);
+NMX_API int nmx_lu_unpack_f32(nmx_ctx ctx, int64_t n, const float *LU, int64_t lda,
+                              const int32_t *ipiv, float *P, int64_t ldp, float *L, int64_t ldl,
+                              float *U, int64_t ldu, void *stream);
+NMX_API int nmx_inverse_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, double *X,
+                            int64_t ldx, int32_t *ipiv, int32_t *info, void *stream);
+NMX_API int nmx_inverse_f32(nmx_ctx ctx, int64_t n, const float *A, int64_t lda, float *X,
+                            int64_t ldx, int32_t *ipiv, int32_t *info, void *stream);
+
 /* ---- Householder QR (m >= n) and the thin Q --------------------------------
  *
  * nmx_geqrf_*: factor the m x n row-major A (lda) in place into LAPACK's
@@ -285,6 +315,24 @@ NMX_API int nmx_orgqr_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int
                           const float *tau, float *Q, int64_t ldq, void *stream);
 NMX_API int nmx_orgqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
                           const double *tau, double *Q, int64_t ldq, void *stream);
+/* nmx_ormqr_*: B := Q^T B in place for the m x nrhs row-major B (ldb), Q the
+ * full orthogonal factor of geqrf's output, never formed -- numax's
+ * QR.apply_q_transpose (numax/linalg/qr.mojo:470-530): the panels' block
+ * reflectors in factorization order.  The leading n rows are the thin Q^T B.
+ * nmx_qr_solve_*: x (n) = the least-squares solution of A x ~= b (m) from
+ * geqrf's output -- numax's QR.solve / lstsq (numax/linalg/qr.mojo:532-612):
+ * Q^T b (in `work`, m values, device) then the back substitution with R.
+ * Rank deficiency is not detected, as in numax. */
+NMX_API int nmx_ormqr_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int64_t ldf,
+                          const float *tau, float *B, int64_t ldb, int64_t nrhs, void *stream);
+NMX_API int nmx_ormqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
+                          const double *tau, double *B, int64_t ldb, int64_t nrhs, void *stream);
+NMX_API int nmx_qr_solve_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int64_t ldf,
+                             const float *tau, const float *b, float *x, float *work,
+                             void *stream);
+NMX_API int nmx_qr_solve_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
+                             const double *tau, const double *b, double *x, double *work,
+                             void *stream);
 
 /* ---- the dense factorizations' GEMM ---------------------------------------
  *

@@ -63,9 +63,19 @@ SIGNATURES = {
     "nmx_geqrf_f64": (ci, [vp, i64, i64, vp, i64, vp, vp]),
     "nmx_orgqr_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
     "nmx_orgqr_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),
+    "nmx_ormqr_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, i64, vp]),
+    "nmx_ormqr_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, i64, vp]),
+    "nmx_qr_solve_f32": (ci, [vp, i64, i64, vp, i64, vp, vp, vp, vp, vp]),
+    "nmx_qr_solve_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, vp, vp, vp]),
     "nmx_gesv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
     "nmx_gemm_sub_f32": (ci, [vp, i64, i64, i64, vp, i64, vp, i64, vp, i64, ci, vp]),
     "nmx_gesv_ir_reserve": (ci, [vp, i64, ci]),
+    "nmx_lu_slogdet_f64": (ci, [vp, i64, vp, i64, vp, vp, vp]),
+    "nmx_lu_slogdet_f32": (ci, [vp, i64, vp, i64, vp, vp, vp]),
+    "nmx_lu_unpack_f64": (ci, [vp, i64, vp, i64, vp, vp, i64, vp, i64, vp, i64, vp]),
+    "nmx_lu_unpack_f32": (ci, [vp, i64, vp, i64, vp, vp, i64, vp, i64, vp, i64, vp]),
+    "nmx_inverse_f64": (ci, [vp, i64, vp, i64, vp, i64, vp, vp, vp]),
+    "nmx_inverse_f32": (ci, [vp, i64, vp, i64, vp, i64, vp, vp, vp]),
     "nmx_posv_ir_f64": (ci, [vp, i64, vp, i64, vp, vp, ci, C.c_double, ci, vp, vp]),
     "nmx_posv_ir_reserve": (ci, [vp, i64, ci]),
     "nmx_gemm_f64": (ci, [vp, ci, ci, i64, i64, i64, C.c_double, vp, i64, vp, i64, C.c_double,

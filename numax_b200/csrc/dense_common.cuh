@@ -141,6 +141,11 @@ int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int3
 // The tallest panel the tournament-pivoting leaf takes (dense_lu.cu).
 int64_t tournament_max_rows();
 
+// Rows 0..n-1 of B (ncols columns) interchanged in order as ipiv says
+// (numax's laswp on a right-hand-side block; dense_lu.cu).
+template <typename T>
+void laswp_rows(cudaStream_t st, T *B, int64_t ldb, int n, int ncols, const int32_t *ipiv);
+
 // Recursive lower Cholesky of the n x n row-major A in place (dense_potrf.cu),
 // numax's potrf_diag rule at the leaves, updates through `gs` (its precision
 // sends the FP32 SYRK / triangular-solve products to the tensor cores).  The

@@ -858,6 +858,15 @@ static int getrf_lookahead(LuRun<T> &R, int nb) {
 int64_t tournament_max_rows() { return (int64_t)kCaluMaxCtas * kCaluRows; }
 
 template <typename T>
+void laswp_rows(cudaStream_t st, T *B, int64_t ldb, int n, int ncols, const int32_t *ipiv) {
+    const int threads = 128;
+    laswp_kernel<T><<<(unsigned)ceil_div(ncols, threads), threads, 0, st>>>(B, ldb, ncols, 0, n,
+                                                                          ipiv, 0, 0);
+}
+template void laswp_rows<double>(cudaStream_t, double *, int64_t, int, int, const int32_t *);
+template void laswp_rows<float>(cudaStream_t, float *, int64_t, int, int, const int32_t *);
+
+template <typename T>
 int getrf_run(nmx_ctx ctx, const GemmSub &gs, int64_t n, T *A, int64_t lda, int32_t *ipiv,
               int32_t *info, bool tournament) {
     cudaStream_t st = gs.st;

@@ -422,9 +422,87 @@ static int orgqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, con
     return 0;
 }
 
+// B := Q^T B for the m x nrhs block B (ldb): numax's QR.apply_q_transpose
+// (numax/linalg/qr.mojo:470-530) -- the reflectors in factorization order,
+// each panel through its block reflector (T^T), Q never formed.
+template <typename T>
+static int ormqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, const T *tau, T *B,
+                 int64_t ldb, int64_t nrhs, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(m >= 0 && m < (int64_t(1) << 31), 2, "m out of range");
+    NMX_ARG_CHECK(n >= 0 && n <= m, 3, "need 0 <= n <= m");
+    NMX_ARG_CHECK(F != nullptr || n == 0, 4, "F is NULL");
+    NMX_ARG_CHECK(ldf >= std::max<int64_t>(1, n), 5, "ldf < max(1, n)");
+    NMX_ARG_CHECK(tau != nullptr || n == 0, 6, "tau is NULL");
+    NMX_ARG_CHECK(B != nullptr || nrhs == 0 || m == 0, 7, "B is NULL");
+    NMX_ARG_CHECK(ldb >= std::max<int64_t>(1, nrhs), 8, "ldb < max(1, nrhs)");
+    NMX_ARG_CHECK(nrhs >= 0, 9, "nrhs < 0");
+    if (n == 0 || nrhs == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    QrRun<T> R;
+    NMX_TRY(qr_setup<T>(ctx, st, m, std::max<int64_t>(n, nrhs), R));
+    for (int k = 0; k < n; k += kQrW) {
+        const int w = (int)std::min<int64_t>(kQrW, n - k);
+        const int64_t mk = m - k;
+        pack_v_kernel<T><<<(unsigned)ceil_div(mk * kQrW, 256), 256, 0, st>>>(F, ldf, (int)m, k, w,
+                                                                             R.Vd, nullptr);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, nullptr, R.sc.gram_part));
+        larft_kernel<T><<<1, 256, 0, st>>>(R.sc.gram_part, 1, tau, k, w, R.Tm, 1);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_TRY(apply_reflector<T>(R, k, B, ldb, 0, (int)nrhs));
+    }
+    return 0;
+}
+
+// x = argmin ||A x - b||: numax's QR.solve (numax/linalg/qr.mojo:532-612),
+// Q^T b (into b's copy `work`, m values) then the back substitution with R.
+template <typename T>
+static int qr_solve(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, const T *tau,
+                    const T *b, T *x, T *work, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(m >= 0 && m < (int64_t(1) << 31), 2, "m out of range");
+    NMX_ARG_CHECK(n >= 0 && n <= m, 3, "need 0 <= n <= m");
+    NMX_ARG_CHECK(F != nullptr || n == 0, 4, "F is NULL");
+    NMX_ARG_CHECK(ldf >= std::max<int64_t>(1, n), 5, "ldf < max(1, n)");
+    NMX_ARG_CHECK(tau != nullptr || n == 0, 6, "tau is NULL");
+    NMX_ARG_CHECK(b != nullptr || m == 0, 7, "b is NULL");
+    NMX_ARG_CHECK(x != nullptr || n == 0, 8, "x is NULL");
+    NMX_ARG_CHECK(work != nullptr || m == 0, 9, "work is NULL");
+    if (n == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NMX_CUDA_TRY(cudaMemcpyAsync(work, b, sizeof(T) * (size_t)m, cudaMemcpyDeviceToDevice, st));
+    NMX_TRY(ormqr<T>(ctx, m, n, F, ldf, tau, work, 1, 1, stream));
+    NMX_CUDA_TRY(cudaMemcpyAsync(x, work, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    GemmSub gs;
+    gs.st = st;
+    return trsm_upper<T, false>(gs, F, ldf, 0, (int)n, x, 1, 0, 1);
+}
+
 }  // namespace nmx
 
 extern "C" {
+
+NMX_API int nmx_ormqr_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int64_t ldf,
+                          const float *tau, float *B, int64_t ldb, int64_t nrhs, void *stream) {
+    return nmx::ormqr<float>(ctx, m, n, F, ldf, tau, B, ldb, nrhs, stream);
+}
+NMX_API int nmx_ormqr_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
+                          const double *tau, double *B, int64_t ldb, int64_t nrhs, void *stream) {
+    return nmx::ormqr<double>(ctx, m, n, F, ldf, tau, B, ldb, nrhs, stream);
+}
+NMX_API int nmx_qr_solve_f32(nmx_ctx ctx, int64_t m, int64_t n, const float *F, int64_t ldf,
+                             const float *tau, const float *b, float *x, float *work,
+                             void *stream) {
+    return nmx::qr_solve<float>(ctx, m, n, F, ldf, tau, b, x, work, stream);
+}
+NMX_API int nmx_qr_solve_f64(nmx_ctx ctx, int64_t m, int64_t n, const double *F, int64_t ldf,
+                             const double *tau, const double *b, double *x, double *work,
+                             void *stream) {
+    return nmx::qr_solve<double>(ctx, m, n, F, ldf, tau, b, x, work, stream);
+}
 
 NMX_API int nmx_geqrf_f32(nmx_ctx ctx, int64_t m, int64_t n, float *A, int64_t lda, float *tau,
                           void *stream) {

@@ -76,7 +76,7 @@ struct nmx_context {
     int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the LU (-1: 256, 0: off)
     int64_t tune_lu_panel_sms = -1;   // SMs the look-ahead keeps free of the update GEMMs (-1, 0: none)
     // Grow-only named device buffers, one per use, kept for the context's life.
-    static constexpr int kSlots = 10;
+    static constexpr int kSlots = 11;
     void *slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Returns a device buffer of at least `bytes`, reusing the context's.
@@ -96,7 +96,8 @@ enum WsSlot {
     kWsCalu = 6,
     kWsGemm16Panel = 7,
     kWsWork64 = 8,  // FP64 factors of the refinement's last precision level
-    kWsBest = 9     // the refinement's best iterate
+    kWsBest = 9,    // the refinement's best iterate
+    kWsAux = 10     // inverse's factor copy, PLU's permutation
 };
 }
 

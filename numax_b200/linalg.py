@@ -4,6 +4,10 @@ Mirrors numax's Tensor-tier call surface (numax/linalg/__init__.mojo:323-426):
 
     lu_factor(a) -> LU            numax/linalg/lu.mojo:454-701
     LU.solve(b), LU.det(), LU.slogdet()   numax/linalg/lu.mojo:181-451
+    lu(a) -> (P, L, U), LU.plu()  numax/linalg/lu.mojo:877-975
+    inverse(a)                    numax/linalg/basic.mojo:149-192
+    qr_factor(a) -> QR, QR.r(), QR.q(), QR.apply_q_transpose(b), QR.solve(b), lstsq(a, b)
+                                  numax/linalg/qr.mojo:330-746
     solve(a, b)                   numax/linalg/basic.mojo:55-146
     cholesky(a)                   numax/linalg/cholesky.mojo:233-468
     cholesky_solve(lower, b)      numax/linalg/cholesky.mojo:471-580
@@ -17,7 +21,6 @@ synchronizes before returning, and the raised messages are numax's.
 """
 from __future__ import annotations
 
-import math
 
 import torch
 
@@ -87,17 +90,32 @@ class LU:
         torch.cuda.current_stream(a.device).synchronize()
         return x.reshape(b.shape)
 
+    def _slogdet3(self):
+        a = self.factored
+        out = torch.zeros(3, dtype=a.dtype, device=a.device)
+        _lib.call(f"nmx_lu_slogdet_{_SUF[a.dtype]}", _ctx(a.device), self.n, a.data_ptr(),
+                  max(1, a.stride(0)), self.pivots.data_ptr(), out.data_ptr(), _stream(a.device))
+        return out.cpu().tolist()  # synchronizes
+
     def det(self):
-        """det(A) = sign * prod(diag(U)) (numax/linalg/lu.mojo:382-451)."""
-        return self.sign * torch.prod(torch.diagonal(self.factored)).item()
+        """det(A) = sign * prod(diag(U)) (numax/linalg/lu.mojo:382-403), on the device."""
+        return self._slogdet3()[2]
 
     def slogdet(self):
-        """(sign, log|det|) like numpy.linalg.slogdet."""
-        d = torch.diagonal(self.factored)
-        if bool((d == 0).any()):
-            return 0.0, -math.inf
-        sign = self.sign * (1 if int((d < 0).sum().item()) % 2 == 0 else -1)
-        return float(sign), float(torch.log(torch.abs(d)).sum().item())
+        """(sign, ln|det|), (0, -inf) when singular (numax/linalg/lu.mojo:405-451)."""
+        s, lg, _ = self._slogdet3()
+        return float(s), float(lg)
+
+    def plu(self):
+        """(P, L, U) with A = P L U (numax's lu, numax/linalg/lu.mojo:877-975)."""
+        a = self.factored
+        P, L, U = (torch.empty_like(a) for _ in range(3))
+        if self.n:
+            _lib.call(f"nmx_lu_unpack_{_SUF[a.dtype]}", _ctx(a.device), self.n, a.data_ptr(),
+                      a.stride(0), self.pivots.data_ptr(), P.data_ptr(), P.stride(0),
+                      L.data_ptr(), L.stride(0), U.data_ptr(), U.stride(0), _stream(a.device))
+        torch.cuda.current_stream(a.device).synchronize()
+        return P, L, U
 
 
 def lu_factor(a) -> LU:
@@ -126,6 +144,29 @@ def lu_factor(a) -> LU:
 def solve(a, b):
     """x with a x = b (numax/linalg/basic.mojo:55-146)."""
     return lu_factor(a).solve(b)
+
+
+def lu(a):
+    """(P, L, U) with a = P L U (numax/linalg/lu.mojo:877-975)."""
+    return lu_factor(a).plu()
+
+
+def inverse(a):
+    """a^-1 by one LU and one solve against the identity
+    (numax/linalg/basic.mojo:149-192); a singular a gives non-finite
+    entries, not an error."""
+    _check_matrix("a", a)
+    dev = _resolve_device(a.device)
+    n = a.shape[0]
+    x = torch.empty((n, n), dtype=a.dtype, device=dev)
+    piv = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    if n:
+        A = a.contiguous()
+        _lib.call(f"nmx_inverse_{_SUF[a.dtype]}", _ctx(dev), n, A.data_ptr(), A.stride(0),
+                  x.data_ptr(), x.stride(0), piv.data_ptr(), info.data_ptr(), _stream(dev))
+    torch.cuda.current_stream(dev).synchronize()
+    return x
 
 
 def det(a):
@@ -191,6 +232,40 @@ class QR:
                       f.stride(0), self.taus.data_ptr(), q.data_ptr(), q.stride(0), _stream(f.device))
         torch.cuda.current_stream(f.device).synchronize()
         return q
+
+    def apply_q_transpose(self, b):
+        """Q^T b against the full Q, without forming it (m x k result; its
+        leading n rows are the thin product) -- numax/linalg/qr.mojo:470-530."""
+        f = self.factored
+        x = _as_rhs(b, self.m, f.dtype, f.device)
+        if self.n and x.shape[1]:
+            _lib.call(f"nmx_ormqr_{_SUF[f.dtype]}", _ctx(f.device), self.m, self.n, f.data_ptr(),
+                      f.stride(0), self.taus.data_ptr(), x.data_ptr(), x.stride(0), x.shape[1],
+                      _stream(f.device))
+        torch.cuda.current_stream(f.device).synchronize()
+        return x.reshape(b.shape)
+
+    def solve(self, b):
+        """The least-squares x minimizing ||A x - b|| for a vector b
+        (numax/linalg/qr.mojo:532-612): Q^T b, then R's back substitution."""
+        f = self.factored
+        if b.dim() != 1:
+            raise ValueError("QR.solve takes a vector b")
+        bb = _as_rhs(b, self.m, f.dtype, f.device).reshape(self.m)
+        x = torch.empty(self.n, dtype=f.dtype, device=f.device)
+        work = torch.empty(self.m, dtype=f.dtype, device=f.device)
+        if self.n:
+            _lib.call(f"nmx_qr_solve_{_SUF[f.dtype]}", _ctx(f.device), self.m, self.n,
+                      f.data_ptr(), f.stride(0), self.taus.data_ptr(), bb.data_ptr(),
+                      x.data_ptr(), work.data_ptr(), _stream(f.device))
+        torch.cuda.current_stream(f.device).synchronize()
+        return x
+
+
+def lstsq(a, b):
+    """The least-squares solution of a x ~= b (m >= n) through qr_factor and
+    QR.solve (numax's lstsq over the Tensor tier, numax/linalg/qr.mojo:746)."""
+    return qr_factor(a).solve(b)
 
 
 def qr_factor(a) -> QR:

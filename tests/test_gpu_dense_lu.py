@@ -212,3 +212,60 @@ def test_lu_config_order_8192_lookahead_matches_lapack():
     rcond, _ = sl.lapack.dgecon(lu, np.abs(a).sum(0).max(), norm="1")
     kappa = 1.0 / rcond
     assert rel(x, sl.lu_solve((lu, piv), b)) <= max(1e-12, 16 * np.finfo(float).eps * kappa)
+
+
+@pytest.mark.parametrize("n", [1, 3, 33, 200, 1000])
+def test_lu_det_slogdet_plu_on_device(oracle, n):
+    """LU.det / LU.slogdet / lu -> (P, L, U) from the device entry points
+    against the oracle's restatement of numax's (pivot parity x diagonal,
+    sum of logs, interchanges replayed on the identity) and numpy."""
+    from numax_b200 import linalg
+    rng = np.random.Generator(np.random.PCG64(7000 + n))
+    a = rng.standard_normal((n, n))
+    f = gpu_lu(a)
+    lu, piv, sign, info = oracle.lu_factor(a, block=16, base=16)
+    s, lg = f.slogdet()
+    ws, wl = np.linalg.slogdet(a)
+    assert s == ws and abs(lg - wl) <= 1e-12 * max(1.0, abs(wl))
+    if n <= 200:
+        d = f.det()
+        assert abs(d - oracle.det(lu, sign)) <= 1e-12 * abs(oracle.det(lu, sign))
+    P, L, U = (t.cpu().numpy() for t in linalg.lu(torch.from_numpy(a).cuda()))
+    p, l, u = oracle.plu(lu, piv)
+    np.testing.assert_array_equal(P, p)
+    assert rel(L, l) <= 1e-12 and rel(U, u) <= 1e-12
+    assert np.abs(P @ L @ U - a).max() <= 1e-12 * np.abs(a).max() * n
+
+
+def test_lu_det_slogdet_singular_and_golden():
+    """A singular matrix gives (0, -inf) and det 0 (numax's convention); the
+    exchange matrix's determinant is -1 (numax's fixture)."""
+    from numax_b200 import linalg
+    a = np.array([[1.0, 2.0, 3.0], [2.0, 4.0, 6.0], [1.0, 0.0, 1.0]])
+    f = gpu_lu(a)
+    assert f.slogdet() == (0.0, -np.inf)
+    assert f.det() == 0.0
+    nx = np.load(os.path.join(GOLD, "numax_fixtures.npz"))
+    assert abs(linalg.det(torch.from_numpy(nx["exchange"]).cuda()) + 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("dtype,n", [(np.float64, 1), (np.float64, 5), (np.float64, 64),
+                                     (np.float64, 257), (np.float64, 1500), (np.float32, 300)])
+def test_inverse_matches_numpy(dtype, n):
+    """numax's inverse (one LU, one solve against the identity): A A^-1 = I
+    and agreement with numpy's inverse within the conditioning."""
+    from numax_b200 import linalg
+    rng = np.random.Generator(np.random.PCG64(8000 + n))
+    a = (rng.standard_normal((n, n)) + n ** 0.5 * np.eye(n)).astype(dtype)
+    x = linalg.inverse(torch.from_numpy(a).cuda()).cpu().numpy().astype(np.float64)
+    a64 = a.astype(np.float64)
+    tol = 1e-12 if dtype == np.float64 else 1e-4
+    assert np.abs(a64 @ x - np.eye(n)).max() <= tol * n
+    assert rel(x, np.linalg.inv(a64)) <= tol * 10
+
+
+def test_inverse_singular_is_non_finite():
+    from numax_b200 import linalg
+    a = np.array([[1.0, 2.0], [2.0, 4.0]])
+    x = linalg.inverse(torch.from_numpy(a).cuda()).cpu().numpy()
+    assert not np.all(np.isfinite(x))

@@ -71,3 +71,27 @@ def test_qr_config_262144x256_f32_vs_lapack():
     q = f.q().double()
     eye = torch.eye(n, dtype=torch.float64, device="cuda")
     assert float((q.T @ q - eye).abs().max()) <= 1e-5
+
+
+@pytest.mark.parametrize("dtype,m,n,k", [(np.float64, 300, 33, 5), (np.float64, 2000, 100, 17),
+                                         (np.float32, 4096, 64, 3), (np.float64, 40, 40, 1)])
+def test_qr_apply_q_transpose_and_lstsq(dtype, m, n, k):
+    """numax's QR.apply_q_transpose (Q^T B against the full Q, Q never formed)
+    against LAPACK's full Q, and QR.solve / lstsq against numpy's
+    least-squares solution."""
+    import scipy.linalg as sl
+    from numax_b200 import linalg
+    rng = np.random.Generator(np.random.PCG64(m + 3 * n + k))
+    a = rng.standard_normal((m, n)).astype(dtype)
+    B = rng.standard_normal((m, k)).astype(dtype)
+    f = linalg.qr_factor(torch.from_numpy(a).cuda())
+    got = f.apply_q_transpose(torch.from_numpy(B).cuda()).cpu().numpy().astype(np.float64)
+    qf, _ = sl.qr(a.astype(np.float64), mode="full")
+    # Same reflectors (LAPACK's sign convention), so the full Q agrees.
+    want = qf.T @ B.astype(np.float64)
+    tol = 1e-12 if dtype == np.float64 else 2e-5
+    assert rel(got, want) <= tol
+    b = rng.standard_normal(m).astype(dtype)
+    x = linalg.lstsq(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()).cpu().numpy()
+    xr = np.linalg.lstsq(a.astype(np.float64), b.astype(np.float64), rcond=None)[0]
+    assert rel(x.astype(np.float64), xr) <= (1e-11 if dtype == np.float64 else 1e-4)
