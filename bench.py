@@ -46,10 +46,18 @@ def draw_sizes(count, seed):
     return rng.integers(NMIN, NMAX + 1, size=count).astype(np.int32)
 
 
-def shard(rank, count):
-    """Rank `rank`'s own shard (weak scaling): its matrix sizes and the seed
-    of its data."""
-    return draw_sizes(count, SEED + rank), SEED + 1000 * rank
+def shard(rank, count, world=1):
+    """Rank `rank`'s shard (weak scaling): the job draws world x count sizes
+    and the library's partitioner (nmx_batched_partition, longest processing
+    time first) splits them by predicted cost, every rank computing the same
+    split with no communication.  Returns the rank's sizes and the seed of
+    its data."""
+    if world == 1:
+        return draw_sizes(count, SEED), SEED
+    from numax_b200.batched import partition
+    ns_all = draw_sizes(count * world, SEED)
+    dev_of, _ = partition(ns_all, world, NRHS)
+    return ns_all[dev_of == rank], SEED + 1000 * rank
 
 
 def max_over_ranks(x, world, device):
@@ -622,7 +630,7 @@ def run_ours(args):
     dtype = torch.float64 if args.dtype == "f64" else torch.float32
     esize = 8 if args.dtype == "f64" else 4
 
-    ns, data_seed = shard(rank, args.count)
+    ns, data_seed = shard(rank, args.count, world)
     A, B = make_batch_torch(ns, NRHS, dtype, dev, data_seed)
     L = torch.empty_like(A)
     X = torch.empty_like(B)

@@ -139,6 +139,16 @@ NMX_API int nmx_batched_plan_autotune(nmx_ctx ctx, nmx_batched_plan plan, const 
  * per CTA and CTAs launched; up to max_buckets entries, *nbuckets = count. */
 NMX_API int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *threads,
                                       int32_t *ctas, int max_buckets, int32_t *nbuckets);
+/* Split one ragged batch over `ndev` devices by predicted cost (host only, no
+ * device needed): dev_of[i] receives the device of matrix i, cost_per_dev
+ * (may be NULL) each device's total.  The cost of a matrix is its flops
+ * (n^3/3 + 2 nrhs n^2) plus its n^2-element read and write weighted at the
+ * B200's FP64 / HBM balance; matrices go largest first to the least-loaded
+ * device (longest processing time first, deterministic ties).  Each device
+ * then builds its own plan over its share: no data moves between devices.
+ * No numax counterpart (numax runs on one device). */
+NMX_API int nmx_batched_partition(int64_t count, const int32_t *n_host, int nrhs, int ndev,
+                                  int32_t *dev_of, double *cost_per_dev);
 /* Set the CTA shape of one size bucket (bucket >= 0) or of all (-1) by hand,
  * in place of the default or the autotuner's pick (no numax counterpart):
  * threads 64, 96, 128 or 192 select the packed-triangle kernel, 256 the FP64

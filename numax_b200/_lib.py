@@ -44,6 +44,7 @@ SIGNATURES = {
     "nmx_batched_plan_autotune": (ci, [vp, vp, vp, vp, vp, vp, vp, ci, vp]),
     "nmx_batched_plan_schedule": (ci, [vp, vp, vp, vp, ci, vp]),
     "nmx_batched_plan_set_shape": (ci, [vp, vp, ci, ci]),
+    "nmx_batched_partition": (ci, [i64, vp, ci, ci, vp, vp]),
     "nmx_potrf_potrs_batched_graph_f64": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "nmx_potrf_potrs_batched_graph_f32": (ci, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "nmx_syevj_batched_plan": (ci, [vp, i64, vp, C.POINTER(vp)]),

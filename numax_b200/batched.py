@@ -38,6 +38,19 @@ def ragged_offsets(ns, cols=None) -> np.ndarray:
     return off
 
 
+def partition(ns, ndev: int, nrhs: int = 4):
+    """Split a ragged batch over `ndev` devices by predicted cost (longest
+    processing time first; host only, nmx_batched_partition).  Returns
+    (dev_of, cost_per_dev): the device of each matrix and each device's
+    total predicted cost."""
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    dev_of = np.empty(len(ns), dtype=np.int32)
+    cost = np.empty(ndev, dtype=np.float64)
+    _lib.call("nmx_batched_partition", len(ns), ns.ctypes.data, int(nrhs), int(ndev),
+              dev_of.ctypes.data, cost.ctypes.data)
+    return dev_of, cost
+
+
 def _resolve_device(device) -> torch.device:
     if device is None:
         return torch.device("cuda", torch.cuda.current_device())

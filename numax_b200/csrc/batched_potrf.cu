@@ -1135,6 +1135,45 @@ int nmx_batched_plan_schedule(nmx_batched_plan plan, int32_t *nmax, int32_t *thr
     return 0;
 }
 
+int nmx_batched_partition(int64_t count, const int32_t *n_host, int nrhs, int ndev,
+                          int32_t *dev_of, double *cost_per_dev) {
+    using namespace nmx;
+    NMX_ARG_CHECK(count >= 0 && count < (int64_t(1) << 31), 1, "count out of range");
+    NMX_ARG_CHECK(n_host != nullptr || count == 0, 2, "n_host is NULL");
+    NMX_ARG_CHECK(nrhs >= 0 && nrhs <= kPotrfMaxRhs, 3, "nrhs must be in 0..8");
+    NMX_ARG_CHECK(ndev >= 1 && ndev <= 1024, 4, "ndev must be in 1..1024");
+    NMX_ARG_CHECK(dev_of != nullptr || count == 0, 5, "dev_of is NULL");
+    for (int64_t i = 0; i < count; ++i)
+        NMX_ARG_CHECK(n_host[i] >= 1 && n_host[i] <= kPotrfMaxN, 2, "every n_i must be in 1..128");
+    // Cost of one matrix: its flops (n^3/3 for the factor, 2 nrhs n^2 for the
+    // solves) plus its bytes (n^2 read and written, 8 bytes each) weighted as
+    // flops at the FP64 / HBM balance of the part (about 6 flops a byte).
+    auto cost = [&](int n) {
+        const double d = n;
+        return d * d * d / 3.0 + 2.0 * nrhs * d * d + 6.0 * 16.0 * d * d;
+    };
+    // Longest processing time first: matrices by cost descending (index
+    // ascending among equals, so the split is deterministic), each to the
+    // least-loaded device (lowest index among equals).
+    std::vector<int32_t> order((size_t)count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return n_host[a] > n_host[b]; });
+    std::vector<double> load((size_t)ndev, 0.0);
+    // A min-heap of (load, device) would be O(log ndev) per matrix; ndev is
+    // small, so a linear scan keeps the tie-breaking obvious.
+    for (int32_t i : order) {
+        int best = 0;
+        for (int d = 1; d < ndev; ++d)
+            if (load[d] < load[best]) best = d;
+        dev_of[i] = best;
+        load[best] += cost(n_host[i]);
+    }
+    if (cost_per_dev)
+        for (int d = 0; d < ndev; ++d) cost_per_dev[d] = load[d];
+    return 0;
+}
+
 int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket, int threads) {
     using namespace nmx;
     NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
