@@ -63,6 +63,14 @@ NMX_API int nmx_destroy(nmx_ctx ctx);
 NMX_API const char *nmx_last_error_string(void);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
 NMX_API int nmx_version(void);
+/* Wait for everything enqueued on `stream` (numax's ctx.synchronize(), which
+ * ends every Tensor-tier call: numax/linalg/lu.mojo:677). */
+NMX_API int nmx_synchronize(nmx_ctx ctx, void *stream);
+/* Copy `bytes` from device memory to host memory after the work queued on
+ * `stream`, and wait for it (how a front end reads an `info` word back to
+ * raise numax's message, numax/linalg/cholesky.mojo:385-394). */
+NMX_API int nmx_memcpy_to_host(nmx_ctx ctx, void *dst, const void *src, int64_t bytes,
+                               void *stream);
 /* Per-context tuning knobs, the hook the autotuner writes (0 = automatic):
  *   "lu.leaf_ctas"  CTAs of the cooperative LU leaf panel
  *   "lu.cluster"    cap on the CTAs of the cluster LU leaf (-1 = no cap,

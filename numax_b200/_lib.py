@@ -34,6 +34,8 @@ SIGNATURES = {
     "nmx_destroy": (ci, [vp]),
     "nmx_last_error_string": (C.c_char_p, []),
     "nmx_version": (ci, []),
+    "nmx_synchronize": (ci, [vp, vp]),
+    "nmx_memcpy_to_host": (ci, [vp, vp, vp, i64, vp]),
     "nmx_tune_set": (ci, [vp, C.c_char_p, i64]),
     "nmx_tune_get": (ci, [vp, C.c_char_p, C.POINTER(i64)]),
     "nmx_potrf_potrs_batched_plan": (ci, [vp, ci, i64, vp, ci, C.POINTER(vp)]),

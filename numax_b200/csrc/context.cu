@@ -146,6 +146,26 @@ int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value) {
     return 0;
 }
 
+int nmx_synchronize(nmx_ctx ctx, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    nmx::DeviceGuard g(ctx->device);
+    NMX_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return 0;
+}
+
+int nmx_memcpy_to_host(nmx_ctx ctx, void *dst, const void *src, int64_t bytes, void *stream) {
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(dst != nullptr || bytes == 0, 2, "dst is NULL");
+    NMX_ARG_CHECK(src != nullptr || bytes == 0, 3, "src is NULL");
+    NMX_ARG_CHECK(bytes >= 0, 4, "bytes < 0");
+    if (bytes == 0) return 0;
+    nmx::DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NMX_CUDA_TRY(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost, st));
+    NMX_CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
 int nmx_destroy(nmx_ctx ctx) {
     if (!ctx) return 0;
     {

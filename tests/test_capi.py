@@ -59,3 +59,23 @@ def test_tuning_keys_documented(lib):
     documented = set(re.findall(r'"([a-z_]+\.[a-z_]+)"', block))
     assert accepted and accepted == documented, (accepted, documented)
     assert lib.nmx_tune_set(None, b"lu.lookahead", 256) == -1
+
+
+def test_mojo_shim_binds_only_declared_symbols(lib):
+    """Every C symbol the Mojo binding (mojo/nmx_la.mojo) looks up is declared
+    in the header and exported by the library, and the shim covers every
+    family of entry points numax's gpu=True branches need."""
+    src = open(os.path.join(ROOT, "mojo", "nmx_la.mojo")).read()
+    used = set(re.findall(r'"(nmx_\w+)"', src))
+    declared = set(declared_symbols())
+    assert used <= declared, used - declared
+    assert all(hasattr(lib, n) for n in used)
+    for family in ("nmx_getrf_f64", "nmx_getrs_f64", "nmx_lu_slogdet_f64", "nmx_lu_unpack_f64",
+                   "nmx_inverse_f64", "nmx_potrf_f64", "nmx_potrs_f64", "nmx_geqrf_f32",
+                   "nmx_orgqr_f32", "nmx_ormqr_f32", "nmx_qr_solve_f32", "nmx_gesv_ir_f64",
+                   "nmx_posv_ir_f64", "nmx_potrf_potrs_batched_plan",
+                   "nmx_batched_plan_destroy", "nmx_syevj_batched_plan", "nmx_syevj_plan_destroy",
+                   "nmx_synchronize", "nmx_memcpy_to_host"):
+        assert family in used, family
+    # numax's Cholesky raise text, reproduced verbatim.
+    assert "cholesky: matrix is not positive definite (non-positive pivot at index " in src

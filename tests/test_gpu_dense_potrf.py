@@ -89,3 +89,26 @@ def test_cholesky_config_order_8192_matches_lapack():
     bm = rng.standard_normal((n, 16))
     x = linalg.cholesky_solve(L, torch.from_numpy(bm).cuda()).cpu().numpy()
     assert rel(x, sl.cho_solve((want, True), bm)) <= 1e-12
+
+
+def test_info_readback_for_the_mojo_raise():
+    """The path the Mojo binding takes for numax's raise: nmx_potrf_f64 then
+    nmx_memcpy_to_host of the info word, which names numax's 0-based index
+    (info - 1) of the first non-positive pivot; nmx_synchronize on the
+    stream."""
+    import ctypes as C
+    from numax_b200 import _lib
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    nx = np.load(os.path.join(GOLD, "numax_fixtures.npz"))
+    a = torch.from_numpy(np.ascontiguousarray(nx["later_block"])).cuda()
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    n = a.shape[0]
+    assert lib.nmx_potrf_f64(ctx, n, C.c_void_p(a.data_ptr()), n, C.c_void_p(info.data_ptr()),
+                             C.c_void_p(stream)) == 0
+    host = C.c_int32(-1)
+    assert lib.nmx_memcpy_to_host(ctx, C.byref(host), C.c_void_p(info.data_ptr()), 4,
+                                  C.c_void_p(stream)) == 0
+    assert host.value - 1 == 3  # numax's "non-positive pivot at index 3"
+    assert lib.nmx_synchronize(ctx, C.c_void_p(stream)) == 0
