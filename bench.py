@@ -357,12 +357,11 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
     return out
 
 
-def run_dense(dev, n=8192, nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
+def run_dense(dev, orders=(4096, 8192, 16384), nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
     """The dense factorizations at the single-matrix configs: FP64 LU + 16-RHS
-    solve and FP64 Cholesky + 16-RHS solve at order n, FP32 Householder QR
+    solve and FP64 Cholesky + 16-RHS solve at each order, FP32 Householder QR
     (geqrf, then orgqr) of qr_m x qr_n.  Device time (CUDA events) of one
-    call each after a warm-up call; rates against FP64 37 TF/s and FP32
-    75 TF/s nominal (MEASURED_PEAKS.json has no FP64/FP32 figure)."""
+    call each after a warm-up call; rates in TF/s (LAPACK flop counts)."""
     import torch
     from numax_b200 import _lib
     ctx = _lib.context(dev.index)
@@ -382,39 +381,40 @@ def run_dense(dev, n=8192, nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1)
 
-    out = {"n": n, "nrhs": nrhs}
-    a = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
-    b = torch.randn((n, nrhs), generator=gen, dtype=torch.float64, device=dev)
-    lu, x = torch.empty_like(a), torch.empty_like(b)
-    piv = torch.empty(n, dtype=torch.int32, device=dev)
-    info = torch.empty(1, dtype=torch.int32, device=dev)
+    out = {"nrhs": nrhs, "lu_f64": {}, "cholesky_f64": {}}
+    for n in orders:
+        a = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+        b = torch.randn((n, nrhs), generator=gen, dtype=torch.float64, device=dev)
+        lu, x = torch.empty_like(a), torch.empty_like(b)
+        piv = torch.empty(n, dtype=torch.int32, device=dev)
+        info = torch.empty(1, dtype=torch.int32, device=dev)
 
-    def lu_solve():
-        lu.copy_(a)
-        x.copy_(b)
-        _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(), sp)
-        _lib.call("nmx_getrs_f64", ctx, n, nrhs, lu.data_ptr(), n, piv.data_ptr(), x.data_ptr(),
-                  nrhs, sp)
-    ms = timed(lu_solve)
-    fl = 2 * n ** 3 / 3 + 2 * n * n * nrhs
-    berr = float((b - a @ x).abs().max() / (a.abs().sum(1).max() * x.abs().max() + b.abs().max()))
-    out["lu_f64"] = {"ms": ms, "tflops": fl / ms / 1e9, "fp64_frac_nominal": fl / ms / 1e9 / 37.0,
-                     "backward_error": berr}
-    g = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
-    spd = g @ g.T / n + torch.eye(n, dtype=torch.float64, device=dev)
-    del g
+        def lu_solve():
+            lu.copy_(a)
+            x.copy_(b)
+            _lib.call("nmx_getrf_f64", ctx, n, lu.data_ptr(), n, piv.data_ptr(), info.data_ptr(), sp)
+            _lib.call("nmx_getrs_f64", ctx, n, nrhs, lu.data_ptr(), n, piv.data_ptr(),
+                      x.data_ptr(), nrhs, sp)
+        ms = timed(lu_solve)
+        fl = 2 * n ** 3 / 3 + 2 * n * n * nrhs
+        berr = float((b - a @ x).abs().max() / (a.abs().sum(1).max() * x.abs().max() + b.abs().max()))
+        out["lu_f64"][str(n)] = {"ms": ms, "tflops": fl / ms / 1e9, "backward_error": berr}
+        g = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+        spd = g @ g.T / n + torch.eye(n, dtype=torch.float64, device=dev)
+        del g
 
-    def chol_solve():
-        lu.copy_(spd)
-        x.copy_(b)
-        _lib.call("nmx_potrf_f64", ctx, n, lu.data_ptr(), n, info.data_ptr(), sp)
-        _lib.call("nmx_potrs_f64", ctx, n, nrhs, lu.data_ptr(), n, x.data_ptr(), nrhs, sp)
-    ms = timed(chol_solve)
-    fl = n ** 3 / 3 + 2 * n * n * nrhs
-    berr = float((b - spd @ x).abs().max() / (spd.abs().sum(1).max() * x.abs().max() + b.abs().max()))
-    out["cholesky_f64"] = {"ms": ms, "tflops": fl / ms / 1e9, "fp64_frac_nominal": fl / ms / 1e9 / 37.0,
-                           "backward_error": berr}
-    del a, b, lu, x, spd
+        def chol_solve():
+            lu.copy_(spd)
+            x.copy_(b)
+            _lib.call("nmx_potrf_f64", ctx, n, lu.data_ptr(), n, info.data_ptr(), sp)
+            _lib.call("nmx_potrs_f64", ctx, n, nrhs, lu.data_ptr(), n, x.data_ptr(), nrhs, sp)
+        ms = timed(chol_solve)
+        fl = n ** 3 / 3 + 2 * n * n * nrhs
+        berr = float((b - spd @ x).abs().max() /
+                     (spd.abs().sum(1).max() * x.abs().max() + b.abs().max()))
+        out["cholesky_f64"][str(n)] = {"ms": ms, "tflops": fl / ms / 1e9, "backward_error": berr}
+        del a, b, lu, x, spd
+        torch.cuda.empty_cache()
     q = torch.randn((qr_m, qr_n), generator=gen, dtype=torch.float32, device=dev)
     f = torch.empty_like(q)
     qq = torch.empty_like(q)
@@ -428,9 +428,8 @@ def run_dense(dev, n=8192, nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
     ms_q = timed(lambda: _lib.call("nmx_orgqr_f32", ctx, qr_m, qr_n, f.data_ptr(), qr_n,
                                    tau.data_ptr(), qq.data_ptr(), qr_n, sp))
     orth = float((qq.T.double() @ qq.double() - torch.eye(qr_n, dtype=torch.float64, device=dev)).abs().max())
-    out["qr_f32"] = {"m": qr_m, "n": qr_n, "geqrf_ms": ms, "geqrf_tflops": fl / ms / 1e9,
-                     "fp32_frac_nominal": fl / ms / 1e9 / 75.0, "orgqr_ms": ms_q,
-                     "q_orthogonality_err": orth}
+    out["qr_f32"] = {"m": qr_m, "n": qr_n, "geqrf_ms": ms, "tflops": fl / ms / 1e9,
+                     "orgqr_ms": ms_q, "q_orthogonality_err": orth}
     return out
 
 
@@ -481,13 +480,14 @@ def run_eigh(count, dev, steps=3, tol=1e-7, max_sweeps=20):
     V = torch.empty(plan.a_elems, dtype=torch.float32, device=dev)
     sw = torch.empty(len(ns), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    for _ in range(2):
-        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True)
+    schedule = plan.autotune(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True, reps=2)
+    for _ in range(3):
+        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True, graph=True)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(steps):
-        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True)
+        plan.run(A, W, V, sw, tol=tol, max_sweeps=max_sweeps, sort=True, graph=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / steps
@@ -509,7 +509,35 @@ def run_eigh(count, dev, steps=3, tol=1e-7, max_sweeps=20):
     return {"count": count, "ms": ms, "matrices_per_s": count / (ms / 1e3),
             "mean_sweeps": float(swp.mean()), "max_sweeps": int(swp.max()),
             "max_rel_eig_err_vs_fp64": worst, "flop_rate_tflops": flops / (ms / 1e3) / 1e12,
-            "hbm_gbs": bytes_ / (ms / 1e3) / 1e9}
+            "hbm_gbs": bytes_ / (ms / 1e3) / 1e9, "schedule": schedule,
+            "launch": "CUDA graph of the plan (autotuned shapes)"}
+
+
+def measure_gemm_peaks(dev, n=8192):
+    """FP64 and FP32 (no TF32) GEMM rates of the vendor library at n^3 on this
+    GPU, best of 3: the measured denominators of the FP64 and FP32 roofline
+    fractions (the peak file lists HBM and BF16 only)."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    out = {}
+    try:
+        for name, dt in (("fp64_gemm_tflops", torch.float64), ("fp32_gemm_tflops", torch.float32)):
+            a = torch.randn((n, n), dtype=dt, device=dev)
+            b = torch.randn((n, n), dtype=dt, device=dev)
+            best = float("inf")
+            for _ in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                a @ b
+                e1.record()
+                torch.cuda.synchronize(dev)
+                best = min(best, e0.elapsed_time(e1))
+            out[name] = 2.0 * n ** 3 / best / 1e9
+            del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return out
 
 
 def run_chol_ir(n, kappas, dev, seed=SEED):
@@ -745,11 +773,21 @@ def run_ours(args):
     big_achieved = big_bytes / big_s / 1e9
     traffic = read_traffic()
 
+    gemm_peaks = {}
+    if world == 1 and (args.eigh_count > 0 or args.dense):
+        try:
+            gemm_peaks = measure_gemm_peaks(dev)
+        except Exception as exc:
+            gemm_peaks = {"error": f"{type(exc).__name__}: {exc}"}
+
     eigh = None
     if world == 1 and args.eigh_count > 0:
         try:
             eigh = run_eigh(args.eigh_count, dev)
             eigh["hbm_frac"] = eigh["hbm_gbs"] / float(peaks.get("hbm_gbs", 6650.0))
+            if "fp32_gemm_tflops" in gemm_peaks:
+                eigh["fp32_frac_of_measured_sgemm"] = (eigh["flop_rate_tflops"] /
+                                                       gemm_peaks["fp32_gemm_tflops"])
         except Exception as exc:
             eigh = {"error": f"{type(exc).__name__}: {exc}"}
 
@@ -757,6 +795,13 @@ def run_ours(args):
     if world == 1 and args.dense:
         try:
             dense = run_dense(dev)
+            for leg, key in (("lu_f64", "fp64_gemm_tflops"), ("cholesky_f64", "fp64_gemm_tflops")):
+                if key in gemm_peaks:
+                    for rec in dense[leg].values():
+                        rec["frac_of_measured_gemm"] = rec["tflops"] / gemm_peaks[key]
+            if "fp32_gemm_tflops" in gemm_peaks:
+                dense["qr_f32"]["frac_of_measured_gemm"] = (dense["qr_f32"]["tflops"] /
+                                                            gemm_peaks["fp32_gemm_tflops"])
         except Exception as exc:
             dense = {"error": f"{type(exc).__name__}: {exc}"}
 
@@ -795,6 +840,7 @@ def run_ours(args):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "measured_gemm_peaks": gemm_peaks,
         "eigh": eigh,
         "dense": dense,
         "lu_ir": lu_ir,

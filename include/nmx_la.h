@@ -226,6 +226,26 @@ NMX_API int nmx_syevj_plan_sizes(nmx_syevj_plan plan, int64_t *a_elems, int64_t 
 NMX_API int nmx_syevj_batched_f32(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
                                   float *V, int32_t *sweeps, double tol, int max_sweeps, int sort,
                                   void *stream);
+/* Autotuner (no numax counterpart): times every (threads, group) shape --
+ * a warp per matrix in CTAs of 1, 2, 4 or 8 warps, or a CTA of 64, 128 or
+ * 256 threads per matrix -- on each size bucket with these buffers and
+ * arguments (best of `reps`, CUDA events) and keeps the fastest; then runs
+ * the kept schedule once, so W, V and sweeps hold its result.  Synchronizes. */
+NMX_API int nmx_syevj_plan_autotune(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
+                                    float *V, int32_t *sweeps, double tol, int max_sweeps,
+                                    int sort, int reps, void *stream);
+/* Per bucket (largest n first): its largest n, threads per CTA, threads per
+ * matrix (group) and CTAs launched. */
+NMX_API int nmx_syevj_plan_schedule(nmx_syevj_plan plan, int32_t *nmax, int32_t *threads,
+                                    int32_t *group, int32_t *ctas, int max_buckets,
+                                    int32_t *nbuckets);
+/* nmx_syevj_batched_f32 through a CUDA graph of the plan's launches (counter
+ * reset and one persistent kernel per bucket), captured on an internal
+ * stream the first time these buffers and arguments are seen and replayed on
+ * `stream` after that; an autotune or new arguments re-capture. */
+NMX_API int nmx_syevj_batched_graph_f32(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
+                                        float *V, int32_t *sweeps, double tol, int max_sweeps,
+                                        int sort, void *stream);
 
 /* ---- dense LU with partial pivoting, and its solve ----------------------
  *

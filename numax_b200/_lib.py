@@ -53,6 +53,9 @@ SIGNATURES = {
     "nmx_syevj_plan_destroy": (ci, [vp]),
     "nmx_syevj_plan_sizes": (ci, [vp, C.POINTER(i64), C.POINTER(i64)]),
     "nmx_syevj_batched_f32": (ci, [vp, vp, vp, vp, vp, vp, C.c_double, ci, ci, vp]),
+    "nmx_syevj_plan_autotune": (ci, [vp, vp, vp, vp, vp, vp, C.c_double, ci, ci, ci, vp]),
+    "nmx_syevj_plan_schedule": (ci, [vp, vp, vp, vp, vp, ci, vp]),
+    "nmx_syevj_batched_graph_f32": (ci, [vp, vp, vp, vp, vp, vp, C.c_double, ci, ci, vp]),
     "nmx_potrf_potrs_batched_noalloc_f64": (ci, [vp, i64, vp, ci, vp, vp, vp, vp, vp, vp]),
     "nmx_getrf_f64": (ci, [vp, i64, vp, i64, vp, vp, vp]),
     "nmx_getrf_f32": (ci, [vp, i64, vp, i64, vp, vp, vp]),

@@ -223,9 +223,7 @@ class EighBatch:
                 pass
             self._plan = None
 
-    def run(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
-            sort: bool = False):
-        """Enqueue on the current stream; returns (W, V, sweeps)."""
+    def _outputs(self, A, W, V, sweeps):
         _check_tensor("A", A, torch.float32, self.a_elems, self.device)
         if W is None:
             W = torch.empty(self.w_elems, dtype=torch.float32, device=self.device)
@@ -236,10 +234,38 @@ class EighBatch:
         _check_tensor("W", W, torch.float32, self.w_elems, self.device)
         _check_tensor("V", V, torch.float32, self.a_elems, self.device)
         _check_tensor("sweeps", sweeps, torch.int32, self.count, self.device)
-        _lib.call("nmx_syevj_batched_f32", self._ctx, self._plan, A.data_ptr(), W.data_ptr(),
-                  V.data_ptr(), sweeps.data_ptr(), float(tol), int(max_sweeps), int(bool(sort)),
+        return W, V, sweeps
+
+    def run(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
+            sort: bool = False, graph: bool = False):
+        """Enqueue on the current stream; returns (W, V, sweeps).  graph=True
+        replays a CUDA graph of the plan's launches (captured the first time
+        these buffers and arguments are seen)."""
+        W, V, sweeps = self._outputs(A, W, V, sweeps)
+        fn = "nmx_syevj_batched_graph_f32" if graph else "nmx_syevj_batched_f32"
+        _lib.call(fn, self._ctx, self._plan, A.data_ptr(), W.data_ptr(), V.data_ptr(),
+                  sweeps.data_ptr(), float(tol), int(max_sweeps), int(bool(sort)),
                   _stream_ptr(self.device))
         return W, V, sweeps
+
+    def autotune(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
+                 sort: bool = False, reps: int = 2):
+        """Time every (threads, group) shape per size bucket on these buffers
+        and keep the fastest (synchronizes; the outputs hold the kept
+        schedule's result).  Returns the schedule."""
+        W, V, sweeps = self._outputs(A, W, V, sweeps)
+        _lib.call("nmx_syevj_plan_autotune", self._ctx, self._plan, A.data_ptr(), W.data_ptr(),
+                  V.data_ptr(), sweeps.data_ptr(), float(tol), int(max_sweeps), int(bool(sort)),
+                  int(reps), _stream_ptr(self.device))
+        return self.schedule()
+
+    def schedule(self):
+        """Per size bucket: n_max, threads per CTA, threads per matrix, CTAs."""
+        nmax, thr, grp, ctas = ((C.c_int32 * 8)() for _ in range(4))
+        nb = C.c_int32()
+        _lib.call("nmx_syevj_plan_schedule", self._plan, nmax, thr, grp, ctas, 8, C.byref(nb))
+        return [{"n_max": nmax[i], "threads": thr[i], "group": grp[i], "ctas": ctas[i]}
+                for i in range(nb.value)]
 
     def __call__(self, A, W=None, V=None, sweeps=None, tol: float = 1e-7, max_sweeps: int = 20,
                  sort: bool = False):

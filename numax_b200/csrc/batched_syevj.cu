@@ -236,6 +236,11 @@ struct nmx_syevj_plan_s {
         size_t smem;
     };
     std::vector<Bucket> buckets;
+    // CUDA graph of one run, for the arguments in graph_key.
+    cudaGraphExec_t graph = nullptr;
+    const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+    double graph_tol = -1.0;
+    int graph_max_sweeps = -1, graph_sort = -1;
 };
 
 namespace nmx {
@@ -264,6 +269,60 @@ static int syevj_configure(nmx_ctx ctx, nmx_syevj_plan_s::Bucket &b) {
     int64_t groups = (int64_t)per_sm * ctx->sm_count * (NT / G);
     int64_t work = b.end - b.begin;
     b.grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(work, NT / G), groups / (NT / G)));
+    return 0;
+}
+
+// The (threads, group) shapes a bucket can run with: a warp per matrix
+// (group 32) in CTAs of 1..8 warps, or a whole CTA per matrix.
+static const int kSyevjShapes[][2] = {{128, 32}, {64, 32}, {256, 32}, {32, 32},
+                                      {64, 64}, {128, 128}, {256, 256}};
+
+static int syevj_configure_shape(nmx_ctx ctx, nmx_syevj_plan_s::Bucket &b, int threads, int group) {
+    switch (threads * 1000 + group) {
+#define NMX_SHAPE(NT, G) \
+    case NT * 1000 + G:  \
+        return syevj_configure<NT, G>(ctx, b);
+        NMX_SHAPE(128, 32)
+        NMX_SHAPE(64, 32)
+        NMX_SHAPE(256, 32)
+        NMX_SHAPE(32, 32)
+        NMX_SHAPE(64, 64)
+        NMX_SHAPE(128, 128)
+        NMX_SHAPE(256, 256)
+#undef NMX_SHAPE
+        default:
+            set_error("unsupported eigh shape %d threads / group %d", threads, group);
+            return NMX_ERR_INTERNAL;
+    }
+}
+
+static int syevj_launch(const BatchedSyevjArgs &args, const nmx_syevj_plan_s::Bucket &b,
+                        int *counter, cudaStream_t st) {
+    switch (b.threads * 1000 + b.group) {
+#define NMX_SHAPE(NT, G)                                                                          \
+    case NT * 1000 + G:                                                                           \
+        syevj_batched_kernel<NT, G><<<b.grid, NT, b.smem, st>>>(args, b.begin, b.end, b.nmax, counter); \
+        break;
+        NMX_SHAPE(128, 32)
+        NMX_SHAPE(64, 32)
+        NMX_SHAPE(256, 32)
+        NMX_SHAPE(32, 32)
+        NMX_SHAPE(64, 64)
+        NMX_SHAPE(128, 128)
+        NMX_SHAPE(256, 256)
+#undef NMX_SHAPE
+        default:
+            set_error("unsupported eigh shape %d threads / group %d", b.threads, b.group);
+            return NMX_ERR_INTERNAL;
+    }
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+static int syevj_run(nmx_syevj_plan_s *plan, const BatchedSyevjArgs &args, cudaStream_t st) {
+    NMX_CUDA_TRY(cudaMemsetAsync(plan->d_counters, 0, sizeof(int32_t) * plan->buckets.size(), st));
+    for (size_t bi = 0; bi < plan->buckets.size(); ++bi)
+        NMX_TRY(syevj_launch(args, plan->buckets[bi], plan->d_counters + bi, st));
     return 0;
 }
 
@@ -347,6 +406,7 @@ NMX_API int nmx_syevj_batched_plan(nmx_ctx ctx, int64_t count, const int32_t *n_
 NMX_API int nmx_syevj_plan_destroy(nmx_syevj_plan plan) {
     if (!plan) return 0;
     nmx::DeviceGuard g(plan->device);
+    if (plan->graph) cudaGraphExecDestroy(plan->graph);
     if (plan->dev) cudaFree(plan->dev);
     delete plan;
     return 0;
@@ -375,17 +435,148 @@ NMX_API int nmx_syevj_batched_f32(nmx_ctx ctx, nmx_syevj_plan plan, const float 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     BatchedSyevjArgs args{plan->d_order, plan->d_n, plan->d_aoff, plan->d_woff, A, W, V,
                           sweeps,        tol,       max_sweeps,   sort ? 1 : 0};
-    NMX_CUDA_TRY(cudaMemsetAsync(plan->d_counters, 0, sizeof(int32_t) * plan->buckets.size(), st));
-    for (size_t bi = 0; bi < plan->buckets.size(); ++bi) {
-        const auto &b = plan->buckets[bi];
-        if (b.group == 32)
-            syevj_batched_kernel<128, 32><<<b.grid, 128, b.smem, st>>>(args, b.begin, b.end, b.nmax,
-                                                                       plan->d_counters + bi);
-        else
-            syevj_batched_kernel<128, 128><<<b.grid, 128, b.smem, st>>>(args, b.begin, b.end, b.nmax,
-                                                                        plan->d_counters + bi);
-        NMX_CUDA_TRY(cudaGetLastError());
+    return syevj_run(plan, args, st);
+}
+
+NMX_API int nmx_syevj_plan_autotune(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
+                                    float *V, int32_t *sweeps, double tol, int max_sweeps,
+                                    int sort, int reps, void *stream) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    NMX_ARG_CHECK(A != nullptr || plan->count == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(W != nullptr || plan->count == 0, 4, "W is NULL");
+    NMX_ARG_CHECK(V != nullptr || plan->count == 0, 5, "V is NULL");
+    NMX_ARG_CHECK(tol >= 0.0, 7, "tol must be >= 0");
+    NMX_ARG_CHECK(max_sweeps >= 0 && max_sweeps <= 1000, 8, "max_sweeps must be in 0..1000");
+    NMX_ARG_CHECK(reps >= 1 && reps <= 100, 10, "reps must be in 1..100");
+    if (plan->count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BatchedSyevjArgs args{plan->d_order, plan->d_n, plan->d_aoff, plan->d_woff, A, W, V,
+                          sweeps,        tol,       max_sweeps,   sort ? 1 : 0};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NMX_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        set_error("autotune: event creation failed");
+        return NMX_ERR_CUDA;
     }
+    int rc = 0;
+    for (size_t bi = 0; bi < plan->buckets.size() && !rc; ++bi) {
+        auto best = plan->buckets[bi];
+        float best_ms = 3.4e38f;
+        for (const auto &shape : kSyevjShapes) {
+            auto cand = plan->buckets[bi];
+            if (syevj_configure_shape(ctx, cand, shape[0], shape[1]) != 0) {
+                clear_error();  // a shape that does not fit is skipped
+                continue;
+            }
+            float ms = 3.4e38f;
+            for (int r = 0; r < reps && !rc; ++r) {
+                if (cudaMemsetAsync(plan->d_counters + bi, 0, sizeof(int32_t), st) != cudaSuccess ||
+                    cudaEventRecord(e0, st) != cudaSuccess) {
+                    set_error("autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                    rc = NMX_ERR_CUDA;
+                    break;
+                }
+                rc = syevj_launch(args, cand, plan->d_counters + bi, st);
+                float t = 0.f;
+                if (!rc && (cudaEventRecord(e1, st) != cudaSuccess ||
+                            cudaEventSynchronize(e1) != cudaSuccess ||
+                            cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)) {
+                    set_error("autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                    rc = NMX_ERR_CUDA;
+                }
+                ms = std::min(ms, t);
+            }
+            if (rc) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = cand;
+            }
+        }
+        plan->buckets[bi] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (plan->graph) {
+        cudaGraphExecDestroy(plan->graph);
+        plan->graph = nullptr;
+    }
+    if (rc) return rc;
+    // The last timed runs may have used other shapes: leave the outputs of
+    // the kept schedule.
+    return syevj_run(plan, args, st);
+}
+
+NMX_API int nmx_syevj_plan_schedule(nmx_syevj_plan plan, int32_t *nmax, int32_t *threads,
+                                    int32_t *group, int32_t *ctas, int max_buckets,
+                                    int32_t *nbuckets) {
+    NMX_ARG_CHECK(plan != nullptr, 1, "plan is NULL");
+    NMX_ARG_CHECK(max_buckets >= 0, 6, "max_buckets < 0");
+    const int nb = (int)plan->buckets.size();
+    for (int i = 0; i < nb && i < max_buckets; ++i) {
+        if (nmax) nmax[i] = plan->buckets[i].nmax;
+        if (threads) threads[i] = plan->buckets[i].threads;
+        if (group) group[i] = plan->buckets[i].group;
+        if (ctas) ctas[i] = plan->buckets[i].grid;
+    }
+    if (nbuckets) *nbuckets = nb;
+    return 0;
+}
+
+NMX_API int nmx_syevj_batched_graph_f32(nmx_ctx ctx, nmx_syevj_plan plan, const float *A, float *W,
+                                        float *V, int32_t *sweeps, double tol, int max_sweeps,
+                                        int sort, void *stream) {
+    using namespace nmx;
+    NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
+    NMX_ARG_CHECK(plan != nullptr, 2, "plan is NULL");
+    NMX_ARG_CHECK(A != nullptr || plan->count == 0, 3, "A is NULL");
+    NMX_ARG_CHECK(W != nullptr || plan->count == 0, 4, "W is NULL");
+    NMX_ARG_CHECK(V != nullptr || plan->count == 0, 5, "V is NULL");
+    NMX_ARG_CHECK(tol >= 0.0, 7, "tol must be >= 0");
+    NMX_ARG_CHECK(max_sweeps >= 0 && max_sweeps <= 1000, 8, "max_sweeps must be in 0..1000");
+    if (plan->count == 0) return 0;
+    DeviceGuard g(ctx->device);
+    const void *key[4] = {A, W, V, sweeps};
+    if (!plan->graph || !std::equal(key, key + 4, plan->graph_key) || plan->graph_tol != tol ||
+        plan->graph_max_sweeps != max_sweeps || plan->graph_sort != (sort ? 1 : 0)) {
+        if (plan->graph) {
+            cudaGraphExecDestroy(plan->graph);
+            plan->graph = nullptr;
+        }
+        cudaStream_t cs = nullptr;
+        NMX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        int rc = 0;
+        BatchedSyevjArgs args{plan->d_order, plan->d_n, plan->d_aoff, plan->d_woff, A, W, V,
+                              sweeps,        tol,       max_sweeps,   sort ? 1 : 0};
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            set_error("graph capture: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = NMX_ERR_CUDA;
+        } else {
+            rc = syevj_run(plan, args, cs);
+            cudaError_t e = cudaStreamEndCapture(cs, &graph);
+            if (!rc && e != cudaSuccess) {
+                set_error("graph capture: %s", cudaGetErrorString(e));
+                rc = NMX_ERR_CUDA;
+            }
+        }
+        if (!rc && cudaGraphInstantiate(&plan->graph, graph, 0) != cudaSuccess) {
+            set_error("graph instantiate: %s", cudaGetErrorString(cudaGetLastError()));
+            plan->graph = nullptr;
+            rc = NMX_ERR_CUDA;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (rc) return rc;
+        std::copy(key, key + 4, plan->graph_key);
+        plan->graph_tol = tol;
+        plan->graph_max_sweeps = max_sweeps;
+        plan->graph_sort = sort ? 1 : 0;
+    }
+    NMX_CUDA_TRY(cudaGraphLaunch(plan->graph, static_cast<cudaStream_t>(stream)));
     return 0;
 }
 

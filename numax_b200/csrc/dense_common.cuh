@@ -66,12 +66,6 @@ inline int gemm_sub_bt(cudaStream_t st, int64_t m, int64_t n, int64_t k, const T
     return gemm_cc<T>(st, false, true, m, n, k, T(-1), A, lda, B, ldb, T(1), C, ldc, lower);
 }
 
-#define NMX_TRY(expr)           \
-    do {                        \
-        const int _rc = (expr); \
-        if (_rc) return _rc;    \
-    } while (0)
-
 // Creates the context's look-ahead streams and events on first use.
 int ctx_lookahead_streams(nmx_ctx ctx);
 

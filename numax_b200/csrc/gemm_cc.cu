@@ -64,10 +64,24 @@ struct GemmArgs {
 // A[m lda + k] (TA false) or A[k lda + m]; (k, n) of op(B) is B[k ldb + n]
 // (TB false) or B[n ldb + k].  Thread order follows the contiguous index so
 // that global reads coalesce.
-template <typename T, int BM, int BN, int BK, int NT, bool TA, bool TB>
+// Shared-memory placement of a tile: K-major ([k][m], pitch BM + 4) or
+// M-major ([m][k], pitch BK + 4).  The FP64 kernel keeps each operand in the
+// order its rows arrive from memory (row-major A: M-major; B^T: N-major), so
+// the copies land on consecutive addresses and the fragment reads stay
+// conflict-free either way; the FP32 kernel reads K-major tiles as float4.
+template <int BM, int BK, bool MMAJOR>
+__device__ __forceinline__ int tile_index(int mm, int kk) {
+    return MMAJOR ? mm * (BK + 4) + kk : kk * (BM + 4) + mm;
+}
+template <int BM, int BK, bool MMAJOR>
+__host__ __device__ constexpr int tile_elems() {
+    return MMAJOR ? BM * (BK + 4) : BK * (BM + 4);
+}
+
+template <typename T, int BM, int BN, int BK, int NT, bool TA, bool TB, bool AM = false,
+          bool BN_MAJOR = false>
 __device__ __forceinline__ void load_stage(const GemmArgs<T> &p, int64_t m0, int64_t n0,
                                            int64_t k0, T *As, T *Bs) {
-    constexpr int PA = BM + 4, PB = BN + 4;
     const int tid = threadIdx.x;
 #pragma unroll
     for (int e = tid; e < BM * BK; e += NT) {
@@ -82,10 +96,11 @@ __device__ __forceinline__ void load_stage(const GemmArgs<T> &p, int64_t m0, int
         const int64_t gm = m0 + mm, gk = k0 + kk;
         const bool ok = gm < p.m && gk < p.k;
         const T *src = ok ? (TA ? p.A + gk * p.lda + gm : p.A + gm * p.lda + gk) : p.A;
+        const int si = tile_index<BM, BK, AM>(mm, kk);
         if (sizeof(T) == 8)
-            cp_async8(smem_u32(As + kk * PA + mm), src, ok);
+            cp_async8(smem_u32(As + si), src, ok);
         else
-            cp_async4(smem_u32(As + kk * PA + mm), src, ok);
+            cp_async4(smem_u32(As + si), src, ok);
     }
 #pragma unroll
     for (int e = tid; e < BN * BK; e += NT) {
@@ -100,10 +115,11 @@ __device__ __forceinline__ void load_stage(const GemmArgs<T> &p, int64_t m0, int
         const int64_t gn = n0 + nn, gk = k0 + kk;
         const bool ok = gn < p.n && gk < p.k;
         const T *src = ok ? (TB ? p.B + gn * p.ldb + gk : p.B + gk * p.ldb + gn) : p.B;
+        const int si = tile_index<BN, BK, BN_MAJOR>(nn, kk);
         if (sizeof(T) == 8)
-            cp_async8(smem_u32(Bs + kk * PB + nn), src, ok);
+            cp_async8(smem_u32(Bs + si), src, ok);
         else
-            cp_async4(smem_u32(Bs + kk * PB + nn), src, ok);
+            cp_async4(smem_u32(Bs + si), src, ok);
     }
 }
 
@@ -173,12 +189,13 @@ __device__ __forceinline__ bool tile_skipped(int lower, int64_t m0, int64_t n0) 
 template <int BM, int BN, int WM, int WN, bool TA, bool TB, int KS = 1>
 __global__ void __launch_bounds__(WM *WN * 32 * KS) dgemm_kernel(GemmArgs<double> p) {
     constexpr int BK = 16, STAGES = 3, NT = WM * WN * 32 * KS;
-    constexpr int PA = BM + 4, PB = BN + 4;
+    constexpr bool AM = !TA, BNM = TB;  // M-major A, N-major B (see tile_index)
+    constexpr int SA = tile_elems<BM, BK, AM>(), SB = tile_elems<BN, BK, BNM>();
     constexpr int TM = BM / WM, TN = BN / WN, FM = TM / 8, FN = TN / 8;
     static_assert(KS == 1 || KS == 2 || KS == 4, "K split of 1, 2 or 4 groups");
     extern __shared__ __align__(16) double dsm[];
     double *As = dsm;
-    double *Bs = dsm + STAGES * BK * PA;
+    double *Bs = dsm + STAGES * SA;
     const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
     if (tile_skipped<BM, BN>(p.lower, m0, n0)) return;
     const int warp_all = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -194,8 +211,8 @@ __global__ void __launch_bounds__(WM *WN * 32 * KS) dgemm_kernel(GemmArgs<double
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
         if (s < KT)
-            load_stage<double, BM, BN, BK, NT, TA, TB>(p, m0, n0, (int64_t)s * BK, As + s * BK * PA,
-                                                      Bs + s * BK * PB);
+            load_stage<double, BM, BN, BK, NT, TA, TB, AM, BNM>(p, m0, n0, (int64_t)s * BK,
+                                                               As + s * SA, Bs + s * SB);
         cp_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
@@ -204,19 +221,19 @@ __global__ void __launch_bounds__(WM *WN * 32 * KS) dgemm_kernel(GemmArgs<double
         {
             const int nk = kt + STAGES - 1, s = nk % STAGES;
             if (nk < KT)
-                load_stage<double, BM, BN, BK, NT, TA, TB>(p, m0, n0, (int64_t)nk * BK,
-                                                          As + s * BK * PA, Bs + s * BK * PB);
+                load_stage<double, BM, BN, BK, NT, TA, TB, AM, BNM>(p, m0, n0, (int64_t)nk * BK,
+                                                                   As + s * SA, Bs + s * SB);
             cp_commit();
         }
-        const double *as = As + (kt % STAGES) * BK * PA;
-        const double *bs = Bs + (kt % STAGES) * BK * PB;
+        const double *as = As + (kt % STAGES) * SA;
+        const double *bs = Bs + (kt % STAGES) * SB;
 #pragma unroll
         for (int k4 = 4 * ks; k4 < BK; k4 += 4 * KS) {
             double a[FM], b[FN];
 #pragma unroll
-            for (int i = 0; i < FM; ++i) a[i] = as[(k4 + fk) * PA + wm0 + i * 8 + fr];
+            for (int i = 0; i < FM; ++i) a[i] = as[tile_index<BM, BK, AM>(wm0 + i * 8 + fr, k4 + fk)];
 #pragma unroll
-            for (int j = 0; j < FN; ++j) b[j] = bs[(k4 + fk) * PB + wn0 + j * 8 + fr];
+            for (int j = 0; j < FN; ++j) b[j] = bs[tile_index<BN, BK, BNM>(wn0 + j * 8 + fr, k4 + fk)];
 #pragma unroll
             for (int i = 0; i < FM; ++i)
 #pragma unroll
@@ -366,7 +383,8 @@ __global__ void __launch_bounds__(256) sgemm_kernel(GemmArgs<float> p) {
 template <int BM, int BN, int WM, int WN, bool TA, bool TB, int KS = 1>
 int launch_d(cudaStream_t st, const GemmArgs<double> &p) {
     constexpr int BK = 16, STAGES = 3;
-    constexpr size_t pipe = sizeof(double) * STAGES * BK * ((BM + 4) + (BN + 4));
+    constexpr size_t pipe =
+        sizeof(double) * STAGES * (tile_elems<BM, BK, !TA>() + tile_elems<BN, BK, TB>());
     constexpr size_t red = sizeof(double) * (KS - 1) * BM * BN;
     const size_t smem = pipe > red ? pipe : red;
     auto kern = dgemm_kernel<BM, BN, WM, WN, TA, TB, KS>;

@@ -36,6 +36,13 @@ void clear_error();
         }                                                                               \
     } while (0)
 
+// Propagate a nonzero status.
+#define NMX_TRY(expr)           \
+    do {                        \
+        const int _rc = (expr); \
+        if (_rc) return _rc;    \
+    } while (0)
+
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {
     int prev = -1;

@@ -117,3 +117,39 @@ def test_batched_eigh_rejects_bad_sizes():
     import numax_b200 as nb
     with pytest.raises(nb._lib.NmxError):
         nb.EighBatch(np.array([65], dtype=np.int32))
+
+
+def test_eigh_autotune_and_graph_replay():
+    """The eigh autotuner keeps a valid (threads, group) shape per bucket and
+    leaves correct eigenvalues; a CUDA-graph replay gives bit-identical
+    results to the direct launches and re-captures for new arguments."""
+    import numax_b200 as nb
+    rng = np.random.Generator(np.random.PCG64(77))
+    ns = np.concatenate([np.full(300, 24), rng.integers(16, 65, size=300)]).astype(np.int32)
+    mats = []
+    for n in ns:
+        g = rng.standard_normal((n, n))
+        mats.append(((g + g.T) / 2).astype(np.float32).ravel())
+    A = torch.from_numpy(np.concatenate(mats)).cuda()
+    plan = nb.EighBatch(ns)
+    sched = plan.autotune(A, tol=1e-7, max_sweeps=20, sort=True, reps=1)
+    assert all((s["group"] == 32 or s["group"] == s["threads"]) and s["ctas"] >= 1 for s in sched)
+    W1, V1, sw1 = plan.run(A, tol=1e-7, max_sweeps=20, sort=True)
+    W1, V1 = W1.clone(), V1.clone()
+    torch.cuda.synchronize()
+    off = 0
+    Wh = W1.cpu().numpy()
+    for i, n in enumerate(ns):
+        ref = np.linalg.eigvalsh(mats[i].reshape(n, n).astype(np.float64))
+        assert np.abs(Wh[off:off + n] - ref).max() <= 1e-5 * np.abs(ref).max()
+        off += n
+    Wg = torch.empty_like(W1)
+    Vg = torch.empty_like(V1)
+    swg = torch.empty_like(sw1)
+    for _ in range(2):  # capture, then replay
+        plan.run(A, Wg, Vg, swg, tol=1e-7, max_sweeps=20, sort=True, graph=True)
+        torch.cuda.synchronize()
+        assert torch.equal(Wg, W1) and torch.equal(Vg, V1)
+    plan.run(A, Wg, Vg, swg, tol=1e-7, max_sweeps=3, sort=True, graph=True)  # new argument
+    torch.cuda.synchronize()
+    assert int(swg.max()) <= 3
