@@ -164,6 +164,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def kernel_name(shape, dtype):
+    """The kernel a batched plan's CTA shape code selects."""
+    if shape >= 1000:
+        w = (shape - 1000) // 32
+        return f"potrf_tile_batched_kernel<{w}> (8x8 DMMA tiles, {w} warps per matrix)"
+    return f"potrf_potrs_batched_kernel<{'double' if dtype == 'f64' else 'float'}, {shape}>"
+
+
 def read_traffic():
     """Per-launch DRAM bytes from the committed ncu summary, if any."""
     try:
@@ -701,14 +709,14 @@ def run_ours(args):
     value = job_value(world, len(ns), args.steps, total_s)
 
     # ---- the dominant kernel alone: the n in (96, 128] bucket -------------
-    # (potrf_potrs_batched_kernel<double, 192>, about half of the step), as a
-    # plan over the same sizes with its own seeded data, timed per launch.
+    # (about half of the step), as a plan over the same sizes with its own
+    # seeded data and its autotuned shape, timed per launch.
     ns_big = ns[ns > 96]
     Ab, Bb = make_batch_torch(ns_big, NRHS, dtype, dev, SEED + 77 + 1000 * rank)
     Lb, Xb = torch.empty_like(Ab), torch.empty_like(Bb)
     ib = torch.empty(len(ns_big), dtype=torch.int32, device=dev)
     plan_big = nb.CholeskySolveBatch(ns_big, nrhs=NRHS, dtype=dtype, device=dev)
-    plan_big.autotune(Ab, Bb, Xb, ib, Lb, reps=2)
+    big_shape = plan_big.autotune(Ab, Bb, Xb, ib, Lb, reps=2)[0]["threads"]
     for _ in range(3):
         plan_big.run(Ab, Bb, Xb, ib, Lb)
     barrier()
@@ -827,7 +835,7 @@ def run_ours(args):
                    "schedule": schedule, "launch": "CUDA graph of the plan (autotuned shapes)"},
         "roofline": {"bound": "hbm", "achieved": big_achieved, "peak": peak, "unit": "GB/s",
                      "frac": big_achieved / peak, "traffic": traffic,
-                     "kernel": "potrf_potrs_batched_kernel<double, 192> (n in 97..128)",
+                     "kernel": kernel_name(big_shape, args.dtype) + " (n in 97..128)",
                      "peak_source": peak_src + " (hbm_gbs, MEASURED_PEAKS.json)",
                      "algorithmic_bytes_per_launch": big_bytes, "matrices_per_launch": int(len(ns_big)),
                      "launch_ms": big_s * 1e3,

@@ -28,6 +28,14 @@ from . import _lib
 _DT = {torch.float64: (_lib.NMX_F64, "f64"), torch.float32: (_lib.NMX_F32, "f32")}
 
 
+def tile_shape(warps: int) -> int:
+    """CTA shape code of the FP64 8 x 8 DMMA tile kernel with `warps` (1, 2,
+    4 or 8) warps per matrix, as the schedule reports it."""
+    if warps not in (1, 2, 4, 8):
+        raise ValueError("warps must be 1, 2, 4 or 8")
+    return 1000 + 32 * warps
+
+
 def ragged_offsets(ns, cols=None) -> np.ndarray:
     """Element offsets of a ragged batch: matrix i is n_i x (cols or n_i)."""
     ns = np.asarray(ns, dtype=np.int64)
@@ -161,7 +169,8 @@ class CholeskySolveBatch:
 
     def force_shape(self, threads: int, bucket: int = -1):
         """Fix the CTA shape of one size bucket (or all, bucket = -1): 64, 96,
-        128 or 192 threads (packed-triangle kernel) or 256 (the FP64 kernel on
+        128 or 192 threads (packed-triangle kernel) or tile_shape(w) =
+        1000 + 32 w for w = 1, 2, 4, 8 warps per matrix (the FP64 kernel on
         8 x 8 DMMA tiles).  Returns the schedule."""
         _lib.call("nmx_batched_plan_set_shape", self._ctx, self._plan, int(bucket), int(threads))
         return self.schedule()

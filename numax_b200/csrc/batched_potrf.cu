@@ -736,14 +736,16 @@ static int potrf_threads_for(int nmax) {
     return nmax <= 32 ? 64 : (nmax <= 96 ? 128 : kPotrfBigThreads);
 }
 
-// CTA shape 256 selects the 8 x 8 DMMA tile kernel (FP64 only,
-// batched_potrf_tile.cuh); the others are potrf_potrs_batched_kernel's.
-constexpr int kTileShape = kTileNW * 32;
+// CTA shapes 1032, 1064, 1128 and 1256 (1000 + threads) select the 8 x 8
+// DMMA tile kernel with 1, 2, 4 or 8 warps per matrix (FP64 only,
+// batched_potrf_tile.cuh); 64, 96, 128 and 192 potrf_potrs_batched_kernel.
+static const int kAllShapes[] = {64, 96, 128, 192, kTileShapeBase + 32, kTileShapeBase + 64,
+                                 kTileShapeBase + 128, kTileShapeBase + 256};
 
 // Dynamic shared memory of a CTA shape for a bucket of matrices up to nmax.
 template <typename T>
 static size_t shape_smem(int threads, int nmax, int nrhs) {
-    if (threads == kTileShape) return sizeof(double) * (size_t)tile_smem_doubles(nmax);
+    if (is_tile_shape(threads)) return sizeof(double) * (size_t)tile_smem_doubles(nmax, nrhs);
     return sizeof(T) * (size_t)potrf_smem_elems(nmax, nrhs);
 }
 
@@ -761,14 +763,21 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
         NMX_CASE(128)
         NMX_CASE(192)
 #undef NMX_CASE
-        case kTileShape:
-            if constexpr (sizeof(T) == 8) {
-                potrf_tile_batched_kernel<16><<<b.grid, kTileShape, b.smem, st>>>(args, b.begin, b.end,
-                                                                              b.nmax, counter);
-                break;
-            }
-            set_error("the tile shape is FP64 only");
-            return NMX_ERR_INTERNAL;
+#define NMX_TCASE(WPM)                                                                    \
+    case kTileShapeBase + 32 * WPM:                                                        \
+        if constexpr (sizeof(T) == 8) {                                                    \
+            potrf_tile_batched_kernel<WPM><<<b.grid, 32 * WPM, b.smem, st>>>(args, b.begin, \
+                                                                           b.end, b.nmax,  \
+                                                                           counter);       \
+            break;                                                                         \
+        }                                                                                  \
+        set_error("the tile kernel is FP64 only");                                         \
+        return NMX_ERR_INTERNAL;
+        NMX_TCASE(1)
+        NMX_TCASE(2)
+        NMX_TCASE(4)
+        NMX_TCASE(8)
+#undef NMX_TCASE
         default:
             set_error("unsupported thread count %d", b.threads);
             return NMX_ERR_INTERNAL;
@@ -812,29 +821,45 @@ static int shape_occupancy(nmx_ctx ctx, int threads, size_t smem, int *per_sm) {
         NMX_OCC(128)
         NMX_OCC(192)
 #undef NMX_OCC
-        case kTileShape:
-            if constexpr (sizeof(T) == 8) {
-                NMX_CUDA_TRY(set_max_dynamic_smem(potrf_tile_batched_kernel<16>, ctx));
-                NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    per_sm, potrf_tile_batched_kernel<16>, kTileShape, smem));
-            }
-            break;
+#define NMX_TOCC(WPM)                                                                   \
+    case kTileShapeBase + 32 * WPM:                                                      \
+        if constexpr (sizeof(T) == 8) {                                                  \
+            NMX_CUDA_TRY(set_max_dynamic_smem(potrf_tile_batched_kernel<WPM>, ctx));     \
+            NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                  \
+                per_sm, potrf_tile_batched_kernel<WPM>, 32 * WPM, smem));                \
+        }                                                                                \
+        break;
+        NMX_TOCC(1)
+        NMX_TOCC(2)
+        NMX_TOCC(4)
+        NMX_TOCC(8)
+#undef NMX_TOCC
         default:
             break;
     }
     return 0;
 }
 
+// Default CTA shape of a bucket: for FP64 the tile kernel with 1 warp per
+// matrix up to n = 64, 2 up to 96 and 4 up to 128 (the fastest shapes on a
+// B200 for n ~ U[8, 128] with 4 right-hand sides); for FP32 the
+// packed-triangle kernel.
+template <typename T>
+static int default_shape(int nmax) {
+    if (sizeof(T) == 8) return kTileShapeBase + 32 * (nmax <= 64 ? 1 : (nmax <= 96 ? 2 : 4));
+    return potrf_threads_for(nmax);
+}
+
 template <typename T>
 static int configure_buckets(nmx_ctx ctx, nmx_batched_plan_s *p) {
     for (auto &b : p->buckets) {
-        b.threads = potrf_threads_for(b.nmax);
-        if (!shape_covers(b.threads, b.nmax, p->nrhs)) {
+        b.threads = default_shape<T>(b.nmax);
+        if (!is_tile_shape(b.threads) && !shape_covers(b.threads, b.nmax, p->nrhs)) {
             set_error("internal: %d threads cannot cover n=%d with %d right-hand sides", b.threads,
                       b.nmax, p->nrhs);
             return NMX_ERR_INTERNAL;
         }
-        b.smem = sizeof(T) * (size_t)potrf_smem_elems(b.nmax, p->nrhs);
+        b.smem = shape_smem<T>(b.threads, b.nmax, p->nrhs);
         if (b.smem + 64 > ctx->smem_optin) {
             set_error("bucket nmax=%d needs %zu B of shared memory (> %zu)", b.nmax, b.smem,
                       ctx->smem_optin);
@@ -898,9 +923,9 @@ static int autotune(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const 
     for (size_t bi = 0; bi < plan->buckets.size() && !rc; ++bi) {
         auto best = plan->buckets[bi];
         float best_ms = 3.4e38f;
-        for (int threads : {64, 96, 128, 192, kTileShape}) {
+        for (int threads : kAllShapes) {
             auto cand = plan->buckets[bi];
-            if (threads == kTileShape) {
+            if (is_tile_shape(threads)) {
                 if (sizeof(T) != 8) continue;
             } else if (!shape_covers(threads, cand.nmax, plan->nrhs)) {
                 continue;
@@ -1181,15 +1206,15 @@ int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket, i
     NMX_ARG_CHECK(bucket >= -1 && bucket < (int)plan->buckets.size(), 3,
                   "bucket must be -1 (all) or a bucket index");
     NMX_ARG_CHECK(threads == 64 || threads == 96 || threads == 128 || threads == 192 ||
-                      threads == kTileShape,
-                  4, "threads must be 64, 96, 128, 192 or 256 (the FP64 tile kernel)");
-    NMX_ARG_CHECK(threads != kTileShape || plan->dtype == NMX_F64, 4,
-                  "the 256-thread tile kernel is FP64 only");
+                      is_tile_shape(threads),
+                  4, "threads must be 64, 96, 128, 192, or 1032, 1064, 1128, 1256 (the FP64 tile kernel)");
+    NMX_ARG_CHECK(!is_tile_shape(threads) || plan->dtype == NMX_F64, 4,
+                  "the tile kernel is FP64 only");
     DeviceGuard g(ctx->device);
     for (int bi = 0; bi < (int)plan->buckets.size(); ++bi) {
         if (bucket >= 0 && bi != bucket) continue;
         auto &b = plan->buckets[bi];
-        NMX_ARG_CHECK(threads == kTileShape || shape_covers(threads, b.nmax, plan->nrhs), 4,
+        NMX_ARG_CHECK(is_tile_shape(threads) || shape_covers(threads, b.nmax, plan->nrhs), 4,
                       "that CTA shape cannot cover this bucket's sizes");
         const size_t smem = plan->dtype == NMX_F64 ? shape_smem<double>(threads, b.nmax, plan->nrhs)
                                                    : shape_smem<float>(threads, b.nmax, plan->nrhs);

@@ -1,42 +1,61 @@
-// Batched Cholesky + cho_solve on 8 x 8 DMMA tiles (FP64), a second CTA
-// shape for the plan of batched_potrf.cu: the same work as
+// Batched Cholesky + cho_solve on 8 x 8 DMMA tiles (FP64), the second kernel
+// family of the plan in batched_potrf.cu: the same work as
 // potrf_potrs_batched_kernel (numax's Array-tier cholesky + cholesky_solve,
 // numax/linalg/_array/cholesky.mojo:26-92, per matrix of a ragged batch) in
-// a layout built around mma.sync.m8n8k4.f64.
+// a layout built around mma.sync.m8n8k4.f64, for a group of WPM warps per
+// matrix (one CTA = one group; several CTAs share an SM).
 //
-// A matrix's lower triangle is held in shared memory as 8 x 8 tiles, each
-// stored row-major -- which is exactly the DMMA accumulator layout (lane l
-// owns elements 2l and 2l + 1: row l/4, columns 2(l%4), 2(l%4) + 1) -- so
-// every tile load and store is one conflict-free 16-byte access per lane.
-// The right-hand sides ride as one more tile row: B^T (nrhs <= 8 rows) under
-// the matrix, so the forward substitution y = L^-1 b is the panel solve of
-// that row.  Per 8-column step K:
-//   1. one warp factors the diagonal tile in registers (lane = an element
-//      pair; the column's pivot, its scaling and the rank-1 update move by
-//      shuffles) with numax's rule l_jj = sqrt(guard_nonzero(d, 1e-30)), and
-//      forms W_K = L_KK^-1 in the same loop, off the pivot chain;
-//   2. every tile (I, K) of the panel becomes L_IK = A_IK W_K^T: two DMMAs;
-//      the result is stored as a tile and once more in A-fragment order
-//      (element (m, k) of the k4 step q at [q][lane], lane = 4m + k % 4),
-//      which is also the B-fragment order of L_IK^T;
-//   3. the trailing tiles (I, J), K < J <= I, take A_IJ -= L_IK L_JK^T: two
-//      DMMAs with both operands read in fragment order, conflict-free.
-// The back substitution x = L^-T y runs as X^T = Y^T L^-1 over the stored
-// tiles: for J from the last block up, the warps split the products
-// X^T_I L_IJ (I > J) and one warp applies W_J.
+// Shared memory of a CTA: the lower triangle as 8 x 8 tiles (tile (I, J),
+// J <= I, at slot I(I+1)/2 + J), the right-hand sides as the nrhs rows of B^T
+// (block J: nrhs x 8, row-major) and the inverted pivots 1/l_jj.  Inside a
+// tile, element (r, c) sits at 8r + 2((c/2) ^ g(r)) + c%2 with
+// g(r) = 2((r/2)%2): the column pairs of rows 2, 3, 6, 7 swapped in halves.
+// With that swizzle the three ways a tile is read are all conflict-free
+// shared accesses, with no shuffles and no second copy:
+//   accumulator (lane l: row l/4, columns 2(l%4), 2(l%4)+1, one double2),
+//   A fragment, and B fragment of the transpose (lane l: row l/4, column
+//   4q + l%4),
+//   B fragment (lane l: row 4q + l%4, column l/4).
+// A factored diagonal tile holds L_KK in its lower triangle and the strict
+// lower triangle of W_K = L_KK^-1, transposed, in its upper triangle (the
+// diagonal of W_K is the inverted pivots), so the panel and the back
+// substitution read W_K without recomputing it.
+//
+// Per 8-column step K (two barriers):
+//   1. panel: L_IK = A_IK W_K^T for every tile below the diagonal (two
+//      tiles in flight per warp), and the right-hand sides' block
+//      Y_K = B_K W_K^T (the forward substitution);
+//   2. trailing update A_IJ -= L_IK L_JK^T, K < J <= I, and B_J -= Y_K L_JK^T.
+//      One warp (rotating with K) takes tile (K+1, K+1) first and factors
+//      it right away (the look-ahead: each lane a scalar 8 x 8 Cholesky of
+//      its own copy, then W one column per lane), then a smaller share of the
+//      remaining tiles; the other warps split the rest into contiguous runs,
+//      two tiles in flight at a time.
+// The back substitution X^T = Y^T L^-1 runs right-looking from the last
+// block: X^T_J = S_J W_J, then S_I -= X^T_J L_JI for every I < J, spread
+// over the warps.
 #pragma once
 
 namespace nmx {
 
-constexpr int kTileNW = 8;  // warps per CTA of the tile kernel
+// CTA shapes of the tile kernel in a plan's schedule: 1000 + threads.
+constexpr int kTileShapeBase = 1000;
+// Diagonal-tile factorization, in trailing-tile units, kept off its warp's share.
+constexpr int kTileDiagUnits = 6;
 
-// Shared-memory doubles for matrices with T = ceil(nmax / 8) tile rows:
-// the tile store (lower tiles and the right-hand-side row), the panel in
-// fragment order (reused for X^T in fragment order by the back solve), the
-// diagonal tiles' inverses W_K and the back solve's per-warp partials.
-__host__ __device__ inline int tile_smem_doubles(int nmax) {
+__host__ __device__ inline bool is_tile_shape(int shape) {
+    return shape == kTileShapeBase + 32 || shape == kTileShapeBase + 64 ||
+           shape == kTileShapeBase + 128 || shape == kTileShapeBase + 256;
+}
+
+// Shared-memory doubles for matrices up to nmax with nrhs right-hand sides.
+__host__ __device__ inline int tile_smem_doubles(int nmax, int nrhs) {
     const int T = (nmax + 7) / 8;
-    return (T * (T + 1) / 2 + T) * 64 + (T + 1) * 64 + T * 64 + kTileNW * 64;
+    return T * (T + 1) / 2 * 64 + T * 8 * nrhs + T * 8;
+}
+
+__device__ __forceinline__ int swz(int r, int c) {
+    return 8 * r + 2 * ((c >> 1) ^ (((r >> 1) & 1) << 1)) + (c & 1);
 }
 
 __device__ __forceinline__ void dmma8(double (&c)[2], double a, double b) {
@@ -55,214 +74,403 @@ __device__ __forceinline__ double afrag_of(double v0, double v1, int q, int lane
     return (lane & 1) ? x1 : x0;
 }
 
-template <int TMAX>
-__device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *smem) {
+// Factors, in one warp, the diagonal tile K held (updated) in shared memory.
+// Every lane runs the same scalar 8 x 8 Cholesky on its own register copy of
+// the lower triangle (broadcast reads), so the pivot chain is rsqrt and two
+// FMAs per column with no shuffles (numax's rule
+// l_jj = sqrt(guard_nonzero(d, 1e-30)) as l_jj = g / sqrt(g)).
+// W = L^-1 runs one column per lane.  Stores L_KK (lower triangle of the
+// tile, and global L), W's strict lower triangle transposed into the tile's
+// upper triangle, and the inverted pivots.  Returns the 1-based column of
+// the first pivot d <= 0 among the tile's valid columns, 0 if none.
+__device__ __forceinline__ int factor_diag_tile(double *tile, double *dinv, double *L, int n, int K,
+                                                int lane) {
+    double a[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int p = 0; 2 * p <= i; ++p) {
+            const double2 v = *reinterpret_cast<const double2 *>(tile + swz(i, 2 * p));
+            a[i][2 * p] = v.x;
+            if (2 * p + 1 <= i) a[i][2 * p + 1] = v.y;
+        }
+    const int valid = n - 8 * K;
+    int first = 0;
+    double inv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const double d = a[j][j];
+        if (first == 0 && j < valid && d <= 0.0) first = j + 1;
+        const double g = guard_nonzero(d, 1e-30);
+        inv[j] = rsqrt(g);
+        a[j][j] = g * inv[j];
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i) a[i][j] *= inv[j];
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i)
+#pragma unroll
+            for (int k = j + 1; k <= i; ++k) a[i][k] -= a[i][j] * a[k][j];
+    }
+    // Lane l: column c = l % 8 of W = L^-1 (lanes 8.. repeat it), with
+    // w_j = 0 above the diagonal: w_i = (delta_ic - sum_{j<i} l_ij w_j) / l_ii.
+    const int c = lane & 7;
+    double w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        double sum = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+        for (int j = 0; j < i; ++j) sum -= a[i][j] * w[j];
+        w[i] = sum * inv[i];
+    }
+    __syncwarp();
+    // L's lower triangle (every lane stores the same values), W's strict
+    // lower triangle transposed (lane c: position (c, i) = W[i][c], i > c),
+    // the inverted pivots.
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+#pragma unroll
+        for (int p = 0; 2 * p + 1 <= i; ++p)
+            *reinterpret_cast<double2 *>(tile + swz(i, 2 * p)) = make_double2(a[i][2 * p], a[i][2 * p + 1]);
+        if ((i & 1) == 0) tile[swz(i, i)] = a[i][i];
+    }
+    if (lane < 8) {
+#pragma unroll
+        for (int i = 1; i < 8; ++i)
+            if (i > c) tile[swz(c, i)] = w[i];
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+        *reinterpret_cast<double2 *>(dinv + 8 * K + 2 * p) = make_double2(inv[2 * p], inv[2 * p + 1]);
+    __syncwarp();
+    const int r = lane >> 2, c0 = 2 * (lane & 3);
+    const double2 v = *reinterpret_cast<const double2 *>(tile + swz(r, c0));
+    const int gi = 8 * K + r, gj = 8 * K + c0;
+    if (gi < n) {
+        if (gj <= gi) L[(int64_t)gi * n + gj] = v.x;
+        if (gj + 1 <= gi) L[(int64_t)gi * n + gj + 1] = v.y;
+    }
+    return first;
+}
+
+// Row gi, columns gj and gj + 1 (gj even) of an n-column row-major matrix.
+__device__ __forceinline__ void store_pair(double *M, int n, int gi, int gj, double x0, double x1) {
+    if (gi >= n) return;
+    double *p = M + (int64_t)gi * n + gj;
+    if (gj + 1 < n && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        *reinterpret_cast<double2 *>(p) = make_double2(x0, x1);
+    } else {
+        if (gj < n) p[0] = x0;
+        if (gj + 1 < n) p[1] = x1;
+    }
+}
+
+template <int WPM>
+__device__ __forceinline__ void group_sync() {
+    if (WPM == 1)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+// Roles rotate over the warps so that co-resident CTAs, and the steps of one
+// matrix, spread the serial diagonal work over the SM's schedulers: tile D's
+// diagonal factorization runs in warp (D + off) % WPM, right-hand-side block
+// I of the back substitution in warp (I + off) % WPM, with `off` per CTA.
+template <int WPM>
+__device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *smem, int off,
+                               int *s_info) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int M = WPM - 1;  // WPM is a power of two
     const int n = args.ns[idx], nrhs = args.nrhs;
     const int T = (n + 7) >> 3;
     const double *A = static_cast<const double *>(args.A) + args.a_off[idx];
     double *L = static_cast<double *>(args.L) + args.a_off[idx];
     const double *B = static_cast<const double *>(args.B) + args.b_off[idx];
     double *X = static_cast<double *>(args.X) + args.b_off[idx];
-    const int tri_T = T * (T + 1) / 2;
-    double *TS = smem;                       // (tri_T + T) tiles
-    double *PB = TS + (tri_T + T) * 64;      // (T + 1) tiles, fragment order
-    double *WS = PB + (T + 1) * 64;          // T tiles, row-major
-    double *RED = WS + T * 64;               // kTileNW tiles
-    auto slot = [&](int I, int J) { return I < T ? I * (I + 1) / 2 + J : tri_T + J; };
+    double *TS = smem;                        // T(T+1)/2 tiles, swizzled
+    double *RB = TS + T * (T + 1) / 2 * 64;   // T blocks of nrhs x 8: B^T, Y^T, X^T
+    double *DI = RB + T * 8 * nrhs;           // 8T inverted pivots
+    const int r = lane >> 2, cp = lane & 3;   // accumulator row, column pair
+    auto tile = [&](int I, int J) { return TS + (I * (I + 1) / 2 + J) * 64; };
+    auto rb_afrag = [&](int J, int q) -> double {
+        return r < nrhs ? RB[J * 8 * nrhs + r * 8 + 4 * q + cp] : 0.0;
+    };
 
-    // ---- load: lower tiles of A, and B^T as the last tile row ------------
-    // Element e of the store: tile s = e / 64, (r, c) = ((e % 64) / 8, e % 8).
-    // All copies in flight at once (cp.async); out of range (past n, or above
-    // the diagonal) is zero-filled, and the padded diagonal entries then set
-    // to 1 so that the padding factors to the identity.
-    const int nel = (tri_T + T) * 64;
-    const unsigned ts0 = (unsigned)__cvta_generic_to_shared(TS);
-#pragma unroll 4
-    for (int e = threadIdx.x; e < nel; e += kTileNW * 32) {
-        const int s = e >> 6, r = (e >> 3) & 7, c = e & 7;
-        const double *src = A;
-        bool ok;
-        if (s < tri_T) {
-            int I = (int)((sqrtf(8.f * (float)s + 1.f) - 1.f) * 0.5f);
-            I -= (I * (I + 1)) / 2 > s;
-            I += ((I + 1) * (I + 2)) / 2 <= s;
-            const int J = s - (I * (I + 1)) / 2;
-            const int gi = 8 * I + r, gj = 8 * J + c;
-            ok = gi < n && gj <= gi;
-            if (ok) src = A + (int64_t)gi * n + gj;
-        } else {
-            const int gj = 8 * (s - tri_T) + c;
-            ok = r < nrhs && gj < n;
-            if (ok) src = B + (int64_t)gj * nrhs + r;
+    // ---- load: the lower tiles of A and B^T, all copies in flight ----------
+    // Warp w takes tiles w, w + WPM, ... in slot order; lane l the elements
+    // (l/4, 2(l%4)) and (l/4, 2(l%4) + 1), as one 16-byte copy when the pair
+    // is in range and aligned.  Out of range (past n, or above the diagonal)
+    // is zero-filled.
+    {
+        const unsigned ts0 = (unsigned)__cvta_generic_to_shared(TS);
+        const int ntile = T * (T + 1) / 2;
+        int I = 0, J = warp;
+        while (J > I) {
+            J -= I + 1;
+            ++I;
         }
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(ts0 + 8u * (unsigned)e),
-                     "l"(src), "r"(ok ? 8 : 0)
-                     : "memory");
+        for (int s = warp; s < ntile; s += WPM) {
+            const int gi = 8 * I + r, gj = 8 * J + 2 * cp;
+            const bool ok0 = gi < n && gj <= gi, ok1 = gi < n && gj + 1 <= gi;
+            const double *src = ok0 ? A + (int64_t)gi * n + gj : A;
+            const unsigned dst = ts0 + 8u * (unsigned)(s * 64 + swz(r, 2 * cp));
+            if (ok1 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src)
+                             : "memory");
+            } else {
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                             "r"(ok0 ? 8 : 0)
+                             : "memory");
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst + 8u),
+                             "l"(ok1 ? src + 1 : A), "r"(ok1 ? 8 : 0)
+                             : "memory");
+            }
+            J += WPM;
+            while (J > I) {
+                J -= I + 1;
+                ++I;
+            }
+        }
+        const unsigned rb0 = (unsigned)__cvta_generic_to_shared(RB);
+        for (int e = threadIdx.x; e < T * 8 * nrhs; e += WPM * 32) {
+            const int Jb = e / (8 * nrhs), rem = e - Jb * 8 * nrhs, rr = rem >> 3, cc = rem & 7;
+            const int gj = 8 * Jb + cc;
+            const bool ok = gj < n;
+            const double *src = ok ? B + (int64_t)gj * nrhs + rr : B;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                             rb0 + 8u * (unsigned)e),
+                         "l"(src), "r"(ok ? 8 : 0)
+                         : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x < 8 * T - n) {
-        const int g = n + threadIdx.x, o = g - 8 * (T - 1);
-        TS[slot(T - 1, T - 1) * 64 + 9 * o] = 1.0;
+    group_sync<WPM>();
+    if (warp == (off & M)) {
+        // The padded diagonal entries (at most 7) set to 1 so that the
+        // padding factors to the identity; then the first diagonal tile.
+        if (lane < 8 * T - n) {
+            const int o = n + lane - 8 * (T - 1);
+            tile(T - 1, T - 1)[swz(o, o)] = 1.0;
+        }
+        __syncwarp();
+        const int bad = factor_diag_tile(tile(0, 0), DI, L, n, 0, lane);
+        if (lane == 0) *s_info = bad;
     }
-    int info_local = 0;
-    __syncthreads();
+    group_sync<WPM>();
 
     for (int K = 0; K < T; ++K) {
-        // ---- 1. diagonal tile (warp 0) -------------------------------------
-        if (warp == 0) {
-            double *tile = TS + slot(K, K) * 64;
-            const double2 t = *reinterpret_cast<const double2 *>(tile + 2 * lane);
-            double v0 = t.x, v1 = t.y;
-            const int r = lane >> 2, c0 = 2 * (lane & 3);
-            double w0 = (r == c0) ? 1.0 : 0.0, w1 = (r == c0 + 1) ? 1.0 : 0.0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int src = 4 * j + (j >> 1);
-                const double d = __shfl_sync(0xffffffffu, (j & 1) ? v1 : v0, src);
-                if (lane == 0 && info_local == 0 && 8 * K + j < n && d <= 0.0)
-                    info_local = 8 * K + j + 1;
-                const double g = guard_nonzero(d, 1e-30);
-                const double inv = rsqrt(g);
-                const double ljj = g * inv;
-                // Column j of L: the diagonal entry and the rows below scaled.
-                if (c0 == j) v0 = (r == j) ? ljj : (r > j ? v0 * inv : v0);
-                if (c0 + 1 == j) v1 = (r == j) ? ljj : (r > j ? v1 * inv : v1);
-                const double col = (j & 1) ? v1 : v0;
-                const double lrj = __shfl_sync(0xffffffffu, col, 4 * r + (j >> 1));
-                const double lc0 = __shfl_sync(0xffffffffu, col, 4 * c0 + (j >> 1));
-                const double lc1 = __shfl_sync(0xffffffffu, col, 4 * (c0 + 1) + (j >> 1));
-                if (r > j) {
-                    if (c0 > j && c0 <= r) v0 -= lrj * lc0;
-                    if (c0 + 1 > j && c0 + 1 <= r) v1 -= lrj * lc1;
-                }
-                // W = L^-1 by forward elimination: row j is final once scaled,
-                // then the rows below lose l_rj times it.
-                if (r == j) {
-                    w0 *= inv;
-                    w1 *= inv;
-                }
-                const double wj0 = __shfl_sync(0xffffffffu, w0, 4 * j + (lane & 3));
-                const double wj1 = __shfl_sync(0xffffffffu, w1, 4 * j + (lane & 3));
-                if (r > j) {
-                    w0 -= lrj * wj0;
-                    w1 -= lrj * wj1;
-                }
-            }
-            *reinterpret_cast<double2 *>(tile + 2 * lane) = make_double2(v0, v1);
-            *reinterpret_cast<double2 *>(WS + K * 64 + 2 * lane) = make_double2(w0, w1);
-            // L's diagonal tile: the lower triangle inside the matrix.
-            const int gi = 8 * K + r, gj = 8 * K + c0;
-            if (gi < n) {
-                if (gj <= gi) L[(int64_t)gi * n + gj] = v0;
-                if (gj + 1 <= gi) L[(int64_t)gi * n + gj + 1] = v1;
-            }
-        }
-        __syncthreads();
-        // ---- 2. panel: L_IK = A_IK W_K^T, I = K+1 .. T (T: the RHS row) ---
+        // ---- 1. panel: L_IK = A_IK W_K^T (I = K+1 .. T-1), Y_K = B_K W_K^T ----
         {
-            // B-fragments of W_K^T: element (k = 4q + l%4, n = l/4) = W[l/4][4q + l%4].
-            const double b0 = WS[K * 64 + 8 * (lane >> 2) + (lane & 3)];
-            const double b1 = WS[K * 64 + 8 * (lane >> 2) + 4 + (lane & 3)];
-            for (int I = K + 1 + warp; I <= T; I += kTileNW) {
-                double *tile = TS + slot(I, K) * 64;
-                const double2 t = *reinterpret_cast<const double2 *>(tile + 2 * lane);
-                const double a0 = afrag_of(t.x, t.y, 0, lane), a1 = afrag_of(t.x, t.y, 1, lane);
+            // B-fragment of W_K^T: element (k = 4q + l%4, col l/4) = W[l/4][k]:
+            // below the diagonal in the tile's upper triangle, on it the
+            // inverted pivot, above it zero.
+            const double *tk = tile(K, K);
+            double b[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int k = 4 * q + cp;
+                const double t = tk[swz(k, r)];
+                b[q] = k < r ? t : (k == r ? DI[8 * K + r] : 0.0);
+            }
+            const int prank = (warp - off) & M;
+            for (int I = K + 1 + prank; I < T; I += 2 * WPM) {
+                // Two tiles in flight: both read before either is stored.
+                const bool has_b = I + WPM < T;
+                double *ta = tile(I, K), *tb = tile(has_b ? I + WPM : I, K);
+                const double a0 = ta[swz(r, cp)], a1 = ta[swz(r, 4 + cp)];
+                const double e0 = tb[swz(r, cp)], e1 = tb[swz(r, 4 + cp)];
+                double xa[2] = {0.0, 0.0}, xb[2] = {0.0, 0.0};
+                dmma8(xa, a0, b[0]);
+                dmma8(xb, e0, b[0]);
+                dmma8(xa, a1, b[1]);
+                dmma8(xb, e1, b[1]);
+                *reinterpret_cast<double2 *>(ta + swz(r, 2 * cp)) = make_double2(xa[0], xa[1]);
+                store_pair(L, n, 8 * I + r, 8 * K + 2 * cp, xa[0], xa[1]);
+                if (has_b) {
+                    *reinterpret_cast<double2 *>(tb + swz(r, 2 * cp)) = make_double2(xb[0], xb[1]);
+                    store_pair(L, n, 8 * (I + WPM) + r, 8 * K + 2 * cp, xb[0], xb[1]);
+                }
+            }
+            if (nrhs > 0 && prank == ((T - 1 - K) & M)) {
                 double acc[2] = {0.0, 0.0};
-                dmma8(acc, a0, b0);
-                dmma8(acc, a1, b1);
-                *reinterpret_cast<double2 *>(tile + 2 * lane) = make_double2(acc[0], acc[1]);
-                PB[I * 64 + lane] = afrag_of(acc[0], acc[1], 0, lane);
-                PB[I * 64 + 32 + lane] = afrag_of(acc[0], acc[1], 1, lane);
-                if (I < T) {
-                    const int gi = 8 * I + (lane >> 2), gj = 8 * K + 2 * (lane & 3);
-                    if (gi < n) {
-                        if (gj < n) L[(int64_t)gi * n + gj] = acc[0];
-                        if (gj + 1 < n) L[(int64_t)gi * n + gj + 1] = acc[1];
+                dmma8(acc, rb_afrag(K, 0), b[0]);
+                dmma8(acc, rb_afrag(K, 1), b[1]);
+                if (r < nrhs)
+                    *reinterpret_cast<double2 *>(RB + K * 8 * nrhs + r * 8 + 2 * cp) =
+                        make_double2(acc[0], acc[1]);
+            }
+        }
+        group_sync<WPM>();
+        // ---- 2. trailing update --------------------------------------------
+        // Units: tiles (I, J), K < J <= I < T, in order J ascending, I from J;
+        // unit 0 is (K+1, K+1).
+        const int nt = T - K - 1;
+        if (nt > 0) {
+            const int U = nt * (nt + 1) / 2;
+            // Rank 0 is the warp that factors tile (K+1, K+1).
+            const int rank = (warp - (K + 1 + off)) & M;
+            int u0, u1;  // this warp's run of units 1 .. U-1
+            if (WPM == 1) {
+                u0 = 1;
+                u1 = U;
+            } else {
+                const int c0 = max(0, (U - 1 - kTileDiagUnits * (WPM - 1)) / WPM);
+                constexpr int others = WPM > 1 ? WPM - 1 : 1;
+                const int per = (U - 1 - c0 + others - 1) / others;
+                if (rank == 0) {
+                    u0 = 1;
+                    u1 = 1 + c0;
+                } else {
+                    u0 = min(U, 1 + c0 + (rank - 1) * per);
+                    u1 = min(U, u0 + per);
+                }
+            }
+            if (rank == 0) {
+                // Tile (K+1, K+1) updated first, then factored.
+                const int D = K + 1;
+                const double *td = tile(D, K);
+                double *tc = tile(D, D);
+                const double2 v = *reinterpret_cast<const double2 *>(tc + swz(r, 2 * cp));
+                double acc[2] = {v.x, v.y};
+                dmma8(acc, -td[swz(r, cp)], td[swz(r, cp)]);
+                dmma8(acc, -td[swz(r, 4 + cp)], td[swz(r, 4 + cp)]);
+                *reinterpret_cast<double2 *>(tc + swz(r, 2 * cp)) = make_double2(acc[0], acc[1]);
+                __syncwarp();
+                const int bad = factor_diag_tile(tc, DI, L, n, D, lane);
+                if (lane == 0 && bad && *s_info == 0) *s_info = 8 * D + bad;
+            }
+            if (u0 < u1) {
+                int J = K + 1, I = u0;
+                while (I >= T - J) {
+                    I -= T - J;
+                    ++J;
+                }
+                I += J;
+                for (int u = u0; u < u1; u += 2) {
+                    // Two units in flight: all operands read before either store.
+                    const int Ja = J, Ia = I;
+                    if (++I == T) I = ++J;
+                    const bool has_b = u + 1 < u1;
+                    const int Jb = has_b ? J : Ja, Ib = has_b ? I : Ia;
+                    if (has_b && ++I == T) I = ++J;
+                    const double *pa = tile(Ia, K), *qa = tile(Ja, K);
+                    const double *pb = tile(Ib, K), *qb = tile(Jb, K);
+                    double *ca = tile(Ia, Ja), *cb = tile(Ib, Jb);
+                    const double a0 = pa[swz(r, cp)], a1 = pa[swz(r, 4 + cp)];
+                    const double ba0 = qa[swz(r, cp)], ba1 = qa[swz(r, 4 + cp)];
+                    const double e0 = pb[swz(r, cp)], e1 = pb[swz(r, 4 + cp)];
+                    const double bb0 = qb[swz(r, cp)], bb1 = qb[swz(r, 4 + cp)];
+                    const double2 va = *reinterpret_cast<const double2 *>(ca + swz(r, 2 * cp));
+                    const double2 vb = *reinterpret_cast<const double2 *>(cb + swz(r, 2 * cp));
+                    double xa[2] = {va.x, va.y}, xb[2] = {vb.x, vb.y};
+                    dmma8(xa, -a0, ba0);
+                    dmma8(xb, -e0, bb0);
+                    dmma8(xa, -a1, ba1);
+                    dmma8(xb, -e1, bb1);
+                    *reinterpret_cast<double2 *>(ca + swz(r, 2 * cp)) = make_double2(xa[0], xa[1]);
+                    if (has_b)
+                        *reinterpret_cast<double2 *>(cb + swz(r, 2 * cp)) = make_double2(xb[0], xb[1]);
+                }
+            }
+            // Right-hand sides: B_J -= Y_K L_JK^T, J = K+1 .. T-1, from the last rank down.
+            if (nrhs > 0) {
+                const double y0 = rb_afrag(K, 0), y1 = rb_afrag(K, 1);
+                for (int J = K + 1 + (M - rank); J < T; J += WPM) {
+                    const double *q = tile(J, K);
+                    double *yc = RB + J * 8 * nrhs + r * 8 + 2 * cp;
+                    double acc[2] = {0.0, 0.0};
+                    if (r < nrhs) {
+                        acc[0] = yc[0];
+                        acc[1] = yc[1];
                     }
+                    dmma8(acc, -y0, q[swz(r, cp)]);
+                    dmma8(acc, -y1, q[swz(r, 4 + cp)]);
+                    if (r < nrhs) *reinterpret_cast<double2 *>(yc) = make_double2(acc[0], acc[1]);
                 }
             }
         }
-        __syncthreads();
-        // ---- 3. trailing update: (I, J), K < J <= I <= T ---------------------
-        {
-            int q = 0;
-            for (int J = K + 1; J < T; ++J) {
-                const double bj0 = PB[J * 64 + lane], bj1 = PB[J * 64 + 32 + lane];
-                for (int I = J; I <= T; ++I, ++q) {
-                    if ((q % kTileNW) != warp) continue;
-                    double *tile = TS + slot(I, J) * 64;
-                    const double2 t = *reinterpret_cast<const double2 *>(tile + 2 * lane);
-                    double acc[2] = {t.x, t.y};
-                    dmma8(acc, -PB[I * 64 + lane], bj0);
-                    dmma8(acc, -PB[I * 64 + 32 + lane], bj1);
-                    *reinterpret_cast<double2 *>(tile + 2 * lane) = make_double2(acc[0], acc[1]);
-                }
-            }
-        }
-        __syncthreads();
+        group_sync<WPM>();
     }
-    if (warp == 0 && lane == 0) args.info[idx] = info_local;
+    if (threadIdx.x == 0) args.info[idx] = *s_info;
 
-    // ---- back substitution: X^T_J = (Y^T_J - sum_{I>J} X^T_I L_IJ) W_J --------
+    // ---- back substitution, right-looking: X^T_J = S_J W_J once every block
+    // below has been applied, then S_I -= X^T_J L_JI for I < J.  Block I's S
+    // lives in RB and is only touched by its owner warp, which finishes block
+    // J-1 right after applying X_J to it; one barrier per block.
     if (nrhs > 0) {
-        double *XA = PB;  // X^T_I in A-fragment order
-        for (int J = T - 1; J >= 0; --J) {
-            // Each warp's share of the products, I = J+1+warp, J+1+warp+8, ...
-            double part[2] = {0.0, 0.0};
-            for (int I = J + 1 + warp; I < T; I += kTileNW) {
-                const double *lt = TS + slot(I, J) * 64;
-                // B-fragment of L_IJ: element (k = 4q + l%4, n = l/4).
-                const double b0 = lt[8 * (lane & 3) + (lane >> 2)];
-                const double b1 = lt[8 * (4 + (lane & 3)) + (lane >> 2)];
-                dmma8(part, XA[I * 64 + lane], b0);
-                dmma8(part, XA[I * 64 + 32 + lane], b1);
+        auto finish_block = [&](int J) {
+            double *yj = RB + J * 8 * nrhs + r * 8 + 2 * cp;
+            double s0 = 0.0, s1 = 0.0;
+            if (r < nrhs) {
+                s0 = yj[0];
+                s1 = yj[1];
             }
-            *reinterpret_cast<double2 *>(RED + warp * 64 + 2 * lane) = make_double2(part[0], part[1]);
-            __syncthreads();
-            if (warp == 0) {
-                const double2 y = *reinterpret_cast<const double2 *>(TS + slot(T, J) * 64 + 2 * lane);
-                double s0 = y.x, s1 = y.y;
+            // B-fragment of W_J: element (k = 4q + l%4, col l/4) = W[k][l/4],
+            // below the diagonal at the tile's transposed position.
+            const double *tj = tile(J, J);
+            double x[2] = {0.0, 0.0};
 #pragma unroll
-                for (int w = 0; w < kTileNW; ++w) {
-                    const double2 p = *reinterpret_cast<const double2 *>(RED + w * 64 + 2 * lane);
-                    s0 -= p.x;
-                    s1 -= p.y;
-                }
-                // X^T_J = S W_J: B-fragment of W_J, element (k = 4q + l%4, n = l/4).
-                const double *wt = WS + J * 64;
-                const double b0 = wt[8 * (lane & 3) + (lane >> 2)];
-                const double b1 = wt[8 * (4 + (lane & 3)) + (lane >> 2)];
-                double x[2] = {0.0, 0.0};
-                dmma8(x, afrag_of(s0, s1, 0, lane), b0);
-                dmma8(x, afrag_of(s0, s1, 1, lane), b1);
-                XA[J * 64 + lane] = afrag_of(x[0], x[1], 0, lane);
-                XA[J * 64 + 32 + lane] = afrag_of(x[0], x[1], 1, lane);
-                // X (n x nrhs row-major): X^T element (rhs l/4, row 8J + 2(l%4) + e).
-                const int rr = lane >> 2, gj = 8 * J + 2 * (lane & 3);
-                if (rr < nrhs) {
-                    if (gj < n) X[(int64_t)gj * nrhs + rr] = x[0];
-                    if (gj + 1 < n) X[(int64_t)(gj + 1) * nrhs + rr] = x[1];
-                }
+            for (int q = 0; q < 2; ++q) {
+                const int k = 4 * q + cp;
+                const double t = tj[swz(r, k)];
+                const double w = k > r ? t : (k == r ? DI[8 * J + r] : 0.0);
+                dmma8(x, afrag_of(s0, s1, q, lane), w);
             }
-            __syncthreads();
+            if (r < nrhs) {
+                *reinterpret_cast<double2 *>(yj) = make_double2(x[0], x[1]);
+                const int gj = 8 * J + 2 * cp;
+                if (gj < n) X[(int64_t)gj * nrhs + r] = x[0];
+                if (gj + 1 < n) X[(int64_t)(gj + 1) * nrhs + r] = x[1];
+            }
+        };
+        if (warp == ((T - 1 + off) & M)) finish_block(T - 1);
+        group_sync<WPM>();
+        for (int J = T - 1; J > 0; --J) {
+            const double x0 = -rb_afrag(J, 0), x1 = -rb_afrag(J, 1);
+            // Largest I <= J-1 owned by this warp, then down by WPM.
+            for (int I = J - 1 - ((J - 1 + off - warp) & M); I >= 0; I -= WPM) {
+                const double *t = tile(J, I);
+                double *yi = RB + I * 8 * nrhs + r * 8 + 2 * cp;
+                double acc[2] = {0.0, 0.0};
+                if (r < nrhs) {
+                    acc[0] = yi[0];
+                    acc[1] = yi[1];
+                }
+                // B-fragment of L_JI: element (k = 4q + l%4, col l/4).
+                dmma8(acc, x0, t[swz(cp, r)]);
+                dmma8(acc, x1, t[swz(4 + cp, r)]);
+                if (r < nrhs) *reinterpret_cast<double2 *>(yi) = make_double2(acc[0], acc[1]);
+                if (I == J - 1) finish_block(J - 1);
+            }
+            group_sync<WPM>();
         }
     }
 }
 
-template <int TMAX>
-__global__ void __launch_bounds__(kTileNW * 32, 4)
+// Registers capped so that the shapes meant for small matrices keep many
+// CTAs per SM: 16 one-warp, 8 two-warp, 3 four-warp, 2 eight-warp CTAs.
+template <int WPM>
+__global__ void __launch_bounds__(WPM * 32, WPM == 4 ? 3 : 512 / (WPM * 32))
     potrf_tile_batched_kernel(BatchedPotrfArgs args, int begin, int end, int nmax, int *counter) {
     double *S = reinterpret_cast<double *>(bp_smem);
-    __shared__ int s_item;
+    __shared__ int s_item, s_off, s_info;
+    if (threadIdx.x == 0) {
+        // This CTA's warp slots on the SM (a hint only): co-resident CTAs
+        // start their role rotation at different warps.
+        unsigned wid;
+        asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
+        s_off = (int)(wid / WPM);
+    }
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(counter, 1);
+            s_info = 0;
+        }
         __syncthreads();
-        const int item = begin + s_item;
+        const int item = begin + s_item, off = s_off;
         __syncthreads();
         if (item >= end) break;
-        potrf_tile_one<TMAX>(args, args.order[item], S);
+        potrf_tile_one<WPM>(args, args.order[item], S, off, &s_info);
         __syncthreads();
     }
 }

@@ -147,8 +147,8 @@ def test_batched_autotune_and_graph_replay(oracle):
     X = torch.empty_like(dB)
     info = torch.empty(len(ns), dtype=torch.int32, device="cuda")
     sched = plan.autotune(dA, dB, X, info, L, reps=2)
-    assert len(sched) == 4 and all(s["threads"] in (64, 96, 128, 192, 256) and s["ctas"] >= 1
-                                   for s in sched)
+    assert len(sched) == 4 and all(s["threads"] in (64, 96, 128, 192, 1032, 1064, 1128, 1256)
+                                   and s["ctas"] >= 1 for s in sched)
     torch.cuda.synchronize()
     assert int(info.abs().sum()) == 0
     assert relerr(X.cpu().numpy(), wantX) <= 1e-12
@@ -214,21 +214,57 @@ def test_batched_f32_full_config_vs_oracle_sample(oracle):
     assert worst_x <= 1e-5, worst_x
 
 
-@pytest.mark.parametrize("dtype", [np.float64])
-def test_batched_tile_shape_matches_oracle(oracle, dtype):
-    """The 8 x 8 DMMA tile kernel (CTA shape 256, FP64), forced on every
-    bucket through the autotuner's schedule override, against the oracle on
-    ragged sizes around every tile edge, several right-hand-side counts, and
-    numax's later-block failure (info = 4, NaN where the oracle has NaN)."""
+@pytest.mark.parametrize("threads", [128, 192])
+def test_batched_packed_shape_f64_matches_oracle(oracle, threads):
+    """The packed-triangle kernel forced on FP64 (the plan's default is the
+    tile kernel) against the oracle on ragged sizes that shape covers."""
     import numax_b200 as nb
+    hi = 128 if threads == 192 else 96
+    rng = np.random.Generator(np.random.PCG64(threads))
+    ns = np.array([1, 8, 9, 16, 17, 33, 64, 65, hi] + list(rng.integers(1, hi + 1, size=150)),
+                  dtype=np.int32)
+    nrhs = 4
+    A, B = make_batch(ns, nrhs, np.float64, seed=threads)
+    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float64)
+    assert all(s["threads"] == threads for s in plan.force_shape(threads))
+    gotA, gotX, info = plan(torch.from_numpy(A.copy()).cuda(), torch.from_numpy(B.copy()).cuda())
+    wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, nrhs)
+    ao = oracle.ragged_offsets(ns)
+    gotA, gotX = gotA.cpu().numpy(), gotX.cpu().numpy()
+    assert (info.cpu().numpy() == 0).all()
+    for i, n in enumerate(ns):
+        blk = gotA[ao[i]:ao[i] + n * n].reshape(n, n)
+        assert relerr(np.tril(blk), np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= 1e-12
+    assert relerr(gotX, wantX) <= 1e-12
+
+
+def test_batched_default_shapes_f64():
+    """The FP64 plan's default schedule: the tile kernel, 1 warp per matrix
+    up to n = 64, 2 up to 96, 4 up to 128."""
+    import numax_b200 as nb
+    ns = np.array([20, 50, 90, 120], dtype=np.int32)
+    sched = nb.CholeskySolveBatch(ns, nrhs=4, dtype=torch.float64).schedule()
+    assert [(s["n_max"], s["threads"]) for s in sched] == [(120, 1128), (90, 1064), (50, 1032),
+                                                          (20, 1032)]
+
+
+@pytest.mark.parametrize("warps", [1, 2, 4, 8])
+def test_batched_tile_shape_matches_oracle(oracle, warps):
+    """The 8 x 8 DMMA tile kernel (FP64) with 1, 2, 4 and 8 warps per matrix,
+    forced on every bucket through the schedule override, against the oracle
+    on ragged sizes around every tile edge, several right-hand-side counts,
+    and numax's later-block failure (info = 4, NaN where the oracle has NaN)."""
+    import numax_b200 as nb
+    shape = nb.batched.tile_shape(warps)
+    dtype = np.float64
     edge = [1, 2, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65, 95, 96, 97, 120, 127, 128]
-    rng = np.random.Generator(np.random.PCG64(256))
+    rng = np.random.Generator(np.random.PCG64(256 + warps))
     for nrhs in (0, 1, 4, 8):
         ns = np.array(edge + list(rng.integers(1, 129, size=120)), dtype=np.int32)
         rng.shuffle(ns)
         A, B = make_batch(ns, nrhs, dtype, seed=nrhs + 40)
         plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float64)
-        plan.force_shape(256)
+        assert all(s["threads"] == shape for s in plan.force_shape(shape))
         dA = torch.from_numpy(A.copy()).cuda()
         dB = torch.from_numpy(B.copy()).cuda() if nrhs else None
         gotA, gotX, info = plan(dA, dB)
@@ -254,7 +290,7 @@ def test_batched_tile_shape_matches_oracle(oracle, dtype):
     A = np.concatenate([goodA[:400], bad, goodA[400:]])
     B = np.concatenate([goodB[:40], np.ones(8), goodB[40:]])
     plan = nb.CholeskySolveBatch(ns, nrhs=2, dtype=torch.float64)
-    plan.force_shape(256)
+    plan.force_shape(shape)
     gotA, gotX, info = plan(torch.from_numpy(A.copy()).cuda(), torch.from_numpy(B.copy()).cuda())
     assert list(info.cpu().numpy()) == [0, 4, 0]
     wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, 2)
