@@ -857,6 +857,42 @@ def run_ours(args):
     return 0
 
 
+def run_big_bucket(args):
+    """The n in 97..128 bucket of this rank's shard alone, the plan's default
+    schedule (no autotuning), `warmup` untimed and `steps` timed launches; one
+    JSON line with the mean launch time.  Used to profile the dominant kernel."""
+    import torch
+    import numax_b200 as nb
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    ns, seed = shard(0, args.count, 1)
+    ns_big = ns[ns > 96]
+    A, B = make_batch_torch(ns_big, NRHS, dtype, dev, seed + 77)
+    L, X = torch.empty_like(A), torch.empty_like(B)
+    info = torch.empty(len(ns_big), dtype=torch.int32, device=dev)
+    plan = nb.CholeskySolveBatch(ns_big, nrhs=NRHS, dtype=dtype, device=dev)
+    for _ in range(max(args.warmup, 1)):
+        plan.run(A, B, X, info, L)
+    stream = torch.cuda.current_stream(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    for e0, e1 in ev:
+        e0.record(stream)
+        plan.run(A, B, X, info, L)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    esize = 8 if args.dtype == "f64" else 4
+    byt = algorithmic_bytes(ns_big, NRHS, esize)
+    print(json.dumps({"bucket": "n in 97..128", "matrices": int(len(ns_big)),
+                      "schedule": plan.schedule(), "launch_ms": ms,
+                      "algorithmic_bytes_per_launch": byt, "achieved_gbs": byt / ms / 1e6,
+                      "info_nonzero": int((info != 0).sum())}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -881,9 +917,14 @@ def main():
                     help="skip the dense LU/Cholesky/QR leg")
     ap.add_argument("--eigh-count", type=int, default=65536,
                     help="matrices in the batched Jacobi eigh leg (0 skips it)")
+    ap.add_argument("--only-big", action="store_true",
+                    help="run only the n in 97..128 bucket of the batch (the dominant kernel), "
+                         "default schedule, for profiling")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_big:
+        return run_big_bucket(args)
     if args.only_dense:
         import torch
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
