@@ -32,8 +32,9 @@
 //      remaining tiles; the other warps split the rest into contiguous runs,
 //      two tiles in flight at a time.
 // The back substitution X^T = Y^T L^-1 runs right-looking from the last
-// block: X^T_J = S_J W_J, then S_I -= X^T_J L_JI for every I < J, spread
-// over the warps.
+// block: X^T_J = S_J W_J (as X_J = W_J^T S_J^T, so both operands come from
+// shared memory in fragment order), then S_I -= X^T_J L_JI for every I < J,
+// spread over the warps.
 #pragma once
 
 namespace nmx {
@@ -41,7 +42,7 @@ namespace nmx {
 // CTA shapes of the tile kernel in a plan's schedule: 1000 + threads.
 constexpr int kTileShapeBase = 1000;
 // Diagonal-tile factorization, in trailing-tile units, kept off its warp's share.
-constexpr int kTileDiagUnits = 6;
+constexpr int kTileDiagUnits = 20;
 
 __host__ __device__ inline bool is_tile_shape(int shape) {
     return shape == kTileShapeBase + 32 || shape == kTileShapeBase + 64 ||
@@ -399,28 +400,31 @@ __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *sm
     // J-1 right after applying X_J to it; one barrier per block.
     if (nrhs > 0) {
         auto finish_block = [&](int J) {
-            double *yj = RB + J * 8 * nrhs + r * 8 + 2 * cp;
-            double s0 = 0.0, s1 = 0.0;
-            if (r < nrhs) {
-                s0 = yj[0];
-                s1 = yj[1];
-            }
-            // B-fragment of W_J: element (k = 4q + l%4, col l/4) = W[k][l/4],
-            // below the diagonal at the tile's transposed position.
+            // X_J = W_J^T S_J^T (8 x nrhs): A = W_J^T, element (m = l/4,
+            // k = 4q + l%4) = W[k][m], below W's diagonal at the tile's
+            // transposed position (m, k); B = S_J^T, element (k, rhs l/4),
+            // read from RB row-major.  No shuffles.
+            __syncwarp();
             const double *tj = tile(J, J);
+            double *yj = RB + J * 8 * nrhs;
             double x[2] = {0.0, 0.0};
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int k = 4 * q + cp;
                 const double t = tj[swz(r, k)];
-                const double w = k > r ? t : (k == r ? DI[8 * J + r] : 0.0);
-                dmma8(x, afrag_of(s0, s1, q, lane), w);
+                const double wa = k > r ? t : (k == r ? DI[8 * J + r] : 0.0);
+                dmma8(x, wa, rb_afrag(J, q));
             }
-            if (r < nrhs) {
-                *reinterpret_cast<double2 *>(yj) = make_double2(x[0], x[1]);
-                const int gj = 8 * J + 2 * cp;
-                if (gj < n) X[(int64_t)gj * nrhs + r] = x[0];
-                if (gj + 1 < n) X[(int64_t)(gj + 1) * nrhs + r] = x[1];
+            __syncwarp();
+            // Lane (row r, rhs 2cp and 2cp + 1): X^T back into RB, X to global.
+            const int gj = 8 * J + r;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int h = 2 * cp + e;
+                if (h < nrhs) {
+                    yj[h * 8 + r] = x[e];
+                    if (gj < n) X[(int64_t)gj * nrhs + h] = x[e];
+                }
             }
         };
         if (warp == ((T - 1 + off) & M)) finish_block(T - 1);
