@@ -9,9 +9,11 @@
 //
 // Here the panel is a cooperative kernel over every SM: each CTA keeps its
 // share of the panel's rows in shared memory; per column, one grid barrier
-// reduces the column norm (every CTA sums the same partials in the same
-// order, so all agree on beta and tau), a second reduces the dot products
-// with the remaining panel columns.  The same pass accumulates the panel's
+// reduces, in one vector, the dot products of the new reflector with the
+// remaining panel columns and the pieces of the next column's norm (every
+// CTA sums the same partials in the same order, so all agree on beta and
+// tau); the norm is downdated from them, with an exact recompute when
+// cancellation would cost accuracy.  The same pass accumulates the panel's
 // Gram matrix V^T V for T and writes V densely (unit diagonal, zeros above)
 // for the GEMMs.  numax's reflector convention is kept exactly:
 // beta = -sign(alpha) ||x|| (alpha <= 0 gives +||x||), tau = (beta-alpha)/beta,
@@ -23,68 +25,176 @@
 namespace nmx {
 
 constexpr int kQrW = 16;  // panel width (numax's default block)
-constexpr int kQrThreads = 256;
+constexpr int kQrThreads = 512;
+
+// Per-CTA partial vector of one reduction round of the panel: [0, 16) the
+// dot products v^T a_c with the panel's remaining columns, then the pieces of
+// the next column's norm below its diagonal (S_aa = sum a^2, S_av = sum v a,
+// S_vv = sum v^2 over the rows below the next diagonal), and that column's
+// diagonal entry and v there (from the CTA that owns the row).
+// Then [21, 37): the Gram column of the new reflector, v_i^T v_j for i < j.
+constexpr int kQrVec = 37;
+constexpr int kQrSaa = 16, kQrSav = 17, kQrSvv = 18, kQrA1 = 19, kQrV1 = 20, kQrGram = 21;
+constexpr int kQrSub = 12;    // sub-sums per element of the cross-CTA sum
+constexpr int kQrMaxG = 192;  // most CTAs of the panel kernel
+constexpr int kQrPart = kQrMaxG;  // partials stored element-major: [kQrVec][kQrMaxG]
+// The next column's norm is downdated from the sums above (one grid barrier
+// per column); it is recomputed exactly, with one more barrier, when the
+// downdated value is below this fraction of the magnitude of its terms.
+constexpr double kQrDowndateTol = 0.5;
 
 template <typename T>
 struct QrScratch {
-    T *part;        // [2][G][kQrW + 1] per-CTA partial sums (double-buffered)
-    T *alpha;       // [2] a[col][col] published by its owner
-    T *gram_part;   // [G][kQrW * kQrW]
+    T *part;        // [2][kQrVec][kQrPart] per-CTA partials (double-buffered)
+    T *gram_part;   // [kQrW * kQrW]: V^T V for larft_kernel
     unsigned *bar;
     int *err;
 };
 
+// T of the block reflector (w x w upper triangular) from the strict upper
+// Gram entries g[p][i] = v_p^T v_i and the taus, numax's larft
+// (numax/linalg/panel.mojo:2076-2169): t_ii = tau_i and
+// t[q][i] = sum_{q<=r<i} t[q][r] (-tau_i g[r][i]), column by column, the rows
+// q of a column in parallel.  One warp (lanes 0..w-1 do the rows).
 template <typename T>
-__device__ __forceinline__ T block_sum(T v, T *red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+__device__ void build_t(const T (*g)[kQrW], const T *taus, int w, T (*t)[kQrW]) {
+    const int q = threadIdx.x & 31;
+    for (int e = q; e < kQrW * kQrW; e += 32) t[e / kQrW][e % kQrW] = T(0);
+    __syncwarp();
+    for (int i = 0; i < w; ++i) {
+        if (q < i) t[q][i] = -taus[i] * g[q][i];
+        __syncwarp();
+        T sum = T(0);
+        if (q < i)
+            for (int r = q; r < i; ++r) sum += t[q][r] * t[r][i];
+        __syncwarp();
+        if (q < i) t[q][i] = sum;
+        if (q == i) t[i][i] = taus[i];
+        __syncwarp();
+    }
+}
+
+// Tm = T or T^T (kQrW x kQrW, zero outside w x w), by one warp.
+template <typename T>
+__device__ void store_t(const T (*t)[kQrW], int transposed, T *Tm) {
+    for (int e = threadIdx.x & 31; e < kQrW * kQrW; e += 32) {
+        const int p = e / kQrW, q = e - p * kQrW;
+        Tm[e] = transposed ? t[q][p] : t[p][q];
+    }
+}
+
+// One reduction round: this CTA's partial vector p (per thread) is summed
+// over the block and published, then after the grid barrier every CTA sums
+// all CTAs' vectors in the same fixed order (so all agree bit for bit) into
+// tot.  Returns false if the barrier gave up.
+template <typename T>
+__device__ __forceinline__ bool reduce_round(T (&p)[kQrVec], QrScratch<T> &sc, unsigned &gen,
+                                             T *wred, T *sub, T *tot, int *s_flag) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, G = gridDim.x;
+#pragma unroll
+    for (int i = 0; i < kQrVec; ++i) {
+        T v = p[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) wred[warp * kQrVec + i] = v;
+    }
     __syncthreads();
-    if (lane == 0) red[warp] = v;
+    T *slot = sc.part + (size_t)(gen & 1) * kQrVec * kQrPart;
+    if (threadIdx.x < kQrVec) {
+        T t = T(0);
+#pragma unroll
+        for (int w = 0; w < kQrThreads / 32; ++w) t += wred[w * kQrVec + threadIdx.x];
+        slot[(size_t)threadIdx.x * kQrPart + blockIdx.x] = t;
+    }
+    if (!grid_barrier(sc.bar, gen++, (unsigned)G, sc.err, s_flag)) return false;
+    if (threadIdx.x < kQrVec * kQrSub) {
+        // All of this thread's loads in flight at once, then summed in order.
+        constexpr int kPer = (kQrMaxG + kQrSub - 1) / kQrSub;
+        const int i = threadIdx.x / kQrSub, s = threadIdx.x - i * kQrSub;
+        const T *src = slot + (size_t)i * kQrPart;
+        T v[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int g = s + u * kQrSub;
+            v[u] = g < G ? __ldcg(src + g) : T(0);
+        }
+        T acc = T(0);
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) acc += v[u];
+        sub[i * kQrSub + s] = acc;
+    }
     __syncthreads();
-    T t = T(0);
-    for (int w = 0; w < kQrThreads / 32; ++w) t += red[w];
-    return t;
+    if (threadIdx.x < kQrVec) {
+        T acc = T(0);
+#pragma unroll
+        for (int q = 0; q < kQrSub; ++q) acc += sub[threadIdx.x * kQrSub + q];
+        tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    return true;
 }
 
 // Factor panel columns [k, k+w) over rows [k, m) in place; Vd receives V
-// (rows [k, m) x w, row-major ld kQrW) and tau[k..k+w) the scales.
+// (rows [k, m) x w, row-major ld kQrW) and tau[k..k+w) the scales.  One
+// reduction round (one grid barrier) per column: the round after column j's
+// reflector carries its dot products with the remaining panel columns and
+// the pieces of column j+1's norm, which every CTA then downdates itself.
 template <typename T>
-__global__ void __launch_bounds__(kQrThreads)
+__global__ void __launch_bounds__(kQrThreads, 1)
     geqr2_coop_kernel(T *A, int64_t lda, int m, int k, int w, int rows_per_cta, T *tau, T *Vd,
-                      QrScratch<T> sc) {
+                      T *Tm, int transposed, QrScratch<T> sc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int ldl = kQrW + 1;
     T *loc = reinterpret_cast<T *>(smem_raw);
-    __shared__ T red[kQrThreads / 32];
-    __shared__ T s_fac[kQrW];
+    __shared__ T wred[(kQrThreads / 32) * kQrVec];
+    __shared__ T sub[kQrVec * kQrSub];
+    __shared__ T tot[kQrVec];
+    __shared__ T s_gram[kQrW][kQrW], s_t[kQrW][kQrW], s_tau[kQrW], s_f[kQrW];
     __shared__ int s_flag;
-    const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const int cta = blockIdx.x, tid = threadIdx.x;
     const int r0 = k + cta * rows_per_cta;
     const int nloc = max(0, min(rows_per_cta, m - r0));
-    for (int e = tid; e < nloc * w; e += kQrThreads) {
-        int r = e / w, j = e - r * w;
-        loc[r * ldl + j] = A[(int64_t)(r0 + r) * lda + k + j];
+    {
+        // Every copy in flight at once.
+        const unsigned l0 = (unsigned)__cvta_generic_to_shared(loc);
+        for (int e = tid; e < nloc * w; e += kQrThreads) {
+            const int r = e / w, j = e - r * w;
+            const T *src = A + (int64_t)(r0 + r) * lda + k + j;
+            if constexpr (sizeof(T) == 8)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                                 l0 + (unsigned)(sizeof(T) * (r * ldl + j))),
+                             "l"(src)
+                             : "memory");
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                                 l0 + (unsigned)(sizeof(T) * (r * ldl + j))),
+                             "l"(src)
+                             : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
     __syncthreads();
     unsigned gen = 0;
+    // Column 0: its norm below the diagonal and its diagonal entry.
+    T alpha, below;
+    {
+        T p[kQrVec];
+#pragma unroll
+        for (int i = 0; i < kQrVec; ++i) p[i] = T(0);
+        for (int r = tid; r < nloc; r += kQrThreads) {
+            const int gr = r0 + r;
+            const T x = loc[r * ldl];
+            if (gr > k) p[kQrSaa] += x * x;
+            else if (gr == k) p[kQrA1] = x;
+        }
+        if (!reduce_round(p, sc, gen, wred, sub, tot, &s_flag)) return;
+        alpha = tot[kQrA1];
+        below = tot[kQrSaa];
+    }
     for (int j = 0; j < w; ++j) {
         const int col = k + j;
-        const int slot = j & 1;
-        const bool own_col = col >= r0 && col < r0 + nloc;
-        // ||x||^2 over rows strictly below the diagonal.
-        T partial = T(0);
-        for (int r = tid; r < nloc; r += kQrThreads)
-            if (r0 + r > col) {
-                T v = loc[r * ldl + j];
-                partial += v * v;
-            }
-        partial = block_sum(partial, red);
-        if (tid == 0) sc.part[((size_t)slot * G + cta) * (kQrW + 1)] = partial;
-        if (own_col && tid == 0) sc.alpha[slot] = loc[(col - r0) * ldl + j];
-        if (!grid_barrier(sc.bar, gen++, (unsigned)G, sc.err, &s_flag)) return;
-        T below = T(0);
-        for (int g = 0; g < G; ++g) below += __ldcg(&sc.part[((size_t)slot * G + g) * (kQrW + 1)]);
-        const T alpha = __ldcg(&sc.alpha[slot]);
+        // numax's reflector: beta = -sign(alpha) ||x||, tau = (beta - alpha) / beta,
+        // v = x / (alpha - beta); no reflection when the sub-column is zero.
         T this_tau = T(0), scale = T(0), beta = alpha;
         const bool reflect = below != T(0);
         if (reflect) {
@@ -92,42 +202,94 @@ __global__ void __launch_bounds__(kQrThreads)
             if (alpha > T(0)) beta = -beta;
             this_tau = (beta - alpha) / beta;
             scale = T(1) / (alpha - beta);
-            for (int r = tid; r < nloc; r += kQrThreads)
-                if (r0 + r > col) loc[r * ldl + j] *= scale;
-            if (own_col && tid == 0) loc[(col - r0) * ldl + j] = beta;
-        }
-        if (cta == 0 && tid == 0) tau[col] = this_tau;
-        __syncthreads();
-        if (!reflect || j + 1 == w) continue;
-        // dot_c = a[col][c] + sum_{r > col} v_r a[r][c] for the remaining panel columns.
-        for (int c = j + 1; c < w; ++c) {
-            T d = T(0);
             for (int r = tid; r < nloc; r += kQrThreads) {
                 const int gr = r0 + r;
-                if (gr > col) d += loc[r * ldl + j] * loc[r * ldl + c];
-                else if (gr == col) d += loc[r * ldl + c];
+                if (gr > col) loc[r * ldl + j] *= scale;
+                else if (gr == col) loc[r * ldl + j] = beta;
             }
-            d = block_sum(d, red);
-            if (tid == 0) sc.part[((size_t)slot * G + cta) * (kQrW + 1) + c] = d;
         }
-        if (!grid_barrier(sc.bar, gen++, (unsigned)G, sc.err, &s_flag)) return;
-        if (tid < w && tid > j) {
-            T d = T(0);
-            for (int g = 0; g < G; ++g) d += __ldcg(&sc.part[((size_t)slot * G + g) * (kQrW + 1) + tid]);
-            s_fac[tid] = this_tau * d;
-        }
+        if (cta == 0 && tid == 0) tau[col] = this_tau;
+        if (tid == 0) s_tau[j] = this_tau;
+        const bool more = j + 1 < w;
         __syncthreads();
+        // The round: v_j's Gram column; unless j is the panel's last column,
+        // its dot products with the remaining columns and column j+1's norm
+        // pieces.
+        T p[kQrVec];
+#pragma unroll
+        for (int i = 0; i < kQrVec; ++i) p[i] = T(0);
+        // Every column accumulates (no per-column tests); only the entries
+        // the round needs are read afterwards: dots for j < c < w, Gram for c < j.
         for (int r = tid; r < nloc; r += kQrThreads) {
             const int gr = r0 + r;
-            if (gr > col) {
-                const T v = loc[r * ldl + j];
-                for (int c = j + 1; c < w; ++c) loc[r * ldl + c] -= s_fac[c] * v;
-            } else if (gr == col) {
-                for (int c = j + 1; c < w; ++c) loc[r * ldl + c] -= s_fac[c];
+            if (gr < col) continue;
+            const T *row = loc + r * ldl;
+            if (gr == col) {
+#pragma unroll
+                for (int c = 0; c < kQrW; ++c) {
+                    const T x = row[c];
+                    p[c] += x;
+                    p[kQrGram + c] += x;
+                }
+            } else {
+                const T v = row[j];
+#pragma unroll
+                for (int c = 0; c < kQrW; ++c) {
+                    const T x = row[c];
+                    p[c] += v * x;
+                    p[kQrGram + c] += x * v;
+                }
+                if (more) {
+                    const T a = row[j + 1];
+                    if (gr == col + 1) {
+                        p[kQrA1] = a;
+                        p[kQrV1] = v;
+                    } else {
+                        p[kQrSaa] += a * a;
+                        p[kQrSav] += v * a;
+                        p[kQrSvv] += v * v;
+                    }
+                }
             }
         }
+        if (!reduce_round(p, sc, gen, wred, sub, tot, &s_flag)) return;
+        if (tid < j) s_gram[tid][j] = tot[kQrGram + tid];
+        if (!more) break;
+        if (tid < kQrW) s_f[tid] = (tid > j && tid < w) ? this_tau * tot[tid] : T(0);
+        __syncthreads();
+        // a_c -= (tau d_c) v for the remaining panel columns (v_col = 1); the
+        // factor is zero for the other columns, which keep their values.
+        for (int r = tid; r < nloc; r += kQrThreads) {
+            const int gr = r0 + r;
+            if (gr < col) continue;
+            T *row = loc + r * ldl;
+            const T v = gr == col ? T(1) : row[j];
+#pragma unroll
+            for (int c = 0; c < kQrW; ++c) row[c] = fma(-s_f[c], v, row[c]);
+        }
+        // Column j+1: its diagonal entry after the update (the same fma the
+        // owner applied) and its norm below the diagonal, downdated.
+        const T f = this_tau * tot[j + 1];
+        const T saa = tot[kQrSaa], sav = tot[kQrSav], svv = tot[kQrSvv];
+        alpha = fma(-f, tot[kQrV1], tot[kQrA1]);
+        T bl = saa - T(2) * f * sav + f * f * svv;
+        if (!(bl >= T(kQrDowndateTol) * (saa + f * f * svv))) {
+            __syncthreads();
+            T q[kQrVec];
+#pragma unroll
+            for (int i = 0; i < kQrVec; ++i) q[i] = T(0);
+            for (int r = tid; r < nloc; r += kQrThreads)
+                if (r0 + r > col + 1) {
+                    const T x = loc[r * ldl + j + 1];
+                    q[kQrSaa] += x * x;
+                }
+            if (!reduce_round(q, sc, gen, wred, sub, tot, &s_flag)) return;
+            bl = tot[kQrSaa];
+        }
+        below = bl;
         __syncthreads();
     }
+    __syncthreads();
     // Write the factored panel back and the dense V (unit diagonal, zeros above).
     for (int e = tid; e < nloc * w; e += kQrThreads) {
         const int r = e / w, j = e - r * w, gr = r0 + r;
@@ -136,120 +298,298 @@ __global__ void __launch_bounds__(kQrThreads)
         const int rel = gr - k;
         Vd[(int64_t)rel * kQrW + j] = rel > j ? v : (rel == j ? T(1) : T(0));
     }
-    // Partial Gram matrix V^T V of this CTA's rows.
-    __syncthreads();
-    for (int e = tid; e < w * w; e += kQrThreads) {
-        const int p = e / w, q = e - p * w;
-        T s = T(0);
-        for (int r = 0; r < nloc; ++r) {
-            const int rel = r0 + r - k;
-            const T vp = rel > p ? loc[r * ldl + p] : (rel == p ? T(1) : T(0));
-            const T vq = rel > q ? loc[r * ldl + q] : (rel == q ? T(1) : T(0));
-            s += vp * vq;
-        }
-        sc.gram_part[(size_t)cta * kQrW * kQrW + p * kQrW + q] = s;
+    // T of the panel's block reflector, once (CTA 0, warp 0).
+    if (cta == 0 && tid < 32) {
+        build_t<T>(s_gram, s_tau, w, s_t);
+        store_t<T>(s_t, transposed, Tm);
     }
 }
 
-// T (or T^T when `transposed`) of the block reflector from the Gram matrix
-// and taus, numax's larft (numax/linalg/panel.mojo:2076-2169): one thread.
+// T (or T^T when `transposed`) of a block reflector from the sum of G
+// partial Gram matrices (kQrW x kQrW each) and the taus, on one CTA.
 template <typename T>
 __global__ void larft_kernel(const T *gram_part, int G, const T *tau, int k, int w, T *Tm,
                              int transposed) {
     __shared__ T g[kQrW][kQrW];
     __shared__ T t[kQrW][kQrW];
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-        const int p = e / w, q = e - p * w;
+    __shared__ T taus[kQrW];
+    for (int e = threadIdx.x; e < kQrW * kQrW; e += blockDim.x) {
+        const int p = e / kQrW, q = e - p * kQrW;
         T s = T(0);
         for (int c = 0; c < G; ++c) s += gram_part[(size_t)c * kQrW * kQrW + p * kQrW + q];
         g[p][q] = s;
-        t[p][q] = T(0);
     }
+    if (threadIdx.x < kQrW) taus[threadIdx.x] = threadIdx.x < w ? tau[k + threadIdx.x] : T(0);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        t[0][0] = tau[k];
-        for (int i = 1; i < w; ++i) {
-            const T ti = tau[k + i];
-            for (int p = 0; p < i; ++p) t[p][i] = -ti * g[p][i];
-            for (int q = 0; q < i; ++q) {
-                T s = T(0);
-                for (int r = q; r < i; ++r) s += t[q][r] * t[r][i];
-                t[q][i] = s;
-            }
-            t[i][i] = ti;
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kQrW * kQrW; e += blockDim.x) {
-        const int p = e / kQrW, q = e - p * kQrW;
-        T v = (p < w && q < w) ? (transposed ? t[q][p] : t[p][q]) : T(0);
-        Tm[p * kQrW + q] = v;
+    if (threadIdx.x < 32) {
+        build_t<T>(g, taus, w, t);
+        store_t<T>(t, transposed, Tm);
     }
 }
 
-// W = V^T C over the rows of a tall panel, split by rows: CTA (g, b) forms
-// the partial product of row chunk g with columns [256 b, 256 b + 256) of C
-// -- one thread per column, kQrW accumulators, V's rows staged through
-// shared memory -- and leaves it at part[g] (kQrW x nc).  Reads C once.
-constexpr int kVtcRows = 64;
-constexpr int kVtcMaxChunks = 512;
-template <typename T>
-__global__ void __launch_bounds__(256) vtc_partial_kernel(const T *V, const T *C, int64_t ldc,
-                                                          int mk, int nc, int rows_per, T *part) {
-    __shared__ T vs[kVtcRows][kQrW];
-    const int g = blockIdx.x;
-    const int c = blockIdx.y * 256 + threadIdx.x;
-    const int r0 = g * rows_per, r1 = min(mk, r0 + rows_per);
-    T acc[kQrW];
-#pragma unroll
-    for (int j = 0; j < kQrW; ++j) acc[j] = T(0);
-    for (int rb = r0; rb < r1; rb += kVtcRows) {
-        const int nr = min(kVtcRows, r1 - rb);
-        __syncthreads();
-        for (int e = threadIdx.x; e < kVtcRows * kQrW; e += 256) {
-            const int i = e / kQrW, j = e - i * kQrW;
-            vs[i][j] = i < nr ? V[(int64_t)(rb + i) * kQrW + j] : T(0);
-        }
-        __syncthreads();
-        if (c < nc) {
-            const T *col = C + (int64_t)rb * ldc + c;
-#pragma unroll 4
-            for (int i = 0; i < nr; ++i) {
-                const T x = col[(int64_t)i * ldc];
-#pragma unroll
-                for (int j = 0; j < kQrW; ++j) acc[j] += vs[i][j] * x;
-            }
-        }
-    }
-    if (c < nc)
-#pragma unroll
-        for (int j = 0; j < kQrW; ++j) part[((int64_t)g * kQrW + j) * nc + c] = acc[j];
-}
+// ---- the block reflector on a column block C (mk x nc, ldc) ----------------
+// C := (I - V T' V^T) C with V (mk x kQrW, ld kQrW) and T' = Tm, in three
+// kernels that touch C with VEC-wide accesses (16 bytes) where C allows it:
+//   qr_wpart_kernel:  part[g] = V_g^T C_g for row block g (kQrW x nc);
+//   qr_wsum_kernel:   W = sum_g part[g], in a fixed order;
+//   qr_update_kernel: Y = Tm W in shared memory, then C -= V Y.
+// A CTA covers up to kQrUCols columns (blockIdx.y) with kQrUThreads threads.
+constexpr int kQrUThreads = 256;
+constexpr int kQrUCols = 256;
+constexpr int kVtcMaxChunks = 512;  // most row blocks of qr_wpart_kernel
+constexpr int kQrRowsInFlight = 8;  // rows of C loaded before any is used
 
-// W = sum over the G partials (in chunk order, so every run sums alike), then
-// Y = Tm W (kQrW x kQrW times kQrW x nc), or Y = W when Tm is null.  A CTA per
-// 16 columns, thread (j, c).
-template <typename T>
-__global__ void __launch_bounds__(kQrW * 16) vtc_reduce_kernel(const T *part, int G, int nc,
-                                                              const T *Tm, T *Y) {
-    __shared__ T w[kQrW][17];
-    const int j = threadIdx.x / 16, cc = threadIdx.x % 16, c = blockIdx.x * 16 + cc;
-    T s = T(0);
-    if (c < nc) {
-#pragma unroll 8
-        for (int g = 0; g < G; ++g) s += part[((int64_t)g * kQrW + j) * nc + c];
-    }
-    w[j][cc] = s;
-    __syncthreads();
-    if (c >= nc) return;
-    if (Tm) {
-        T y = T(0);
-#pragma unroll
-        for (int p = 0; p < kQrW; ++p) y += Tm[j * kQrW + p] * w[p][cc];
-        Y[(int64_t)j * nc + c] = y;
+template <typename T, int VEC>
+__device__ __forceinline__ void load_vec(const T *p, T (&x)[VEC]) {
+    if constexpr (VEC * sizeof(T) == 16) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 v = *reinterpret_cast<const float4 *>(p);
+            x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+        } else {
+            const double2 v = *reinterpret_cast<const double2 *>(p);
+            x[0] = v.x; x[1] = v.y;
+        }
     } else {
-        Y[(int64_t)j * nc + c] = s;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) x[e] = p[e];
     }
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void store_vec(T *p, const T (&x)[VEC]) {
+    if constexpr (VEC * sizeof(T) == 16) {
+        if constexpr (sizeof(T) == 4)
+            *reinterpret_cast<float4 *>(p) = make_float4(x[0], x[1], x[2], x[3]);
+        else
+            *reinterpret_cast<double2 *>(p) = make_double2(x[0], x[1]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) p[e] = x[e];
+    }
+}
+
+// The kQrW entries of V's row r (64- or 128-byte aligned rows).
+template <typename T>
+__device__ __forceinline__ void load_vrow(const T *V, int64_t r, T (&v)[kQrW]) {
+    constexpr int E = 16 / sizeof(T);
+    const T *p = V + r * kQrW;
+#pragma unroll
+    for (int i = 0; i < kQrW; i += E) {
+        T x[E];
+        load_vec<T, E>(p + i, x);
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[i + e] = x[e];
+    }
+}
+
+// Threads split as nq column groups (VEC columns each, nq a power of two
+// covering the block's columns, at most kQrUCols / VEC) times ph = 256 / nq
+// rows in flight.
+// Rows of V staged in shared memory per chunk (double-buffered).
+constexpr int kQrVChunk = 128;
+
+// Start copying V rows [cs, min(ce, cs + kQrVChunk)) into vs (16-byte pieces).
+template <typename T>
+__device__ __forceinline__ void stage_v(const T *V, int cs, int ce, T *vs) {
+    const int rows = min(kQrVChunk, ce - cs);
+    const int pieces = rows * kQrW * (int)sizeof(T) / 16;
+    const unsigned s0 = (unsigned)__cvta_generic_to_shared(vs);
+    const char *src = reinterpret_cast<const char *>(V + (int64_t)cs * kQrW);
+    for (int i = threadIdx.x; i < pieces; i += kQrUThreads)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s0 + 16u * i),
+                     "l"(src + 16 * (int64_t)i)
+                     : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void vrow_smem(const T *vs, int i, T (&v)[kQrW]) {
+    constexpr int E = 16 / sizeof(T);
+#pragma unroll
+    for (int j = 0; j < kQrW; j += E) {
+        T x[E];
+        load_vec<T, E>(vs + i * kQrW + j, x);
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[j + e] = x[e];
+    }
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kQrUThreads, 2)
+    qr_wpart_kernel(const T *V, const T *C, int64_t ldc, int mk, int nc, int rows_per, int nq,
+                    T *part) {
+    extern __shared__ __align__(16) unsigned char qr_smem[];
+    T *red = reinterpret_cast<T *>(qr_smem);  // [ph][kQrW][nq * VEC]
+    T *vs = red + kQrW * kQrUThreads * VEC;   // [2][kQrVChunk][kQrW]
+    const int ph_n = kQrUThreads / nq, wc = nq * VEC;
+    const int q = threadIdx.x % nq, ph = threadIdx.x / nq;
+    const int cl = q * VEC, c0 = blockIdx.y * kQrUCols, c = c0 + cl;
+    const bool active = c < nc;
+    const int r0 = blockIdx.x * rows_per, r1 = min(mk, r0 + rows_per);
+    T acc[kQrW][VEC];
+#pragma unroll
+    for (int j = 0; j < kQrW; ++j)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) acc[j][e] = T(0);
+    // V in chunks of kQrVChunk rows through shared memory (the next chunk's
+    // copy in flight while this one is used); per chunk, kQrRowsInFlight
+    // rows' loads of C issued back to back, then used.
+    if (r0 < r1) stage_v<T>(V, r0, r1, vs);
+    for (int cs = r0, b = 0; cs < r1; cs += kQrVChunk, b ^= 1) {
+        const int ce = min(r1, cs + kQrVChunk);
+        if (ce < r1) {
+            stage_v<T>(V, ce, r1, vs + (b ^ 1) * kQrVChunk * kQrW);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const T *vb = vs + b * kQrVChunk * kQrW;
+        if (active) {
+            for (int rb = cs + ph; rb < ce; rb += kQrRowsInFlight * ph_n) {
+                T x[kQrRowsInFlight][VEC];
+#pragma unroll
+                for (int u = 0; u < kQrRowsInFlight; ++u) {
+                    const int r = rb + u * ph_n;
+                    if (r < ce) {
+                        load_vec<T, VEC>(C + (int64_t)r * ldc + c, x[u]);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) x[u][e] = T(0);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kQrRowsInFlight; ++u) {
+                    const int r = rb + u * ph_n;
+                    if (r < ce) {
+                        T v[kQrW];
+                        vrow_smem<T>(vb, r - cs, v);
+#pragma unroll
+                        for (int j = 0; j < kQrW; ++j)
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) acc[j][e] += v[j] * x[u][e];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < kQrW; ++j)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) red[(ph * kQrW + j) * wc + cl + e] = acc[j][e];
+    __syncthreads();
+    // Sum the row phases in order.
+    for (int o = threadIdx.x; o < kQrW * wc; o += kQrUThreads) {
+        const int j = o / wc, cc = o - j * wc;
+        if (c0 + cc >= nc) continue;
+        T t = T(0);
+        for (int h = 0; h < ph_n; ++h) t += red[(h * kQrW + j) * wc + cc];
+        part[((int64_t)blockIdx.x * kQrW + j) * nc + c0 + cc] = t;
+    }
+}
+
+// W[j][c] = sum over g of part[g][j][c]: a CTA per (32 columns, j), 8
+// lanes over g each summing a fixed residue class, then the lanes in order.
+template <typename T>
+__global__ void __launch_bounds__(256) qr_wsum_kernel(const T *part, int G, int nc, T *W) {
+    __shared__ T s[8][33];
+    const int cc = threadIdx.x % 32, lane = threadIdx.x / 32;
+    const int c = blockIdx.x * 32 + cc, j = blockIdx.y;
+    T t = T(0);
+    if (c < nc) {
+#pragma unroll 4
+        for (int g = lane; g < G; g += 8) t += part[((int64_t)g * kQrW + j) * nc + c];
+    }
+    s[lane][cc] = t;
+    __syncthreads();
+    if (lane == 0 && c < nc) {
+        T u = T(0);
+#pragma unroll
+        for (int h = 0; h < 8; ++h) u += s[h][cc];
+        W[(int64_t)j * nc + c] = u;
+    }
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kQrUThreads, 2)
+    qr_update_kernel(const T *V, T *C, int64_t ldc, int mk, int nc, int rows_per, int nq,
+                     const T *Tm, const T *W) {
+    __shared__ T y[kQrW][kQrUCols];
+    __shared__ T tm[kQrW][kQrW];
+    const int c0 = blockIdx.y * kQrUCols;
+    for (int e = threadIdx.x; e < kQrW * kQrW; e += kQrUThreads) tm[e / kQrW][e % kQrW] = Tm[e];
+    __syncthreads();
+    // Y = Tm W for this CTA's columns.
+    for (int cc = threadIdx.x; cc < kQrUCols; cc += kQrUThreads) {
+        T wcol[kQrW];
+#pragma unroll
+        for (int p = 0; p < kQrW; ++p) wcol[p] = c0 + cc < nc ? W[(int64_t)p * nc + c0 + cc] : T(0);
+#pragma unroll
+        for (int j = 0; j < kQrW; ++j) {
+            T t = T(0);
+#pragma unroll
+            for (int p = 0; p < kQrW; ++p) t += tm[j][p] * wcol[p];
+            y[j][cc] = t;
+        }
+    }
+    __syncthreads();
+    extern __shared__ __align__(16) unsigned char qr_smem[];
+    T *vs = reinterpret_cast<T *>(qr_smem);  // [2][kQrVChunk][kQrW]
+    const int ph_n = kQrUThreads / nq;
+    const int q = threadIdx.x % nq, ph = threadIdx.x / nq;
+    const int cl = q * VEC, c = c0 + cl;
+    const bool active = c < nc;
+    T yr[kQrW][VEC];
+#pragma unroll
+    for (int j = 0; j < kQrW; ++j)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) yr[j][e] = active ? y[j][cl + e] : T(0);
+    const int r0 = blockIdx.x * rows_per, r1 = min(mk, r0 + rows_per);
+    if (r0 < r1) stage_v<T>(V, r0, r1, vs);
+    for (int cs = r0, b = 0; cs < r1; cs += kQrVChunk, b ^= 1) {
+        const int ce = min(r1, cs + kQrVChunk);
+        if (ce < r1) {
+            stage_v<T>(V, ce, r1, vs + (b ^ 1) * kQrVChunk * kQrW);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const T *vb = vs + b * kQrVChunk * kQrW;
+        if (active) {
+            for (int rb = cs + ph; rb < ce; rb += kQrRowsInFlight * ph_n) {
+                T x[kQrRowsInFlight][VEC];
+#pragma unroll
+                for (int u = 0; u < kQrRowsInFlight; ++u) {
+                    const int r = rb + u * ph_n;
+                    if (r < ce) load_vec<T, VEC>(C + (int64_t)r * ldc + c, x[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < kQrRowsInFlight; ++u) {
+                    const int r = rb + u * ph_n;
+                    if (r < ce) {
+                        T v[kQrW];
+                        vrow_smem<T>(vb, r - cs, v);
+#pragma unroll
+                        for (int j = 0; j < kQrW; ++j)
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) x[u][e] -= v[j] * yr[j][e];
+                        store_vec<T, VEC>(C + (int64_t)r * ldc + c, x[u]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Column groups of a trailing kernel for nc columns at VEC per thread.
+static int qr_col_groups(int nc, int vec) {
+    const int need = (int)std::min<int64_t>(ceil_div(nc, vec), kQrUCols / vec);
+    int nq = 1;
+    while (nq < need) nq *= 2;
+    return nq;
 }
 
 template <typename T>
@@ -260,19 +600,46 @@ struct QrRun {
     T *Vd, *Tm, *Yk;  // V (m x 16), T (16 x 16), Y (16 x n)
     T *part;          // kVtcMaxChunks x 16 x n partial products
     QrScratch<T> sc;
+    size_t panel_smem_max;  // dynamic shared memory the panel kernel may use
 };
 
-// Y = Tm V^T C (Tm null: Y = V^T C) for the mk x nc block C.
-template <typename T>
-static int vtc(QrRun<T> &R, int mk, const T *C, int64_t ldc, int nc, const T *Tm, T *Y) {
-    const int cb = (int)ceil_div(nc, 256);
-    int G = (int)std::min<int64_t>({ceil_div(mk, 256), (int64_t)kVtcMaxChunks,
-                                    std::max<int64_t>(1, 4 * (int64_t)R.ctx->sm_count / cb)});
+// Row blocks of the trailing kernels: about `per_sm` CTAs per SM, at least
+// 64 rows each.
+static int qr_row_blocks(nmx_ctx ctx, int mk, int cb, int per_sm, int *rows_per) {
+    int G = (int)std::min<int64_t>({ceil_div(mk, 64), (int64_t)kVtcMaxChunks,
+                                    std::max<int64_t>(1, (int64_t)per_sm * ctx->sm_count / cb)});
     G = std::max(G, 1);
-    const int rows_per = (int)ceil_div(mk, G);
-    G = (int)ceil_div(mk, rows_per);
-    vtc_partial_kernel<T><<<dim3(G, cb), 256, 0, R.st>>>(R.Vd, C, ldc, mk, nc, rows_per, R.part);
-    vtc_reduce_kernel<T><<<(unsigned)ceil_div(nc, 16), kQrW * 16, 0, R.st>>>(R.part, G, nc, Tm, Y);
+    *rows_per = (int)ceil_div(mk, G);
+    return (int)ceil_div(mk, *rows_per);
+}
+
+// Whether C's rows allow 16-byte accesses at every row start.
+template <typename T>
+static bool qr_vec_ok(const T *C, int64_t ldc, int nc) {
+    constexpr int E = 16 / sizeof(T);
+    return (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ldc % E == 0 && nc % E == 0;
+}
+
+// W = V^T C (kQrW x nc, into Wout) for the mk x nc block C.
+template <typename T>
+static int vtc(QrRun<T> &R, int mk, const T *C, int64_t ldc, int nc, T *Wout) {
+    constexpr int E = 16 / sizeof(T);
+    const int cb = (int)ceil_div(nc, kQrUCols);
+    int rows_per = 0;
+    const int G = qr_row_blocks(R.ctx, mk, cb, 2, &rows_per);
+    // Shared memory of the phase sums: ph x kQrW x (nq VEC) = kQrW x 256 VEC values.
+    if (qr_vec_ok(C, ldc, nc)) {
+        const int nq = qr_col_groups(nc, E);
+        const size_t smem = sizeof(T) * ((size_t)kQrW * kQrUThreads * E + 2 * kQrVChunk * kQrW);
+        qr_wpart_kernel<T, E><<<dim3(G, cb), kQrUThreads, smem, R.st>>>(R.Vd, C, ldc, mk, nc,
+                                                                          rows_per, nq, R.part);
+    } else {
+        const int nq = qr_col_groups(nc, 1);
+        const size_t smem = sizeof(T) * ((size_t)kQrW * kQrUThreads + 2 * kQrVChunk * kQrW);
+        qr_wpart_kernel<T, 1><<<dim3(G, cb), kQrUThreads, smem, R.st>>>(R.Vd, C, ldc, mk, nc,
+                                                                          rows_per, nq, R.part);
+    }
+    qr_wsum_kernel<T><<<dim3((unsigned)ceil_div(nc, 32), kQrW), 256, 0, R.st>>>(R.part, G, nc, Wout);
     NMX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -281,34 +648,44 @@ static int vtc(QrRun<T> &R, int mk, const T *C, int64_t ldc, int nc, const T *Tm
 template <typename T>
 static int qr_panel(QrRun<T> &R, T *A, int64_t lda, T *tau, int k, int w, int transposed) {
     const int mk = R.m - k;
-    int G = (int)std::min<int64_t>(R.ctx->sm_count, ceil_div(mk, 64));
+    int G = (int)std::min<int64_t>(std::min(R.ctx->sm_count, kQrMaxG), ceil_div(mk, 64));
     G = std::max(G, 1);
     int rpc = (int)ceil_div(mk, G);
     G = (int)ceil_div(mk, rpc);
     const size_t smem = sizeof(T) * (size_t)rpc * (kQrW + 1);
-    if (smem > R.ctx->smem_optin - 1024) {
+    if (smem > R.panel_smem_max) {
         set_error("QR panel of %d rows does not fit the cooperative grid", mk);
         return NMX_ERR_UNSUPPORTED;
     }
     NMX_CUDA_TRY(cudaMemsetAsync(R.sc.bar, 0, sizeof(unsigned), R.st));
     NMX_CUDA_TRY(cudaMemsetAsync(R.Vd, 0, sizeof(T) * (size_t)mk * kQrW, R.st));
-    void *args[] = {&A, &lda, &R.m, &k, &w, &rpc, &tau, &R.Vd, &R.sc};
+    void *args[] = {&A, &lda, &R.m, &k, &w, &rpc, &tau, &R.Vd, &R.Tm, &transposed, &R.sc};
     NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)geqr2_coop_kernel<T>, dim3(G), dim3(kQrThreads),
                                              args, smem, R.st));
-    larft_kernel<T><<<1, 256, 0, R.st>>>(R.sc.gram_part, G, tau, k, w, R.Tm, transposed);
-    NMX_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
 // C := (I - V T' V^T) C for C = rows [k, m) x cols [c0, c1) of Cm.
 template <typename T>
 static int apply_reflector(QrRun<T> &R, int k, T *Cm, int64_t ldc, int c0, int c1) {
+    constexpr int E = 16 / sizeof(T);
     const int nc = c1 - c0, mk = R.m - k;
     if (nc <= 0) return 0;
     T *C = Cm + (int64_t)k * ldc + c0;
-    // Y = T' (V^T C), then C -= V Y.
-    NMX_TRY(vtc<T>(R, mk, C, ldc, nc, R.Tm, R.Yk));
-    return gemm_cc<T>(R.st, false, false, mk, nc, kQrW, T(-1), R.Vd, kQrW, R.Yk, nc, T(1), C, ldc);
+    // W = V^T C, then Y = T' W and C -= V Y.
+    NMX_TRY(vtc<T>(R, mk, C, ldc, nc, R.Yk));
+    const int cb = (int)ceil_div(nc, kQrUCols);
+    int rows_per = 0;
+    const int G = qr_row_blocks(R.ctx, mk, cb, 4, &rows_per);
+    const size_t vsm = sizeof(T) * 2 * kQrVChunk * kQrW;
+    if (qr_vec_ok(C, ldc, nc))
+        qr_update_kernel<T, E><<<dim3(G, cb), kQrUThreads, vsm, R.st>>>(
+            R.Vd, C, ldc, mk, nc, rows_per, qr_col_groups(nc, E), R.Tm, R.Yk);
+    else
+        qr_update_kernel<T, 1><<<dim3(G, cb), kQrUThreads, vsm, R.st>>>(
+            R.Vd, C, ldc, mk, nc, rows_per, qr_col_groups(nc, 1), R.Tm, R.Yk);
+    NMX_CUDA_TRY(cudaGetLastError());
+    return 0;
 }
 
 template <typename T>
@@ -316,8 +693,8 @@ static int qr_setup(nmx_ctx ctx, cudaStream_t st, int64_t m, int64_t n, QrRun<T>
     const int G = ctx->sm_count;
     const size_t nn = (size_t)std::max<int64_t>(n, kQrW);
     size_t elems = (size_t)m * kQrW + kQrW * kQrW + (size_t)kQrW * nn +
-                   (size_t)kVtcMaxChunks * kQrW * nn + 2 * (size_t)G * (kQrW + 1) + 2 +
-                   (size_t)G * kQrW * kQrW + 64;
+                   (size_t)kVtcMaxChunks * kQrW * nn + 2 * (size_t)kQrVec * kQrPart +
+                   (size_t)kQrW * kQrW + 64;
     void *wsv = nullptr;
     int rc = ctx->ensure_slot(kWsWork, sizeof(T) * elems + 64, &wsv);
     if (rc) return rc;
@@ -330,14 +707,29 @@ static int qr_setup(nmx_ctx ctx, cudaStream_t st, int64_t m, int64_t n, QrRun<T>
     R.Yk = R.Tm + kQrW * kQrW;
     R.part = R.Yk + (size_t)kQrW * nn;
     R.sc.part = R.part + (size_t)kVtcMaxChunks * kQrW * nn;
-    R.sc.alpha = R.sc.part + 2 * (size_t)G * (kQrW + 1);
-    R.sc.gram_part = R.sc.alpha + 2;
-    R.sc.bar = reinterpret_cast<unsigned *>(R.sc.gram_part + (size_t)G * kQrW * kQrW);
+    R.sc.gram_part = R.sc.part + 2 * (size_t)kQrVec * kQrPart;
+    R.sc.bar = reinterpret_cast<unsigned *>(R.sc.gram_part + (size_t)kQrW * kQrW);
     R.sc.err = reinterpret_cast<int *>(R.sc.bar + 1);
     NMX_CUDA_TRY(cudaMemsetAsync(R.sc.err, 0, sizeof(int), st));
+    cudaFuncAttributes fa;
+    NMX_CUDA_TRY(cudaFuncGetAttributes(&fa, geqr2_coop_kernel<T>));
+    R.panel_smem_max = ctx->smem_optin - fa.sharedSizeBytes;
     NMX_CUDA_TRY(cudaFuncSetAttribute(geqr2_coop_kernel<T>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(ctx->smem_optin - 1024)));
+                                      (int)R.panel_smem_max));
+    constexpr int E = 16 / sizeof(T);
+    NMX_CUDA_TRY(cudaFuncSetAttribute(
+        qr_wpart_kernel<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)(sizeof(T) * ((size_t)kQrW * kQrUThreads * E + 2 * kQrVChunk * kQrW))));
+    NMX_CUDA_TRY(cudaFuncSetAttribute(
+        qr_wpart_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)(sizeof(T) * ((size_t)kQrW * kQrUThreads + 2 * kQrVChunk * kQrW))));
+    NMX_CUDA_TRY(cudaFuncSetAttribute(qr_update_kernel<T, E>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(T) * 2 * kQrVChunk * kQrW)));
+    NMX_CUDA_TRY(cudaFuncSetAttribute(qr_update_kernel<T, 1>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(T) * 2 * kQrVChunk * kQrW)));
     return 0;
 }
 
@@ -413,7 +805,7 @@ static int orgqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, con
                                                                              R.Vd, nullptr);
         NMX_CUDA_TRY(cudaGetLastError());
         // Gram matrix of V for T (one partial), then T.
-        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, nullptr, R.sc.gram_part));
+        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, R.sc.gram_part));
         larft_kernel<T><<<1, 256, 0, st>>>(R.sc.gram_part, 1, tau, k, w, R.Tm, 0);
         NMX_CUDA_TRY(cudaGetLastError());
         rc = apply_reflector<T>(R, k, Q, ldq, k, (int)n);
@@ -448,7 +840,7 @@ static int ormqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, con
         pack_v_kernel<T><<<(unsigned)ceil_div(mk * kQrW, 256), 256, 0, st>>>(F, ldf, (int)m, k, w,
                                                                              R.Vd, nullptr);
         NMX_CUDA_TRY(cudaGetLastError());
-        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, nullptr, R.sc.gram_part));
+        NMX_TRY(vtc<T>(R, (int)mk, R.Vd, kQrW, kQrW, R.sc.gram_part));
         larft_kernel<T><<<1, 256, 0, st>>>(R.sc.gram_part, 1, tau, k, w, R.Tm, 1);
         NMX_CUDA_TRY(cudaGetLastError());
         NMX_TRY(apply_reflector<T>(R, k, B, ldb, 0, (int)nrhs));
