@@ -121,9 +121,22 @@ __global__ void __launch_bounds__(kCholTrsmThreads)
     constexpr int NW = kCholTrsmThreads / 32;
     const int nb = w / 32;
     const int rb = r0 + 32 * blockIdx.x, nr = min(32, r1 - rb);
+    // Copies into shared memory go out as cp.async, all in flight at once.
+    auto async8 = [](T *dst, const T *src) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        if constexpr (sizeof(T) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    };
     for (int i = warp; i < 32; i += NW)
-        for (int q = lane; q < w; q += 32)
-            X[i * xp + q] = i < nr ? A[(int64_t)(rb + i) * lda + c + q] : T(0);
+        for (int q = lane; q < w; q += 32) {
+            if (i < nr)
+                async8(&X[i * xp + q], &A[(int64_t)(rb + i) * lda + c + q]);
+            else
+                X[i * xp + q] = T(0);
+        }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
     if (warp < nb) {
         T *D = Li + warp * 32 * 33;
         const int cb = c + 32 * warp;
@@ -149,7 +162,8 @@ __global__ void __launch_bounds__(kCholTrsmThreads)
         const int cb = 32 * b;
         // L's rows [cb, cb+32) x columns [0, cb), transposed: Lt[p][q] = L[cb+q][p].
         for (int q = warp; q < 32; q += NW)
-            for (int p = lane; p < cb; p += 32) Lt[p * 34 + q] = A[(int64_t)(c + cb + q) * lda + c + p];
+            for (int p = lane; p < cb; p += 32) async8(&Lt[p * 34 + q], &A[(int64_t)(c + cb + q) * lda + c + p]);
+        asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
         __syncthreads();
         T acc[4] = {T(0), T(0), T(0), T(0)};
         for (int p = 0; p < cb; ++p) {

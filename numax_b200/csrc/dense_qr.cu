@@ -257,15 +257,16 @@ __global__ void __launch_bounds__(kQrThreads, 1)
         if (!more) break;
         if (tid < kQrW) s_f[tid] = (tid > j && tid < w) ? this_tau * tot[tid] : T(0);
         __syncthreads();
-        // a_c -= (tau d_c) v for the remaining panel columns (v_col = 1); the
-        // factor is zero for the other columns, which keep their values.
+        // a_c -= (tau d_c) v for the remaining panel columns (v_col = 1; the
+        // factor is zero past the panel's width).
         for (int r = tid; r < nloc; r += kQrThreads) {
             const int gr = r0 + r;
             if (gr < col) continue;
             T *row = loc + r * ldl;
             const T v = gr == col ? T(1) : row[j];
 #pragma unroll
-            for (int c = 0; c < kQrW; ++c) row[c] = fma(-s_f[c], v, row[c]);
+            for (int c = 0; c < kQrW; ++c)
+                if (c > j) row[c] = fma(-s_f[c], v, row[c]);
         }
         // Column j+1: its diagonal entry after the update (the same fma the
         // owner applied) and its norm below the diagonal, downdated.
