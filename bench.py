@@ -917,6 +917,8 @@ def main():
                     help="skip the dense LU/Cholesky/QR leg")
     ap.add_argument("--eigh-count", type=int, default=65536,
                     help="matrices in the batched Jacobi eigh leg (0 skips it)")
+    ap.add_argument("--only-qr", action="store_true",
+                    help="run only the FP32 QR leg (geqrf + orgqr of 262144 x 256), for profiling")
     ap.add_argument("--only-big", action="store_true",
                     help="run only the n in 97..128 bucket of the batch (the dominant kernel), "
                          "default schedule, for profiling")
@@ -925,6 +927,12 @@ def main():
         return run_reference(args)
     if args.only_big:
         return run_big_bucket(args)
+    if args.only_qr:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        print(json.dumps({"dense": run_dense(dev, orders=())}), flush=True)
+        return 0
     if args.only_dense:
         import torch
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
