@@ -164,6 +164,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def arith_dtype(schedule, io_dtype):
+    """The arithmetic type of a batched plan's launches: the tile kernel
+    computes in FP64 for both element types, the packed kernel in the batch's
+    own type."""
+    kinds = {"f64" if (s["threads"] >= 1000 or io_dtype == "f64") else io_dtype for s in schedule}
+    return kinds.pop() if len(kinds) == 1 else "+".join(sorted(kinds))
+
+
 def kernel_name(shape, dtype):
     """The kernel a batched plan's CTA shape code selects."""
     if shape >= 1000:
@@ -827,7 +835,8 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": total_s / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": arith_dtype(schedule, args.dtype), "io_dtype": args.dtype,
         "data": "synthetic (seeded torch generator, A=GG^T/n+nI, B~N(0,1))",
         "config": {"workload": "batched uneven Cholesky + cho_solve", "count_per_gpu": len(ns),
                    "n_range": [NMIN, NMAX], "nrhs": NRHS, "parallelism": f"shard{world}",

@@ -115,9 +115,10 @@ NMX_API int nmx_tune_get(nmx_ctx ctx, const char *key, int64_t *value);
  */
 
 /* Build a plan: sorts the batch by size into buckets (n <= 32, 64, 96, 128),
- * gives each bucket its default CTA shape and uploads the schedule: for
- * NMX_F64 the 8 x 8 DMMA tile kernel with 1 warp per matrix up to n = 64,
- * 2 up to 96 and 4 up to 128; for NMX_F32 the packed-triangle kernel.
+ * gives each bucket its default CTA shape and uploads the schedule: the
+ * 8 x 8 DMMA tile kernel with 1 warp per matrix up to n = 64, 2 up to 96 and
+ * 4 up to 128 (it computes in FP64; an NMX_F32 batch is widened on load and
+ * L, X rounded to FP32 on store).
  * nmx_batched_plan_autotune / _set_shape change the shapes.  n_host: count
  * sizes on the HOST.  dtype: NMX_F32 / NMX_F64.  nrhs: 0..8. */
 NMX_API int nmx_potrf_potrs_batched_plan(nmx_ctx ctx, int dtype, int64_t count, const int32_t *n_host,
@@ -137,8 +138,8 @@ NMX_API int nmx_potrf_potrs_batched_f32(nmx_ctx ctx, nmx_batched_plan plan, cons
 
 /* Autotuner (no numax counterpart; numax launches one problem per thread at
  * a compile-time n): times every CTA shape (64, 96, 128, 192 threads of the
- * packed-triangle kernel, and for FP64 the kernel on 8 x 8 DMMA tiles with
- * 1, 2, 4 or 8 warps per matrix, shapes NMX_BATCHED_TILE_SHAPE(warps)) that
+ * packed-triangle kernel, and the kernel on 8 x 8 DMMA tiles with 1, 2, 4
+ * or 8 warps per matrix, shapes NMX_BATCHED_TILE_SHAPE(warps)) that
  * covers each size bucket of the plan on these buffers -- the bucket's
  * persistent kernel alone, best of `reps` runs, CUDA events -- and keeps the
  * fastest in the plan.  Every run computes the whole bucket, so L, X and
@@ -167,7 +168,7 @@ NMX_API int nmx_batched_partition(int64_t count, const int32_t *n_host, int nrhs
 /* Set the CTA shape of one size bucket (bucket >= 0) or of all (-1) by hand,
  * in place of the default or the autotuner's pick (no numax counterpart):
  * threads 64, 96, 128 or 192 select the packed-triangle kernel,
- * NMX_BATCHED_TILE_SHAPE(1, 2, 4 or 8) = 1032, 1064, 1128 or 1256 the FP64
+ * NMX_BATCHED_TILE_SHAPE(1, 2, 4 or 8) = 1032, 1064, 1128 or 1256 the
  * kernel on 8 x 8 DMMA tiles with that many warps per matrix.  Rejects a
  * shape that cannot cover a bucket or does not fit an SM. */
 NMX_API int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket,

@@ -29,8 +29,8 @@ _DT = {torch.float64: (_lib.NMX_F64, "f64"), torch.float32: (_lib.NMX_F32, "f32"
 
 
 def tile_shape(warps: int) -> int:
-    """CTA shape code of the FP64 8 x 8 DMMA tile kernel with `warps` (1, 2,
-    4 or 8) warps per matrix, as the schedule reports it."""
+    """CTA shape code of the 8 x 8 DMMA tile kernel with `warps` (1, 2, 4 or
+    8) warps per matrix, as the schedule reports it."""
     if warps not in (1, 2, 4, 8):
         raise ValueError("warps must be 1, 2, 4 or 8")
     return 1000 + 32 * warps
@@ -170,8 +170,8 @@ class CholeskySolveBatch:
     def force_shape(self, threads: int, bucket: int = -1):
         """Fix the CTA shape of one size bucket (or all, bucket = -1): 64, 96,
         128 or 192 threads (packed-triangle kernel) or tile_shape(w) =
-        1000 + 32 w for w = 1, 2, 4, 8 warps per matrix (the FP64 kernel on
-        8 x 8 DMMA tiles).  Returns the schedule."""
+        1000 + 32 w for w = 1, 2, 4, 8 warps per matrix (the kernel on 8 x 8
+        DMMA tiles, FP64 arithmetic).  Returns the schedule."""
         _lib.call("nmx_batched_plan_set_shape", self._ctx, self._plan, int(bucket), int(threads))
         return self.schedule()
 

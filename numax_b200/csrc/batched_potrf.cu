@@ -737,8 +737,9 @@ static int potrf_threads_for(int nmax) {
 }
 
 // CTA shapes 1032, 1064, 1128 and 1256 (1000 + threads) select the 8 x 8
-// DMMA tile kernel with 1, 2, 4 or 8 warps per matrix (FP64 only,
-// batched_potrf_tile.cuh); 64, 96, 128 and 192 potrf_potrs_batched_kernel.
+// DMMA tile kernel with 1, 2, 4 or 8 warps per matrix (FP64 arithmetic for
+// both element types, batched_potrf_tile.cuh); 64, 96, 128 and 192
+// potrf_potrs_batched_kernel.
 static const int kAllShapes[] = {64, 96, 128, 192, kTileShapeBase + 32, kTileShapeBase + 64,
                                  kTileShapeBase + 128, kTileShapeBase + 256};
 
@@ -763,16 +764,12 @@ static int launch_bucket(const BatchedPotrfArgs &args, const nmx_batched_plan_s:
         NMX_CASE(128)
         NMX_CASE(192)
 #undef NMX_CASE
-#define NMX_TCASE(WPM)                                                                    \
-    case kTileShapeBase + 32 * WPM:                                                        \
-        if constexpr (sizeof(T) == 8) {                                                    \
-            potrf_tile_batched_kernel<WPM><<<b.grid, 32 * WPM, b.smem, st>>>(args, b.begin, \
-                                                                           b.end, b.nmax,  \
-                                                                           counter);       \
-            break;                                                                         \
-        }                                                                                  \
-        set_error("the tile kernel is FP64 only");                                         \
-        return NMX_ERR_INTERNAL;
+#define NMX_TCASE(WPM)                                                                   \
+    case kTileShapeBase + 32 * WPM:                                                       \
+        potrf_tile_batched_kernel<WPM, T><<<b.grid, 32 * WPM, b.smem, st>>>(args, b.begin, \
+                                                                          b.end, b.nmax,  \
+                                                                          counter);       \
+        break;
         NMX_TCASE(1)
         NMX_TCASE(2)
         NMX_TCASE(4)
@@ -823,11 +820,9 @@ static int shape_occupancy(nmx_ctx ctx, int threads, size_t smem, int *per_sm) {
 #undef NMX_OCC
 #define NMX_TOCC(WPM)                                                                   \
     case kTileShapeBase + 32 * WPM:                                                      \
-        if constexpr (sizeof(T) == 8) {                                                  \
-            NMX_CUDA_TRY(set_max_dynamic_smem(potrf_tile_batched_kernel<WPM>, ctx));     \
-            NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                  \
-                per_sm, potrf_tile_batched_kernel<WPM>, 32 * WPM, smem));                \
-        }                                                                                \
+        NMX_CUDA_TRY(set_max_dynamic_smem(potrf_tile_batched_kernel<WPM, T>, ctx));      \
+        NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
+            per_sm, potrf_tile_batched_kernel<WPM, T>, 32 * WPM, smem));                 \
         break;
         NMX_TOCC(1)
         NMX_TOCC(2)
@@ -840,14 +835,12 @@ static int shape_occupancy(nmx_ctx ctx, int threads, size_t smem, int *per_sm) {
     return 0;
 }
 
-// Default CTA shape of a bucket: for FP64 the tile kernel with 1 warp per
-// matrix up to n = 64, 2 up to 96 and 4 up to 128 (the fastest shapes on a
-// B200 for n ~ U[8, 128] with 4 right-hand sides); for FP32 the
-// packed-triangle kernel.
+// Default CTA shape of a bucket: the tile kernel with 1 warp per matrix up
+// to n = 64, 2 up to 96 and 4 up to 128 (the fastest shapes on a B200 for
+// n ~ U[8, 128] with 4 right-hand sides, FP64 and FP32 alike).
 template <typename T>
 static int default_shape(int nmax) {
-    if (sizeof(T) == 8) return kTileShapeBase + 32 * (nmax <= 64 ? 1 : (nmax <= 96 ? 2 : 4));
-    return potrf_threads_for(nmax);
+    return kTileShapeBase + 32 * (nmax <= 64 ? 1 : (nmax <= 96 ? 2 : 4));
 }
 
 template <typename T>
@@ -925,9 +918,7 @@ static int autotune(nmx_ctx ctx, nmx_batched_plan plan, const T *A, T *L, const 
         float best_ms = 3.4e38f;
         for (int threads : kAllShapes) {
             auto cand = plan->buckets[bi];
-            if (is_tile_shape(threads)) {
-                if (sizeof(T) != 8) continue;
-            } else if (!shape_covers(threads, cand.nmax, plan->nrhs)) {
+            if (!is_tile_shape(threads) && !shape_covers(threads, cand.nmax, plan->nrhs)) {
                 continue;
             }
             cand.threads = threads;
@@ -1207,9 +1198,7 @@ int nmx_batched_plan_set_shape(nmx_ctx ctx, nmx_batched_plan plan, int bucket, i
                   "bucket must be -1 (all) or a bucket index");
     NMX_ARG_CHECK(threads == 64 || threads == 96 || threads == 128 || threads == 192 ||
                       is_tile_shape(threads),
-                  4, "threads must be 64, 96, 128, 192, or 1032, 1064, 1128, 1256 (the FP64 tile kernel)");
-    NMX_ARG_CHECK(!is_tile_shape(threads) || plan->dtype == NMX_F64, 4,
-                  "the tile kernel is FP64 only");
+                  4, "threads must be 64, 96, 128, 192, or 1032, 1064, 1128, 1256 (the tile kernel)");
     DeviceGuard g(ctx->device);
     for (int bi = 0; bi < (int)plan->buckets.size(); ++bi) {
         if (bucket >= 0 && bi != bucket) continue;

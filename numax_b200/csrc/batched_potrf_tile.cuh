@@ -1,4 +1,5 @@
-// Batched Cholesky + cho_solve on 8 x 8 DMMA tiles (FP64), the second kernel
+// Batched Cholesky + cho_solve on 8 x 8 DMMA tiles (computed in FP64; FP32
+// batches are widened on load and rounded on store), the second kernel
 // family of the plan in batched_potrf.cu: the same work as
 // potrf_potrs_batched_kernel (numax's Array-tier cholesky + cholesky_solve,
 // numax/linalg/_array/cholesky.mojo:26-92, per matrix of a ragged batch) in
@@ -84,7 +85,8 @@ __device__ __forceinline__ double afrag_of(double v0, double v1, int q, int lane
 // tile, and global L), W's strict lower triangle transposed into the tile's
 // upper triangle, and the inverted pivots.  Returns the 1-based column of
 // the first pivot d <= 0 among the tile's valid columns, 0 if none.
-__device__ __forceinline__ int factor_diag_tile(double *tile, double *dinv, double *L, int n, int K,
+template <typename TM>
+__device__ __forceinline__ int factor_diag_tile(double *tile, double *dinv, TM *L, int n, int K,
                                                 int lane) {
     double a[8][8];
 #pragma unroll
@@ -147,21 +149,26 @@ __device__ __forceinline__ int factor_diag_tile(double *tile, double *dinv, doub
     const double2 v = *reinterpret_cast<const double2 *>(tile + swz(r, c0));
     const int gi = 8 * K + r, gj = 8 * K + c0;
     if (gi < n) {
-        if (gj <= gi) L[(int64_t)gi * n + gj] = v.x;
-        if (gj + 1 <= gi) L[(int64_t)gi * n + gj + 1] = v.y;
+        if (gj <= gi) L[(int64_t)gi * n + gj] = (TM)v.x;
+        if (gj + 1 <= gi) L[(int64_t)gi * n + gj + 1] = (TM)v.y;
     }
     return first;
 }
 
-// Row gi, columns gj and gj + 1 (gj even) of an n-column row-major matrix.
-__device__ __forceinline__ void store_pair(double *M, int n, int gi, int gj, double x0, double x1) {
+// Row gi, columns gj and gj + 1 (gj even) of an n-column row-major matrix
+// of TM (double, or float rounded from the FP64 values).
+template <typename TM>
+__device__ __forceinline__ void store_pair(TM *M, int n, int gi, int gj, double x0, double x1) {
     if (gi >= n) return;
-    double *p = M + (int64_t)gi * n + gj;
-    if (gj + 1 < n && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-        *reinterpret_cast<double2 *>(p) = make_double2(x0, x1);
+    TM *p = M + (int64_t)gi * n + gj;
+    if (gj + 1 < n && (reinterpret_cast<uintptr_t>(p) & (2 * sizeof(TM) - 1)) == 0) {
+        if constexpr (sizeof(TM) == 8)
+            *reinterpret_cast<double2 *>(p) = make_double2(x0, x1);
+        else
+            *reinterpret_cast<float2 *>(p) = make_float2((float)x0, (float)x1);
     } else {
-        if (gj < n) p[0] = x0;
-        if (gj + 1 < n) p[1] = x1;
+        if (gj < n) p[0] = (TM)x0;
+        if (gj + 1 < n) p[1] = (TM)x1;
     }
 }
 
@@ -177,17 +184,19 @@ __device__ __forceinline__ void group_sync() {
 // matrix, spread the serial diagonal work over the SM's schedulers: tile D's
 // diagonal factorization runs in warp (D + off) % WPM, right-hand-side block
 // I of the back substitution in warp (I + off) % WPM, with `off` per CTA.
-template <int WPM>
+// TIO: the batch's element type.  FP32 batches are loaded into the same FP64
+// tiles and computed in FP64; L and X are rounded to FP32 on the way out.
+template <int WPM, typename TIO>
 __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *smem, int off,
                                int *s_info) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int M = WPM - 1;  // WPM is a power of two
     const int n = args.ns[idx], nrhs = args.nrhs;
     const int T = (n + 7) >> 3;
-    const double *A = static_cast<const double *>(args.A) + args.a_off[idx];
-    double *L = static_cast<double *>(args.L) + args.a_off[idx];
-    const double *B = static_cast<const double *>(args.B) + args.b_off[idx];
-    double *X = static_cast<double *>(args.X) + args.b_off[idx];
+    const TIO *A = static_cast<const TIO *>(args.A) + args.a_off[idx];
+    TIO *L = static_cast<TIO *>(args.L) + args.a_off[idx];
+    const TIO *B = static_cast<const TIO *>(args.B) + args.b_off[idx];
+    TIO *X = static_cast<TIO *>(args.X) + args.b_off[idx];
     double *TS = smem;                        // T(T+1)/2 tiles, swizzled
     double *RB = TS + T * (T + 1) / 2 * 64;   // T blocks of nrhs x 8: B^T, Y^T, X^T
     double *DI = RB + T * 8 * nrhs;           // 8T inverted pivots
@@ -202,7 +211,7 @@ __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *sm
     // (l/4, 2(l%4)) and (l/4, 2(l%4) + 1), as one 16-byte copy when the pair
     // is in range and aligned.  Out of range (past n, or above the diagonal)
     // is zero-filled.
-    {
+    if constexpr (sizeof(TIO) == 8) {
         const unsigned ts0 = (unsigned)__cvta_generic_to_shared(TS);
         const int ntile = T * (T + 1) / 2;
         int I = 0, J = warp;
@@ -244,6 +253,68 @@ __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *sm
                          : "memory");
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
+    } else {
+        // FP32: the elements go by cp.async (all in flight) to FP32 slots at
+        // the start of the tile region, element e (tile slot * 64 + swizzled
+        // position) at float index e; then they are widened in place from the
+        // top down: element e's FP64 value overwrites only the FP32 slots of
+        // elements 2e and 2e + 1, already read by then.
+        float *TF = reinterpret_cast<float *>(TS);
+        const unsigned tf0 = (unsigned)__cvta_generic_to_shared(TF);
+        const int ntile = T * (T + 1) / 2;
+        int I = 0, J = warp;
+        while (J > I) {
+            J -= I + 1;
+            ++I;
+        }
+        for (int s = warp; s < ntile; s += WPM) {
+            const int gi = 8 * I + r, gj = 8 * J + 2 * cp;
+            const bool ok0 = gi < n && gj <= gi, ok1 = gi < n && gj + 1 <= gi;
+            const TIO *src = ok0 ? A + (int64_t)gi * n + gj : A;
+            const unsigned dst = tf0 + 4u * (unsigned)(s * 64 + swz(r, 2 * cp));
+            if (ok1 && (reinterpret_cast<uintptr_t>(src) & 7) == 0) {
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src)
+                             : "memory");
+            } else {
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src),
+                             "r"(ok0 ? 4 : 0)
+                             : "memory");
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst + 4u),
+                             "l"(ok1 ? src + 1 : A), "r"(ok1 ? 4 : 0)
+                             : "memory");
+            }
+            J += WPM;
+            while (J > I) {
+                J -= I + 1;
+                ++I;
+            }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        group_sync<WPM>();
+        constexpr int kPer = 8;  // elements per thread per chunk
+        constexpr int kChunk = kPer * WPM * 32;
+        const int nel = ntile * 64;
+        for (int top = nel; top > 0; top -= kChunk) {
+            const int lo = max(0, top - kChunk);
+            float v[kPer];
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int e = lo + threadIdx.x + u * WPM * 32;
+                v[u] = e < top ? TF[e] : 0.f;
+            }
+            group_sync<WPM>();
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int e = lo + threadIdx.x + u * WPM * 32;
+                if (e < top) TS[e] = (double)v[u];
+            }
+            group_sync<WPM>();
+        }
+        for (int e = threadIdx.x; e < T * 8 * nrhs; e += WPM * 32) {
+            const int Jb = e / (8 * nrhs), rem = e - Jb * 8 * nrhs, rr = rem >> 3, cc = rem & 7;
+            const int gj = 8 * Jb + cc;
+            RB[e] = gj < n ? (double)B[(int64_t)gj * nrhs + rr] : 0.0;
+        }
     }
     group_sync<WPM>();
     if (warp == (off & M)) {
@@ -423,7 +494,7 @@ __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *sm
                 const int h = 2 * cp + e;
                 if (h < nrhs) {
                     yj[h * 8 + r] = x[e];
-                    if (gj < n) X[(int64_t)gj * nrhs + h] = x[e];
+                    if (gj < n) X[(int64_t)gj * nrhs + h] = (TIO)x[e];
                 }
             }
         };
@@ -453,7 +524,7 @@ __device__ void potrf_tile_one(const BatchedPotrfArgs &args, int idx, double *sm
 
 // Registers capped so that the shapes meant for small matrices keep many
 // CTAs per SM: 16 one-warp, 8 two-warp, 3 four-warp, 2 eight-warp CTAs.
-template <int WPM>
+template <int WPM, typename TIO>
 __global__ void __launch_bounds__(WPM * 32, WPM == 4 ? 3 : 512 / (WPM * 32))
     potrf_tile_batched_kernel(BatchedPotrfArgs args, int begin, int end, int nmax, int *counter) {
     double *S = reinterpret_cast<double *>(bp_smem);
@@ -474,7 +545,7 @@ __global__ void __launch_bounds__(WPM * 32, WPM == 4 ? 3 : 512 / (WPM * 32))
         const int item = begin + s_item, off = s_off;
         __syncthreads();
         if (item >= end) break;
-        potrf_tile_one<WPM>(args, args.order[item], S, off, &s_info);
+        potrf_tile_one<WPM, TIO>(args, args.order[item], S, off, &s_info);
         __syncthreads();
     }
 }

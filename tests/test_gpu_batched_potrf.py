@@ -214,18 +214,21 @@ def test_batched_f32_full_config_vs_oracle_sample(oracle):
     assert worst_x <= 1e-5, worst_x
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("threads", [128, 192])
-def test_batched_packed_shape_f64_matches_oracle(oracle, threads):
-    """The packed-triangle kernel forced on FP64 (the plan's default is the
-    tile kernel) against the oracle on ragged sizes that shape covers."""
+def test_batched_packed_shape_matches_oracle(oracle, threads, dtype):
+    """The packed-triangle kernel forced on both element types (the plan's
+    default is the tile kernel) against the oracle on ragged sizes that shape
+    covers."""
     import numax_b200 as nb
     hi = 128 if threads == 192 else 96
     rng = np.random.Generator(np.random.PCG64(threads))
     ns = np.array([1, 8, 9, 16, 17, 33, 64, 65, hi] + list(rng.integers(1, hi + 1, size=150)),
                   dtype=np.int32)
     nrhs = 4
-    A, B = make_batch(ns, nrhs, np.float64, seed=threads)
-    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float64)
+    A, B = make_batch(ns, nrhs, dtype, seed=threads)
+    dt = torch.float64 if dtype == np.float64 else torch.float32
+    plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=dt)
     assert all(s["threads"] == threads for s in plan.force_shape(threads))
     gotA, gotX, info = plan(torch.from_numpy(A.copy()).cuda(), torch.from_numpy(B.copy()).cuda())
     wantL, wantX = oracle.batched_cholesky_solve(ns, A, B, nrhs)
@@ -234,18 +237,52 @@ def test_batched_packed_shape_f64_matches_oracle(oracle, threads):
     assert (info.cpu().numpy() == 0).all()
     for i, n in enumerate(ns):
         blk = gotA[ao[i]:ao[i] + n * n].reshape(n, n)
-        assert relerr(np.tril(blk), np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= 1e-12
-    assert relerr(gotX, wantX) <= 1e-12
+        assert relerr(np.tril(blk), np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= TOL[dtype]
+    assert relerr(gotX, wantX) <= TOL[dtype]
 
 
-def test_batched_default_shapes_f64():
-    """The FP64 plan's default schedule: the tile kernel, 1 warp per matrix
-    up to n = 64, 2 up to 96, 4 up to 128."""
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_batched_default_shapes(dt):
+    """The plan's default schedule for both element types: the tile kernel,
+    1 warp per matrix up to n = 64, 2 up to 96, 4 up to 128."""
     import numax_b200 as nb
     ns = np.array([20, 50, 90, 120], dtype=np.int32)
-    sched = nb.CholeskySolveBatch(ns, nrhs=4, dtype=torch.float64).schedule()
+    sched = nb.CholeskySolveBatch(ns, nrhs=4, dtype=dt).schedule()
     assert [(s["n_max"], s["threads"]) for s in sched] == [(120, 1128), (90, 1064), (50, 1032),
                                                           (20, 1032)]
+
+
+@pytest.mark.parametrize("warps", [1, 2, 4, 8])
+def test_batched_tile_shape_f32_matches_oracle(oracle, warps):
+    """The tile kernel on an FP32 batch (widened to FP64 on load, rounded on
+    store) against the oracle's FP32 algorithm: ragged sizes around every tile
+    edge, 0 and 4 right-hand sides, within FP32 tolerance."""
+    import numax_b200 as nb
+    shape = nb.batched.tile_shape(warps)
+    edge = [1, 2, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65, 95, 96, 97, 120, 127, 128]
+    rng = np.random.Generator(np.random.PCG64(512 + warps))
+    for nrhs in (0, 4):
+        ns = np.array(edge + list(rng.integers(1, 129, size=100)), dtype=np.int32)
+        rng.shuffle(ns)
+        A, B = make_batch(ns, nrhs, np.float32, seed=nrhs + 70)
+        plan = nb.CholeskySolveBatch(ns, nrhs=nrhs, dtype=torch.float32)
+        assert all(s["threads"] == shape for s in plan.force_shape(shape))
+        dA = torch.from_numpy(A.copy()).cuda()
+        dB = torch.from_numpy(B.copy()).cuda() if nrhs else None
+        gotA, gotX, info = plan(dA, dB)
+        gotA, info = gotA.cpu().numpy(), info.cpu().numpy()
+        wantL, wantX = oracle.batched_cholesky_solve(ns, A, B if nrhs else np.zeros(0, np.float32), nrhs)
+        ao, bo = oracle.ragged_offsets(ns), oracle.ragged_offsets(ns, nrhs)
+        assert (info == 0).all()
+        for i, n in enumerate(ns):
+            blk = gotA[ao[i]:ao[i] + n * n].reshape(n, n)
+            assert relerr(np.tril(blk), np.tril(wantL[ao[i]:ao[i] + n * n].reshape(n, n))) <= 1e-5
+            np.testing.assert_array_equal(np.triu(blk, 1),
+                                          np.triu(A[ao[i]:ao[i] + n * n].reshape(n, n), 1))
+        if nrhs:
+            gotX = gotX.cpu().numpy()
+            for i, n in enumerate(ns):
+                assert relerr(gotX[bo[i]:bo[i] + n * nrhs], wantX[bo[i]:bo[i] + n * nrhs]) <= 1e-5
 
 
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
