@@ -261,6 +261,153 @@ static int potrf_rec(const GemmSub &gs, T *A, int64_t lda, int c, int w, int32_t
     return potrf_rec<T>(gs, A, lda, c + hw, w - hw, info);
 }
 
+// ---- blocked right-looking driver of the FP64 / FP32 entry points ----------
+// Per 64-column block column k: one panel launch factors the diagonal block
+// and solves the rows below it, then one lower-triangle SYRK updates the
+// trailing matrix.  Every CTA of the panel factors the 64 x 64 diagonal block
+// itself (the same code on the same data, so all agree bit for bit) and
+// forms its inverse, so no CTA waits for another; CTA b then solves rows
+// [k + jb + 64 b, +64) as X = R L_kk^-T = R W^T, and CTA 0 writes L_kk.
+constexpr int kCholNb = 64;
+constexpr int kCholPanelThreads = 256;
+
+template <typename T>
+__host__ __device__ constexpr size_t chol_panel_smem() {
+    return sizeof(T) * 3 * (size_t)kCholNb * (kCholNb + 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCholPanelThreads)
+    chol_panel_kernel(T *A, int64_t lda, int n, int k, int jb, int32_t *info) {
+    extern __shared__ __align__(16) unsigned char cp_smem[];
+    constexpr int ld = kCholNb + 1;
+    constexpr int NT = kCholPanelThreads;
+    T *D = reinterpret_cast<T *>(cp_smem);  // the diagonal block, then L_kk
+    T *Wm = D + kCholNb * ld;               // W = L_kk^-1 (lower), zeros above
+    T *R = Wm + kCholNb * ld;               // this CTA's rows of the panel
+    __shared__ T s_l[kCholNb];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    const int r0 = k + jb + blockIdx.x * kCholNb, nr = max(0, min(kCholNb, n - r0));
+    {
+        // The diagonal block's lower triangle and this CTA's rows, all copies
+        // in flight (cp.async); the rest of D and W starts at zero, W = I.
+        auto async_copy = [](T *dst, const T *src) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+            if constexpr (sizeof(T) == 8)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+        };
+        for (int e = tid; e < jb * jb; e += NT) {
+            const int i = e / jb, j = e - i * jb;
+            if (j <= i)
+                async_copy(&D[i * ld + j], &A[(int64_t)(k + i) * lda + k + j]);
+            else
+                D[i * ld + j] = T(0);
+        }
+        for (int e = tid; e < nr * jb; e += NT) {
+            const int i = e / jb, j = e - i * jb;
+            async_copy(&R[i * ld + j], &A[(int64_t)(r0 + i) * lda + k + j]);
+        }
+        for (int e = tid; e < kCholNb * kCholNb; e += NT) {
+            const int i = e / kCholNb, j = e - i * kCholNb;
+            Wm[i * ld + j] = (i == j && i < jb) ? T(1) : T(0);
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    // numax's potrf_diag rule per column: a pivot d <= 0 is recorded (first
+    // one, 1-based) and floored; l_jj = d / sqrt(d), l_ij = a_ij / sqrt(d).
+    // W = L^-1 is formed alongside by elimination: row j of W is scaled by
+    // 1/sqrt(d), then rows i > j lose l_ij times it.
+    for (int j = 0; j < jb; ++j) {
+        T d = D[j * ld + j];
+        if (d <= T(0)) {
+            if (tid == 0 && s_bad == 0) s_bad = k + j + 1;
+            d = pivot_floor<T>::value;
+        }
+        const T inv = rsqrt(d);
+        if (tid == 0) s_l[j] = d * inv;
+        for (int i = j + 1 + tid; i < jb; i += NT) D[i * ld + j] *= inv;
+        for (int c = tid; c <= j; c += NT) Wm[j * ld + c] *= inv;
+        __syncthreads();
+        // D22 -= l l^T on the lower triangle below column j; W's rows below
+        // j lose l_ij times row j.  Four lanes per row.
+        for (int i = j + 1 + (tid >> 2); i < jb; i += NT / 4) {
+            const T lij = D[i * ld + j];
+#pragma unroll 4
+            for (int l = j + 1 + (tid & 3); l <= i; l += 4) D[i * ld + l] -= lij * D[l * ld + j];
+#pragma unroll 4
+            for (int c = tid & 3; c <= j; c += 4) Wm[i * ld + c] -= lij * Wm[j * ld + c];
+        }
+        __syncthreads();
+    }
+    for (int j = tid; j < jb; j += NT) D[j * ld + j] = s_l[j];
+    __syncthreads();
+    if (blockIdx.x == 0) {
+        for (int e = tid; e < jb * jb; e += NT) {
+            const int i = e / jb, j = e - i * jb;
+            if (j <= i) A[(int64_t)(k + i) * lda + k + j] = D[i * ld + j];
+        }
+        if (tid == 0 && s_bad && *info == 0) *info = s_bad;
+    }
+    // X = R W^T for this CTA's rows: thread (rows 4 (t / 16) + u, columns
+    // 4 (t % 16) + v), W's zeros above the diagonal doing the masking.
+    if (nr > 0) {
+        const int rb = 4 * (tid / 16), cb = 4 * (tid % 16);
+        T acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = T(0);
+        for (int l = 0; l < jb; ++l) {
+            T rv[4], wv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) rv[u] = rb + u < nr ? R[(rb + u) * ld + l] : T(0);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) wv[v] = Wm[(cb + v) * ld + l];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fma(rv[u], wv[v], acc[u][v]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (rb + u < nr && cb + v < jb)
+                    A[(int64_t)(r0 + rb + u) * lda + k + cb + v] = acc[u][v];
+    }
+}
+
+template <typename T>
+static int potrf_blocked(const GemmSub &gs, T *A, int64_t lda, int n, int32_t *info) {
+    static bool attr_set[64][2] = {};
+    int dev = 0;
+    NMX_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr_set[dev][sizeof(T) == 8]) {
+        NMX_CUDA_TRY(cudaFuncSetAttribute(chol_panel_kernel<T>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)chol_panel_smem<T>()));
+        attr_set[dev][sizeof(T) == 8] = true;
+    }
+    for (int k = 0; k < n; k += kCholNb) {
+        const int jb = std::min(kCholNb, n - k);
+        const int below = n - k - jb;
+        const int grid = std::max(1, (int)ceil_div(below, kCholNb));
+        chol_panel_kernel<T><<<grid, kCholPanelThreads, chol_panel_smem<T>(), gs.st>>>(A, lda, n, k,
+                                                                                     jb, info);
+        NMX_CUDA_TRY(cudaGetLastError());
+        if (below > 0)
+            NMX_TRY(gs.sub_bt(below, below, jb, A + (int64_t)(k + jb) * lda + k, lda,
+                              A + (int64_t)(k + jb) * lda + k, lda,
+                              A + (int64_t)(k + jb) * lda + k + jb, lda, true));
+    }
+    return 0;
+}
+
 template <typename T>
 static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void *stream) {
     NMX_ARG_CHECK(ctx != nullptr, 1, "ctx is NULL");
@@ -274,7 +421,7 @@ static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void 
     if (n == 0) return 0;
     GemmSub gs;
     gs.st = st;
-    int rc = potrf_rec<T>(gs, A, lda, 0, (int)n, info);
+    int rc = potrf_blocked<T>(gs, A, lda, (int)n, info);
     if (rc) return rc;
     const int threads = 256;
     zero_upper_kernel<T><<<(unsigned)ceil_div(n * n, threads), threads, 0, st>>>(A, lda, (int)n);
