@@ -278,7 +278,7 @@ __host__ __device__ constexpr size_t chol_panel_smem() {
 
 template <typename T>
 __global__ void __launch_bounds__(kCholPanelThreads)
-    chol_panel_kernel(T *A, int64_t lda, int n, int k, int jb, int32_t *info) {
+    chol_panel_kernel(T *A, int64_t lda, int n, int k, int jb, int c0, int32_t *info) {
     extern __shared__ __align__(16) unsigned char cp_smem[];
     constexpr int ld = kCholNb + 1;
     constexpr int NT = kCholPanelThreads;
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kCholPanelThreads)
     for (int j = 0; j < jb; ++j) {
         T d = D[j * ld + j];
         if (d <= T(0)) {
-            if (tid == 0 && s_bad == 0) s_bad = k + j + 1;
+            if (tid == 0 && s_bad == 0) s_bad = c0 + k + j + 1;
             d = pivot_floor<T>::value;
         }
         const T inv = rsqrt(d);
@@ -382,8 +382,10 @@ __global__ void __launch_bounds__(kCholPanelThreads)
     }
 }
 
+// A holds the n x n block whose first column is column c0 of the whole
+// matrix (for `info`).
 template <typename T>
-static int potrf_blocked(const GemmSub &gs, T *A, int64_t lda, int n, int32_t *info) {
+static int potrf_blocked(const GemmSub &gs, T *A, int64_t lda, int n, int c0, int32_t *info) {
     static bool attr_set[64][2] = {};
     int dev = 0;
     NMX_CUDA_TRY(cudaGetDevice(&dev));
@@ -398,7 +400,7 @@ static int potrf_blocked(const GemmSub &gs, T *A, int64_t lda, int n, int32_t *i
         const int below = n - k - jb;
         const int grid = std::max(1, (int)ceil_div(below, kCholNb));
         chol_panel_kernel<T><<<grid, kCholPanelThreads, chol_panel_smem<T>(), gs.st>>>(A, lda, n, k,
-                                                                                     jb, info);
+                                                                                     jb, c0, info);
         NMX_CUDA_TRY(cudaGetLastError());
         if (below > 0)
             NMX_TRY(gs.sub_bt(below, below, jb, A + (int64_t)(k + jb) * lda + k, lda,
@@ -406,6 +408,22 @@ static int potrf_blocked(const GemmSub &gs, T *A, int64_t lda, int n, int32_t *i
                               A + (int64_t)(k + jb) * lda + k + jb, lda, true));
     }
     return 0;
+}
+
+// Recursive halves above kCholBlockedMax columns (a few large SYRK / TRSM
+// products), the blocked driver below (short chains of launches).
+constexpr int kCholBlockedMax = 4096;
+
+template <typename T>
+static int potrf_hybrid(const GemmSub &gs, T *A, int64_t lda, int c, int w, int32_t *info) {
+    if (w <= kCholBlockedMax) return potrf_blocked<T>(gs, A + (int64_t)c * lda + c, lda, w, c, info);
+    const int hw = (w / 2 + kCholLeaf - 1) / kCholLeaf * kCholLeaf;
+    NMX_TRY(potrf_hybrid<T>(gs, A, lda, c, hw, info));
+    NMX_TRY(trsm_right_lt<T>(gs, A, lda, c, hw, c + hw, c + w));
+    NMX_TRY(gs.sub_bt(w - hw, w - hw, hw, A + (int64_t)(c + hw) * lda + c, lda,
+                      A + (int64_t)(c + hw) * lda + c, lda, A + (int64_t)(c + hw) * lda + c + hw,
+                      lda, true));
+    return potrf_hybrid<T>(gs, A, lda, c + hw, w - hw, info);
 }
 
 template <typename T>
@@ -421,7 +439,7 @@ static int potrf(nmx_ctx ctx, int64_t n, T *A, int64_t lda, int32_t *info, void 
     if (n == 0) return 0;
     GemmSub gs;
     gs.st = st;
-    int rc = potrf_blocked<T>(gs, A, lda, (int)n, info);
+    int rc = potrf_hybrid<T>(gs, A, lda, 0, (int)n, info);
     if (rc) return rc;
     const int threads = 256;
     zero_upper_kernel<T><<<(unsigned)ceil_div(n * n, threads), threads, 0, st>>>(A, lda, (int)n);
