@@ -414,14 +414,26 @@ __global__ void laswp_kernel(T *A, int64_t lda, int ncols, int c, int w, const i
 
 // X := L^-1 X for the w x w (w <= 32) lower block L at (r, r) of A (unit or
 // not) and X = rows [r, r+w) x cols [c0, c1) of B.  One thread per column.
+// cp.async of one element (4 or 8 bytes) into shared memory.
+template <typename T>
+__device__ __forceinline__ void leaf_copy_async(T *dst, const T *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 template <typename T, bool UNIT>
 __global__ void trsm_lower_leaf_kernel(const T *A, int64_t lda, int r, int w, T *B, int64_t ldb,
                                        int c0, int c1) {
     __shared__ T Ls[kTrsmLeaf][kTrsmLeaf + 1];
+    // The block's copies all in flight (cp.async), then one wait.
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         int i = e / w, j = e - i * w;
-        Ls[i][j] = A[(int64_t)(r + i) * lda + r + j];
+        leaf_copy_async(&Ls[i][j], &A[(int64_t)(r + i) * lda + r + j]);
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= c1) return;
@@ -449,14 +461,12 @@ template <typename T, bool TRANS>
 __global__ void trsm_upper_leaf_kernel(const T *A, int64_t lda, int r, int w, T *B, int64_t ldb,
                                        int c0, int c1) {
     __shared__ T Us[kTrsmLeaf][kTrsmLeaf + 1];
+    // The block's copies all in flight (cp.async; TRANS lands transposed).
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         int i = e / w, j = e - i * w;
-        T v = A[(int64_t)(r + i) * lda + r + j];
-        if (TRANS)
-            Us[j][i] = v;
-        else
-            Us[i][j] = v;
+        leaf_copy_async(TRANS ? &Us[j][i] : &Us[i][j], &A[(int64_t)(r + i) * lda + r + j]);
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= c1) return;

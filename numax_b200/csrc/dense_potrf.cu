@@ -67,10 +67,17 @@ template <typename T>
 __global__ void trsm_right_lt_leaf_kernel(T *A, int64_t lda, int c, int w, int r0, int r1) {
     __shared__ T Ls[kCholLeaf][kCholLeaf + 1];
     __shared__ T inv_d[kCholLeaf];
+    // The block's copies all in flight (cp.async), then one wait.
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         int i = e / w, j = e - i * w;
-        Ls[i][j] = A[(int64_t)(c + i) * lda + c + j];
+        const unsigned d = (unsigned)__cvta_generic_to_shared(&Ls[i][j]);
+        const T *src = &A[(int64_t)(c + i) * lda + c + j];
+        if constexpr (sizeof(T) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     // Reciprocals of the diagonal once per block, so each row's solve is a
     // chain of multiply-adds without a division per column.
