@@ -595,6 +595,107 @@ __global__ void __launch_bounds__(kTrsmThreads)
         for (int i = warp; i < w; i += NW) B[(int64_t)(r + i) * ldb + col] = X[i * kTrsmXPitch + lane];
 }
 
+// The same solve for FP64 (and any T): X := L^-1 X for the unit lower w x w
+// block (w <= 256, a multiple of 32), a CTA per 32 columns.  Every copy into
+// shared memory goes by cp.async (the CTA's X, the diagonal blocks, and per
+// block step the rows of L below it), so each is one round trip.
+constexpr int kTrsmTPitchX = 33;
+constexpr int kTrsmTPitchL = 33;
+template <typename T>
+__host__ __device__ constexpr size_t trsm_unit_lower_t_smem(int w) {
+    return sizeof(T) * ((size_t)w * kTrsmTPitchX * 2 + (size_t)(w - 32) * kTrsmTPitchL);
+}
+
+template <typename T>
+__device__ __forceinline__ void trsm_copy_async(T *dst, const T *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+                     "r"(ok ? 8 : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
+                     "r"(ok ? 4 : 0)
+                     : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTrsmThreads)
+    trsm_unit_lower_t_kernel(const T *A, int64_t lda, int r, int w, T *B, int64_t ldb, int c0,
+                             int c1) {
+    extern __shared__ __align__(16) unsigned char tsm_raw[];
+    T *X = reinterpret_cast<T *>(tsm_raw);  // [w][33] the CTA's 32 columns of X
+    T *Li = X + w * kTrsmTPitchX;             // [w/32][32][33] inverted diagonal blocks
+    T *Ls = Li + w * kTrsmTPitchX;            // [w-32][33] L below the current block
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kTrsmThreads / 32;
+    const int nb = w / 32;
+    const int col = c0 + blockIdx.x * 32 + lane;
+    const bool cv = col < c1;
+    for (int i = warp; i < w; i += NW)
+        trsm_copy_async(&X[i * kTrsmTPitchX + lane], cv ? &B[(int64_t)(r + i) * ldb + col] : B, cv);
+    if (warp < nb) {
+        const int rb = r + 32 * warp;
+        T *D = Li + warp * 32 * kTrsmTPitchX;
+        for (int i = 0; i < 32; ++i)
+            trsm_copy_async(&D[i * kTrsmTPitchX + lane], &A[(int64_t)(rb + i) * lda + rb + lane], true);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    if (warp < nb) {
+        // Lane j forms column j of the inverse by forward substitution.
+        T *D = Li + warp * 32 * kTrsmTPitchX;
+        T x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            T t = T(0);
+#pragma unroll
+            for (int p = 0; p < i; ++p) t = fma(D[i * kTrsmTPitchX + p], x[p], t);
+            x[i] = i == lane ? T(1) : (i < lane ? T(0) : -t);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) D[i * kTrsmTPitchX + lane] = x[i];
+    }
+    __syncthreads();
+    for (int b = 0; b < nb; ++b) {
+        const int rb = 32 * b, below = w - rb - 32;
+        for (int i = warp; i < below; i += NW)
+            trsm_copy_async(&Ls[i * kTrsmTPitchL + lane],
+                            &A[(int64_t)(r + rb + 32 + i) * lda + r + rb + lane], true);
+        {
+            const T *D = Li + b * 32 * kTrsmTPitchX;
+            T y[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll 8
+            for (int p = 0; p < 32; ++p) {
+                const T xp = X[(rb + p) * kTrsmTPitchX + lane];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) y[q] = fma(D[(4 * warp + q) * kTrsmTPitchX + p], xp, y[q]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; ++q) X[(rb + 4 * warp + q) * kTrsmTPitchX + lane] = y[q];
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        if (below > 0) {
+            T xb[32];
+#pragma unroll
+            for (int p = 0; p < 32; ++p) xb[p] = X[(rb + p) * kTrsmTPitchX + lane];
+            for (int i = warp; i < below; i += NW) {
+                const T *lr = Ls + i * kTrsmTPitchL;
+                T t = T(0);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) t = fma(lr[q], xb[q], t);
+                X[(rb + 32 + i) * kTrsmTPitchX + lane] -= t;
+            }
+        }
+        __syncthreads();
+    }
+    if (cv)
+        for (int i = warp; i < w; i += NW) B[(int64_t)(r + i) * ldb + col] = X[i * kTrsmTPitchX + lane];
+}
+
 // The row moves of LAPACK-style interchanges ipiv[c .. c+w) (w <= 32), as a
 // list: one warp replays the swaps on the positions they touch (lane k
 // tracks position c + k and, from step k on, possibly one more), then lists

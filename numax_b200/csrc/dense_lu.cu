@@ -647,6 +647,25 @@ int trsm_lower(const GemmSub &gs, const T *A, int64_t lda, int r, int w, T *B, i
                int c1) {
     cudaStream_t st = gs.st;
     if (w <= 0 || c1 <= c0) return 0;
+    if constexpr (UNIT && sizeof(T) == 8) {
+        // Unit lower blocks of 64..256 rows (multiples of 32): one kernel.
+        if (w > kTrsmLeaf && w <= kTrsmMaxW && w % 32 == 0) {
+            static bool attr_set[64] = {};
+            int dev = 0;
+            NMX_CUDA_TRY(cudaGetDevice(&dev));
+            if (dev < 64 && !attr_set[dev]) {
+                NMX_CUDA_TRY(cudaFuncSetAttribute(trsm_unit_lower_t_kernel<T>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)trsm_unit_lower_t_smem<T>(kTrsmMaxW)));
+                attr_set[dev] = true;
+            }
+            trsm_unit_lower_t_kernel<T><<<(unsigned)ceil_div(c1 - c0, 32), kTrsmThreads,
+                                          trsm_unit_lower_t_smem<T>(w), st>>>(A, lda, r, w, B, ldb,
+                                                                              c0, c1);
+            NMX_CUDA_TRY(cudaGetLastError());
+            return 0;
+        }
+    }
     if (w <= kTrsmLeaf) {
         int threads = 128;
         trsm_lower_leaf_kernel<T, UNIT>
