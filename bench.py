@@ -821,6 +821,13 @@ def run_ours(args):
         except Exception as exc:
             dense = {"error": f"{type(exc).__name__}: {exc}"}
 
+    npy = None
+    if world == 1 and args.npy_gib > 0:
+        try:
+            npy = run_npy(dev, A, args.npy_gib)
+        except Exception as exc:
+            npy = {"error": f"{type(exc).__name__}: {exc}"}
+
     lu_ir = None
     if world == 1 and args.lu_n:
         lu_ir = run_lu_ir_legs(args, dev)
@@ -861,9 +868,55 @@ def run_ours(args):
         "eigh": eigh,
         "dense": dense,
         "lu_ir": lu_ir,
+        "npy": npy,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_npy(dev, A, gib=1.0, reps=3):
+    """The .npy seam: save a `gib` GiB slice of the batch from HBM to a
+    file and load it back into HBM (nmx_npy_save / nmx_npy_load, pinned
+    staging, chunked reads overlapping the copies), against the numax-style
+    path of a whole-file host read followed by one copy to the device
+    (numpy.load, then torch .to(device)).  Wall-clock per synchronous call,
+    best of `reps`; the file sits in the page cache (tmpfs when /dev/shm
+    exists), so this is the host pipeline's rate, not a disk's.  The loaded
+    bytes are compared with the source."""
+    import shutil
+    import tempfile
+    import time
+    import torch
+    from numax_b200.io import numpy as npx
+    esize = A.element_size()
+    n = min(int(gib * (1 << 30)) // esize, A.numel())
+    src = A[:n]
+    base = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    tmp = tempfile.mkdtemp(prefix="nmx_npy_", dir=base)
+    path = os.path.join(tmp, "slice.npy")
+    try:
+        def best(fn):
+            ts = []
+            for _ in range(reps):
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                out = fn()
+                torch.cuda.synchronize(dev)
+                ts.append(time.perf_counter() - t0)
+            return min(ts), out
+        t_save, _ = best(lambda: npx.save(src, path))
+        t_load, got = best(lambda: npx.load(path, src.dtype, n, device=dev))
+        same = bool(torch.equal(got.view(torch.uint8), src.view(torch.uint8)))
+        del got
+        t_ref, ref = best(lambda: torch.from_numpy(np.load(path)).to(dev))
+        del ref
+        nbytes = n * esize
+        return {"bytes": nbytes, "file_system": "tmpfs (/dev/shm)" if base else "tmp",
+                "save_gbs": nbytes / t_save / 1e9, "load_gbs": nbytes / t_load / 1e9,
+                "numpy_load_then_copy_gbs": nbytes / t_ref / 1e9,
+                "load_speedup": t_ref / t_load, "bit_exact": same}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def run_big_bucket(args):
@@ -928,6 +981,10 @@ def main():
                     help="matrices in the batched Jacobi eigh leg (0 skips it)")
     ap.add_argument("--only-qr", action="store_true",
                     help="run only the FP32 QR leg (geqrf + orgqr of 262144 x 256), for profiling")
+    ap.add_argument("--npy-gib", type=float, default=1.0,
+                    help="GiB of the .npy save/load leg (0 skips it)")
+    ap.add_argument("--only-npy", action="store_true",
+                    help="run only the .npy save/load leg")
     ap.add_argument("--only-big", action="store_true",
                     help="run only the n in 97..128 bucket of the batch (the dominant kernel), "
                          "default schedule, for profiling")
@@ -941,6 +998,14 @@ def main():
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
         torch.cuda.set_device(dev)
         print(json.dumps({"dense": run_dense(dev, orders=())}), flush=True)
+        return 0
+    if args.only_npy:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        ns, seed = shard(0, args.count, 1)
+        A, _ = make_batch_torch(ns, NRHS, torch.float64, dev, seed)
+        print(json.dumps({"npy": run_npy(dev, A, args.npy_gib)}), flush=True)
         return 0
     if args.only_dense:
         import torch

@@ -43,9 +43,24 @@ extern "C" {
 #define NMX_ERR_ALLOC (-1001)      /* device or host allocation failed */
 #define NMX_ERR_UNSUPPORTED (-1002)/* device is not sm_100 / feature absent */
 #define NMX_ERR_INTERNAL (-1003)   /* internal error (bounded wait expired, ...) */
+#define NMX_ERR_IO (-1004)         /* a file could not be opened, read or written */
+#define NMX_ERR_FORMAT (-1005)     /* a file is not what the call asked for */
 
+/* Element types.  The factorizations take NMX_F32 / NMX_F64; the .npy
+ * interchange takes every code (NMX_BF16 has no numpy dtype). */
 #define NMX_F32 0
 #define NMX_F64 1
+#define NMX_F16 2
+#define NMX_I8 3
+#define NMX_I16 4
+#define NMX_I32 5
+#define NMX_I64 6
+#define NMX_U8 7
+#define NMX_U16 8
+#define NMX_U32 9
+#define NMX_U64 10
+#define NMX_BOOL 11
+#define NMX_BF16 12
 
 typedef struct nmx_context *nmx_ctx;
 typedef struct nmx_batched_plan_s *nmx_batched_plan;
@@ -493,6 +508,50 @@ NMX_API int nmx_posv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda
                             double *x, int mode, double tol, int max_iter, nmx_ir_stats *stats,
                             void *stream);
 NMX_API int nmx_posv_ir_reserve(nmx_ctx ctx, int64_t n, int mode);
+
+/* ---- .npy interchange ----------------------------------------------------
+ *
+ * Replaces numax's `numpy.save` / `numpy.load` / `numpy.load_dyn`
+ * (numax/io/npy.mojo:273-453): read what numpy.save wrote, write what
+ * numpy.load reads, format versions 1.0 and 2.0.  The payload is C order, so a
+ * (count, n, n) stack of matrices saved by numpy is already the batched
+ * entry points' layout (A_i at i * n * n) and loads into it with no host-side
+ * transpose; a ragged batch is a 1-D file of the matrices back to back.
+ *
+ * With ctx != NULL the array lives in device memory on ctx's device and the
+ * payload streams through pinned staging buffers kept in the context:
+ * worker threads read (write) fixed-size chunks of the file while earlier
+ * chunks are copied to (from) the device on `stream`.  With ctx == NULL the
+ * array is host memory and no CUDA call is made.  Both calls return when the
+ * data has landed (numax's calls are synchronous).
+ *
+ * Rejected, with numax's messages (nmx_last_error_string) and
+ * NMX_ERR_FORMAT: a file without the .npy magic (an .npz archive), format
+ * versions other than 1.x / 2.x, a truncated header, Fortran order, a
+ * big-endian descr, a descr naming another element type, a payload length
+ * that disagrees with the header, a rank or an extent other than the
+ * requested ones (npy.mojo:138-260, 349-453).  NMX_ERR_IO when the file
+ * cannot be opened, read or written.
+ */
+#define NMX_NPY_MAX_RANK 64
+/* The header of `path`: *dtype the NMX_* code its descr names (-1 when it
+ * names none of them), *rank, shape[0 .. rank) (room for max_rank entries),
+ * *payload_offset where the payload starts.  Any output may be NULL except
+ * shape when the file's rank is above 0. */
+NMX_API int nmx_npy_header(const char *path, int *dtype, int *rank, int64_t *shape, int max_rank,
+                           int64_t *payload_offset);
+/* Load `path` into `dst` (dst_bytes of room).  The file must hold `dtype`
+ * at rank `rank`; shape[i] >= 0 must equal the file's extent i (numax's
+ * `load`), shape[i] = -1 accepts any extent (numax's `load_dyn`).  On
+ * success shape[] holds the file's extents. */
+NMX_API int nmx_npy_load(nmx_ctx ctx, const char *path, int dtype, int rank, int64_t *shape,
+                         void *dst, int64_t dst_bytes, void *stream);
+/* Write the C-order array `src` (dtype, rank, shape) to `path`, the bytes
+ * numpy.save writes for it: the sorted-key header dict, numpy's spare space
+ * after it, padding to 64 bytes, the payload.  With ctx != NULL the copy
+ * out follows the work already queued on `stream`. */
+NMX_API int nmx_npy_save(nmx_ctx ctx, const char *path, int dtype, int rank,
+                         const int64_t *shape, const void *src, void *stream);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,8 @@ NMX_ERR_CUDA = -1000
 NMX_ERR_ALLOC = -1001
 NMX_ERR_UNSUPPORTED = -1002
 NMX_ERR_INTERNAL = -1003
+NMX_ERR_IO = -1004
+NMX_ERR_FORMAT = -1005
 
 _lock = threading.Lock()
 _lib = None
@@ -57,6 +59,9 @@ SIGNATURES = {
     "nmx_syevj_plan_schedule": (ci, [vp, vp, vp, vp, vp, ci, vp]),
     "nmx_syevj_batched_graph_f32": (ci, [vp, vp, vp, vp, vp, vp, C.c_double, ci, ci, vp]),
     "nmx_potrf_potrs_batched_noalloc_f64": (ci, [vp, i64, vp, ci, vp, vp, vp, vp, vp, vp]),
+    "nmx_npy_header": (ci, [C.c_char_p, C.POINTER(ci), C.POINTER(ci), vp, ci, C.POINTER(i64)]),
+    "nmx_npy_load": (ci, [vp, C.c_char_p, ci, ci, vp, vp, i64, vp]),
+    "nmx_npy_save": (ci, [vp, C.c_char_p, ci, ci, vp, vp, vp]),
     "nmx_getrf_f64": (ci, [vp, i64, vp, i64, vp, vp, vp]),
     "nmx_getrf_f32": (ci, [vp, i64, vp, i64, vp, vp, vp]),
     "nmx_getrs_f64": (ci, [vp, i64, i64, vp, i64, vp, vp, i64, vp]),

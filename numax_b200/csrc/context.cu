@@ -177,6 +177,8 @@ int nmx_destroy(nmx_ctx ctx) {
             if (ctx->la_stream[i]) cudaStreamDestroy(ctx->la_stream[i]);
             if (ctx->la_event[i]) cudaEventDestroy(ctx->la_event[i]);
         }
+        for (void *p : ctx->npy_pinned) cudaFreeHost(p);
+        for (cudaEvent_t e : ctx->npy_event) cudaEventDestroy(e);
     }
     delete ctx;
     return 0;

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/nmx_la.h"
 
@@ -86,6 +87,10 @@ struct nmx_context {
     static constexpr int kSlots = 11;
     void *slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
+    // Pinned host staging of the .npy load/save pipeline and, per buffer, the
+    // event of the copy that last used it (grown on first use).
+    std::vector<void *> npy_pinned;
+    std::vector<cudaEvent_t> npy_event;
     // Returns a device buffer of at least `bytes`, reusing the context's.
     int ensure_workspace(size_t bytes);
     // Same for slot `slot` (see nmx::WsSlot); *out receives the buffer.
