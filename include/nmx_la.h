@@ -509,6 +509,29 @@ NMX_API int nmx_posv_ir_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda
                             void *stream);
 NMX_API int nmx_posv_ir_reserve(nmx_ctx ctx, int64_t n, int mode);
 
+/* ---- symmetric eigendecomposition of one matrix --------------------------
+ *
+ * nmx_syevd_*: the eigenvalues (W, n, ascending) and, when V is not NULL,
+ * orthonormal eigenvectors (V's columns, row-major ldv, V[:, j] for W[j]) of
+ * the symmetric n x n row-major A (lda), reading only its lower triangle --
+ * numax's Tensor-tier eigh (numax/linalg/eigen.mojo:1268-1341); with
+ * V = NULL, numax's eigvalsh.  A is not modified.  The work is FP64 in both
+ * entry points (the FP32 one rounds its outputs): a Householder
+ * tridiagonalization in one cooperative launch, then Sturm bisection
+ * (values only) or divide and conquer on the tridiagonal, then the
+ * reflectors applied to the tridiagonal's eigenvectors.  *info (device
+ * int32) is 1 when A's lower triangle holds a NaN or an infinity (numax
+ * raises that its QL sweep did not converge), else 0; W and V are then
+ * filled with NaN.  Synchronous: returns after the work on `stream` is done
+ * (the divide and conquer sizes its products from counts it reads back).
+ * Order limit: n - 1 <= 8 x 16 x (SM count), 18,944 on a B200; the device
+ * workspace is about 5 n^2 doubles with vectors, n^2 without.
+ */
+NMX_API int nmx_syevd_f64(nmx_ctx ctx, int64_t n, const double *A, int64_t lda, double *W,
+                          double *V, int64_t ldv, int32_t *info, void *stream);
+NMX_API int nmx_syevd_f32(nmx_ctx ctx, int64_t n, const float *A, int64_t lda, float *W, float *V,
+                          int64_t ldv, int32_t *info, void *stream);
+
 /* ---- .npy interchange ----------------------------------------------------
  *
  * Replaces numax's `numpy.save` / `numpy.load` / `numpy.load_dyn`

@@ -59,6 +59,8 @@ SIGNATURES = {
     "nmx_syevj_plan_schedule": (ci, [vp, vp, vp, vp, vp, ci, vp]),
     "nmx_syevj_batched_graph_f32": (ci, [vp, vp, vp, vp, vp, vp, C.c_double, ci, ci, vp]),
     "nmx_potrf_potrs_batched_noalloc_f64": (ci, [vp, i64, vp, ci, vp, vp, vp, vp, vp, vp]),
+    "nmx_syevd_f64": (ci, [vp, i64, vp, i64, vp, vp, i64, vp, vp]),
+    "nmx_syevd_f32": (ci, [vp, i64, vp, i64, vp, vp, i64, vp, vp]),
     "nmx_npy_header": (ci, [C.c_char_p, C.POINTER(ci), C.POINTER(ci), vp, ci, C.POINTER(i64)]),
     "nmx_npy_load": (ci, [vp, C.c_char_p, ci, ci, vp, vp, i64, vp]),
     "nmx_npy_save": (ci, [vp, C.c_char_p, ci, ci, vp, vp, vp]),

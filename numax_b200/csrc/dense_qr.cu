@@ -815,6 +815,31 @@ static int orgqr(nmx_ctx ctx, int64_t m, int64_t n, const T *F, int64_t ldf, con
     return 0;
 }
 
+// B := Q B for the m x ncols block B (ldb), Q = H_0 ... H_{k-1} from
+// reflectors stored as geqrf leaves them in F (m x k, ldf): orgqr's replay,
+// last panel first, on B instead of the identity.  The symmetric
+// eigensolver forms its eigenvectors Q Z with it.
+int qr_apply_q_f64(nmx_ctx ctx, cudaStream_t st, int64_t m, int64_t k, const double *F,
+                   int64_t ldf, const double *tau, double *B, int64_t ldb, int64_t ncols) {
+    if (k <= 0 || ncols <= 0) return 0;
+    QrRun<double> R;
+    NMX_TRY(qr_setup<double>(ctx, st, m, std::max<int64_t>(k, ncols), R));
+    const int steps = (int)ceil_div(k, kQrW);
+    for (int s = 0; s < steps; ++s) {
+        const int kk = (steps - 1 - s) * kQrW;
+        const int w = (int)std::min<int64_t>(kQrW, k - kk);
+        const int64_t mk = m - kk;
+        pack_v_kernel<double><<<(unsigned)ceil_div(mk * kQrW, 256), 256, 0, st>>>(
+            F, ldf, (int)m, kk, w, R.Vd, nullptr);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_TRY(vtc<double>(R, (int)mk, R.Vd, kQrW, kQrW, R.sc.gram_part));
+        larft_kernel<double><<<1, 256, 0, st>>>(R.sc.gram_part, 1, tau, kk, w, R.Tm, 0);
+        NMX_CUDA_TRY(cudaGetLastError());
+        NMX_TRY(apply_reflector<double>(R, kk, B, ldb, 0, (int)ncols));
+    }
+    return 0;
+}
+
 // B := Q^T B for the m x nrhs block B (ldb): numax's QR.apply_q_transpose
 // (numax/linalg/qr.mojo:470-530) -- the reflectors in factorization order,
 // each panel through its block reflector (T^T), Q never formed.

@@ -84,7 +84,7 @@ struct nmx_context {
     int64_t tune_lu_lookahead = -1;   // look-ahead panel width of the LU (-1: 256, 0: off)
     int64_t tune_lu_panel_sms = -1;   // SMs the look-ahead keeps free of the update GEMMs (-1, 0: none)
     // Grow-only named device buffers, one per use, kept for the context's life.
-    static constexpr int kSlots = 11;
+    static constexpr int kSlots = 12;
     void *slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Pinned host staging of the .npy load/save pipeline and, per buffer, the
@@ -109,7 +109,8 @@ enum WsSlot {
     kWsGemm16Panel = 7,
     kWsWork64 = 8,  // FP64 factors of the refinement's last precision level
     kWsBest = 9,    // the refinement's best iterate
-    kWsAux = 10     // inverse's factor copy, PLU's permutation
+    kWsAux = 10,    // inverse's factor copy, PLU's permutation
+    kWsEig = 11     // the symmetric eigensolver's work copy and divide-and-conquer buffers
 };
 }
 

@@ -12,6 +12,7 @@ Mirrors numax's Tensor-tier call surface (numax/linalg/__init__.mojo:323-426):
     cholesky(a)                   numax/linalg/cholesky.mojo:233-468
     cholesky_solve(lower, b)      numax/linalg/cholesky.mojo:471-580
     solve_triangular(a, b, ...)   numax/linalg/triangular.mojo:228-425
+    eigh(a) -> Eigh, eigvalsh(a)  numax/linalg/eigen.mojo:1220-1341, 1449+
 
 Operands are torch tensors on a CUDA device standing in for numax's
 `Tensor` over a `DeviceBuffer`: row-major, float64 or float32, 2-D with unit
@@ -324,3 +325,52 @@ def solve_ir(a, b, precision: str = "bf16", gmres: bool | str = "auto", tol: flo
     stats = {f: getattr(st, f) for f, _ in _lib.IrStats._fields_}
     stats["final_precision"] = _lib.IR_PRECISION_NAMES.get(st.final_precision, "?")
     return x.reshape(b.shape), stats
+
+
+class Eigh:
+    """eigh's result (numax's `Eigh`, numax/linalg/eigen.mojo:1220-1246):
+    `values` ascending, `vectors` orthonormal with `vectors[:, j]` the
+    eigenvector of `values[j]`."""
+
+    def __init__(self, values, vectors):
+        self.values = values
+        self.vectors = vectors
+
+    def __iter__(self):
+        return iter((self.values, self.vectors))
+
+
+def _syevd(name, a, vectors):
+    _check_matrix(name, a, square=False)
+    n, m = a.shape
+    if m != n:
+        raise ValueError(f"{name}: the matrix must be square, got {n} x {m}")
+    if n < 1:
+        raise ValueError(f"{name}: the matrix is empty")
+    if a.stride(1) != 1:
+        a = a.contiguous()
+    dev = a.device
+    w = torch.empty(n, dtype=a.dtype, device=dev)
+    v = torch.empty(n, n, dtype=a.dtype, device=dev) if vectors else None
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call(f"nmx_syevd_{_SUF[a.dtype]}", _ctx(dev), n, a.data_ptr(), a.stride(0), w.data_ptr(),
+              v.data_ptr() if vectors else None, n, info.data_ptr(), _stream(dev))
+    if int(info.item()):
+        raise ValueError(f"{name}: an eigenvalue did not converge -- the matrix holds a NaN or "
+                         "an infinity")
+    return w, v
+
+
+def eigh(a) -> Eigh:
+    """Eigenvalues (ascending) and orthonormal eigenvectors (columns) of the
+    symmetric `a`, reading only its lower triangle (numax's Tensor-tier eigh,
+    numax/linalg/eigen.mojo:1268-1341): tridiagonalization, divide and
+    conquer and the back-transform all on the device (nmx_syevd_*)."""
+    w, v = _syevd("eigh", a, True)
+    return Eigh(w, v)
+
+
+def eigvalsh(a):
+    """The eigenvalues of the symmetric `a`, ascending, lower triangle read
+    (numax's eigvalsh): tridiagonalization and bisection on the device."""
+    return _syevd("eigvalsh", a, False)[0]

@@ -556,3 +556,140 @@ void FN(orc_batched_jacobi_eigh)(int64_t count, const int32_t *ns, const int64_t
 }
 
 #undef A_
+
+/* ---------------------------------------------------------------------- */
+/* Tensor-tier eigh: numax/linalg/eigen.mojo:1268-1430                    */
+/* ---------------------------------------------------------------------- */
+
+/* Symmetric eigendecomposition of the n x n row-major a (lower triangle
+ * read), numax's eigh at block = 1 (the unblocked algorithm every block
+ * width is pinned against):
+ *   sytrd   numax/linalg/eigen.mojo:320-560 with sytd2_column
+ *           (numax/linalg/panel.mojo:589-686): column k's reflector
+ *           annihilates a[k+2.., k]; beta = sqrt(alpha^2 + |x|^2), negated
+ *           when alpha > 0; tau = (beta - alpha) / beta; v = x / (alpha -
+ *           beta) below the implicit 1; tau = 0 when |x| = 0.  Then
+ *           p = A v, w = tau p - (tau^2 / 2)(p . v) v, A -= v w^T + w v^T.
+ *   _tql    implicit QL with Wilkinson shifts (numax/linalg/eigen.mojo:
+ *           966-1060, Numerical Recipes' tqli), the rotations applied to Z
+ *           as push_rotation defines them (eigen.mojo:724-733): column i
+ *           <- c z_i - s z_{i+1}, column i+1 <- s z_i + c z_{i+1}; at most
+ *           60 sweeps per eigenvalue (eigen.mojo:564).
+ *   sort    insertion sort of the values, the vectors' columns permuted
+ *           alike (eigen.mojo:1372-1385); vectors = Q Z (eigen.mojo:1411-1423).
+ * w receives the values ascending; z (n x n, may be NULL for values only)
+ * the vectors as columns.  work: 2 n^2 + 4 n elements.  Returns 0, or
+ * l + 1 when eigenvalue l did not converge. */
+int FN(orc_eigh)(int n, const T *a, int lda, T *w, T *z, T *work) {
+    T *A = work, *Z = work + (size_t)n * n, *d = Z + (size_t)n * n, *e = d + n, *tau = e + n,
+      *p = tau + n;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) A[i * n + j] = j <= i ? a[i * lda + j] : a[j * lda + i];
+    for (int k = 0; k + 2 < n; ++k) {
+        T below = 0;
+        for (int i = k + 2; i < n; ++i) below += A[i * n + k] * A[i * n + k];
+        T alpha = A[(k + 1) * n + k];
+        tau[k] = 0;
+        if (below == 0) continue;
+        T beta = (T)sqrt(alpha * alpha + below);
+        if (alpha > 0) beta = -beta;
+        T t = (beta - alpha) / beta, scale = (T)1 / (alpha - beta);
+        for (int i = k + 2; i < n; ++i) A[i * n + k] *= scale;
+        A[(k + 1) * n + k] = beta;
+        tau[k] = t;
+        /* v = (1, A[k+2.., k]) on rows k+1..; p = A22 v; w = t p + aw v. */
+        T pv = 0;
+        for (int i = k + 1; i < n; ++i) {
+            T s = 0;
+            for (int j = k + 1; j < n; ++j) s += A[i * n + j] * (j == k + 1 ? (T)1 : A[j * n + k]);
+            p[i] = s;
+            pv += s * (i == k + 1 ? (T)1 : A[i * n + k]);
+        }
+        T aw = -(T)0.5 * t * t * pv;
+        for (int i = k + 1; i < n; ++i) p[i] = t * p[i] + aw * (i == k + 1 ? (T)1 : A[i * n + k]);
+        for (int i = k + 1; i < n; ++i) {
+            T vi = i == k + 1 ? (T)1 : A[i * n + k];
+            for (int j = k + 1; j < n; ++j) {
+                T vj = j == k + 1 ? (T)1 : A[j * n + k];
+                A[i * n + j] -= vi * p[j] + p[i] * vj;
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) d[i] = A[i * n + i];
+    for (int i = 0; i + 1 < n; ++i) e[i] = A[(i + 1) * n + i];
+    e[n - 1] = 0;
+    for (int i = 0; i < n * n; ++i) Z[i] = (i / n == i % n) ? (T)1 : (T)0;
+    T eps = sizeof(T) == 8 ? (T)2.220446049250313e-16 : (T)1.1920929e-07;
+    for (int l = 0; l < n; ++l) {
+        int sweeps = 0;
+        for (;;) {
+            int m = l;
+            while (m < n - 1) {
+                T sc = (T)fabs(d[m]) + (T)fabs(d[m + 1]);
+                if ((T)fabs(e[m]) <= eps * sc) break;
+                ++m;
+            }
+            if (m == l) break;
+            if (++sweeps > 60) return l + 1;
+            T g = (d[l + 1] - d[l]) / ((T)2 * e[l]);
+            T r = (T)hypot(g, (T)1);
+            g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+            T s = 1, c = 1, pp = 0;
+            int i = m - 1, under = 0;
+            for (; i >= l; --i) {
+                T f = s * e[i], b = c * e[i];
+                r = (T)hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0) {
+                    d[i + 1] -= pp;
+                    e[m] = 0;
+                    under = 1;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - pp;
+                r = (d[i] - g) * s + (T)2 * c * b;
+                pp = s * r;
+                d[i + 1] = g + pp;
+                g = c * r - b;
+                for (int q = 0; q < n; ++q) {
+                    T zi = Z[q * n + i], zj = Z[q * n + i + 1];
+                    Z[q * n + i] = c * zi - s * zj;
+                    Z[q * n + i + 1] = s * zi + c * zj;
+                }
+            }
+            if (under) continue;
+            d[l] -= pp;
+            e[l] = g;
+            e[m] = 0;
+        }
+    }
+    /* Insertion sort of the values; Z's columns follow. */
+    int *order = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) order[i] = i;
+    for (int i = 1; i < n; ++i)
+        for (int j = i; j > 0 && d[order[j]] < d[order[j - 1]]; --j) {
+            int t = order[j];
+            order[j] = order[j - 1];
+            order[j - 1] = t;
+        }
+    for (int i = 0; i < n; ++i) w[i] = d[order[i]];
+    if (z) {
+        /* z = Q Zs, Q = H_0 ... H_{n-3}: the reflectors applied last first. */
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) z[i * n + j] = Z[i * n + order[j]];
+        for (int k = n - 3; k >= 0; --k) {
+            if (tau[k] == 0) continue;
+            for (int j = 0; j < n; ++j) {
+                T s = z[(k + 1) * n + j];
+                for (int i = k + 2; i < n; ++i) s += A[i * n + k] * z[i * n + j];
+                s *= tau[k];
+                z[(k + 1) * n + j] -= s;
+                for (int i = k + 2; i < n; ++i) z[i * n + j] -= s * A[i * n + k];
+            }
+        }
+    }
+    free(order);
+    return 0;
+}

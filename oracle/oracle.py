@@ -49,6 +49,7 @@ def lib() -> C.CDLL:
                 "orc_qr_factor": (None, [fp, C.c_int64, C.c_int, C.c_int, C.c_int, fp, fp]),
                 "orc_qr_q": (None, [fp, C.c_int64, C.c_int, C.c_int, C.c_int, fp, fp, C.c_int64, fp]),
                 "orc_batched_cholesky_solve": (None, [C.c_int64, _i32p, _i64p, fp, vp, _i64p, fp, fp, C.c_int, C.c_int]),
+                "orc_eigh": (C.c_int, [C.c_int, fp, C.c_int, fp, vp, fp]),
                 "orc_batched_jacobi_eigh": (None, [C.c_int64, _i32p, _i64p, fp, _i64p, fp, fp, C.c_int, C.c_int]),
             }
             for name, (res, args) in sig.items():
@@ -108,6 +109,22 @@ def jacobi_eigh(a: np.ndarray, sweeps: int = 12):
 
 
 # ---- Tensor tier ------------------------------------------------------------
+
+def eigh(a: np.ndarray, vectors: bool = True):
+    """(values ascending, vectors as columns or None) -- numax's Tensor-tier
+    eigh / eigvalsh at block = 1 (sytrd, implicit QL, insertion sort, Q Z).
+    Only the lower triangle of `a` is read."""
+    a = np.ascontiguousarray(a)
+    n = a.shape[0]
+    w = np.empty(n, dtype=a.dtype)
+    z = np.empty((n, n), dtype=a.dtype) if vectors else None
+    work = np.empty(2 * n * n + 4 * n + 1, dtype=a.dtype)
+    rc = _fn("orc_eigh", a.dtype)(n, a, n, w, z.ctypes.data if vectors else None, work)
+    if rc:
+        raise ValueError(f"eigvalsh: eigenvalue {rc - 1} did not converge in 60 sweeps -- the "
+                         "matrix holds a NaN or an infinity")
+    return w, z
+
 
 def getrf_panel(a: np.ndarray, k: int, nb: int):
     """In place on a copy; returns (a, pivots, info)."""

@@ -185,3 +185,33 @@ def test_batched_oracle_matches_per_matrix(oracle):
         np.testing.assert_allclose(a @ x, b, atol=1e-10)
         np.testing.assert_allclose(np.tril(L[ao[i]:ao[i] + n * n].reshape(n, n)),
                                    np.linalg.cholesky(a), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 10, 64, 150])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_eigh_matches_lapack(oracle, n, dtype):
+    """numax's Tensor-tier eigh restated (sytrd, implicit QL, sort, Q Z)
+    against LAPACK's syevd: values ascending, vectors orthonormal and
+    satisfying A v = lambda v; only the lower triangle is read."""
+    rng = np.random.Generator(np.random.PCG64(n))
+    g = rng.standard_normal((n, n))
+    a = ((g + g.T) / 2).astype(dtype)
+    noisy = np.tril(a) + np.triu(rng.standard_normal((n, n)).astype(dtype), 1)
+    w, v = oracle.eigh(noisy)
+    want = np.linalg.eigvalsh(a.astype(np.float64))
+    tol = 1e-13 if dtype == np.float64 else 2e-6
+    scale = max(1.0, np.abs(want).max())
+    assert np.abs(w - want).max() / scale < tol
+    v64 = v.astype(np.float64)
+    assert np.abs(a.astype(np.float64) @ v64 - v64 * w).max() / scale < 20 * tol
+    assert np.abs(v64.T @ v64 - np.eye(n)).max() < 20 * tol
+    w2, none = oracle.eigh(noisy, vectors=False)
+    assert none is None and np.array_equal(w, w2)
+
+
+def test_oracle_eigh_reports_nan():
+    a = np.eye(4)
+    a[2, 1] = np.nan
+    with pytest.raises(ValueError, match="did not converge"):
+        from oracle import oracle as O
+        O.eigh(a)
