@@ -8,12 +8,14 @@
 // Q Z with one more GEMM.  Here every step is on the device:
 //   1. sym_lower_kernel: the lower triangle mirrored into a full FP64 work
 //      copy (tiled transpose), and max |a_ij| for a power-of-two scaling.
-//   2. sytd2_kernel: Householder tridiagonalization in ONE cooperative
-//      launch, two grid rounds per column (the column's norm; then y = A v's
-//      dot with v), each CTA's warps owning fixed rows so the rank-2 update
-//      A -= v w^T + w v^T stays in the owner's cache; v and w are staged in
-//      shared memory by chunks.  Reflectors stay below the subdiagonal in
-//      LAPACK's lower layout, numax's beta/tau convention.
+//   2. latrd_kernel: Householder tridiagonalization by 32-column panels,
+//      each panel ONE cooperative launch with two grid rounds per column
+//      (the column's norm; then W^T v, V^T v and y . v in one vector), the
+//      trailing matrix read once per column for y = A22 v (v staged in
+//      shared memory by chunks) and updated once per panel,
+//      A -= V W^T + W V^T, on the library's FP64 GEMM.  Reflectors stay
+//      below the subdiagonal in LAPACK's lower layout, numax's beta/tau
+//      convention.
 //   3. eigenvalues only: Sturm-count bisection, one thread per eigenvalue.
 //      Eigenvectors: divide and conquer on the tridiagonal (tridiag_dc.cuh):
 //      level by level, every merge of a level at once -- deflation, secular
@@ -97,93 +99,127 @@ __global__ void sym_lower_kernel(const T *A, int64_t lda, int n, double *W, int6
 
 // ---- 2. tridiagonalization ---------------------------------------------------
 
-struct TrdArgs {
-    double *A;
+constexpr int kLrdNb = 32;              // panel width (columns per launch)
+constexpr int kLrdVec = 2 * kLrdNb + 1;  // W^T v, V^T v and y . v: one round's sums
+constexpr int kLrdSub = 4;              // threads per value in the cross-CTA sum
+
+struct LrdArgs {
+    double *A;  // the symmetric work matrix (full storage), scaled
     int64_t lda;
     int n;
+    int p, jb;            // the panel: columns [p, p + jb)
     double *d, *e, *tau;  // diagonal, subdiagonal, reflector scales
-    double *xbuf;         // [2][n] the next column below the diagonal (double-buffered)
-    double *ybuf;         // [n] A22 v
-    double *part;         // [2][G] per-CTA partial sums (double-buffered)
+    double *Vp, *Wp;      // [n][kLrdNb] the panel's v and w, row-major
+    double *xbuf;         // [n] the current column, brought up to date
+    double *ybuf;         // [n] A22 v of the current column
+    double *part;         // [2][kLrdVec][G] per-CTA partial sums (double-buffered)
     unsigned *bar;
     int *err;
-    const unsigned long long *maxabs;
-    int *scale_exp;  // A was scaled by 2^-scale_exp
 };
 
-// One grid-wide sum: every CTA adds its threads' values, publishes the CTA
-// total, and after the barrier sums all CTAs' totals in the same fixed order
-// (so every CTA holds the same bits).  Returns false if the barrier gave up.
-__device__ bool trd_grid_sum(double v, const TrdArgs &a, unsigned &gen, double *red,
-                             double *s_tot, int *s_flag, double *out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, G = gridDim.x;
-    v = warp_sum(v);
-    if (lane == 0) red[warp] = v;
+// One grid round over a vector of `nv` sums: the CTA's threads have added
+// their values into red[warp][v]; every CTA publishes its totals, and after
+// the barrier sums all CTAs' in the same fixed order into out[0 .. nv).
+// Returns false if the barrier gave up.
+__device__ bool lrd_round(const LrdArgs &a, unsigned &gen, int nv, double (*red)[kLrdVec],
+                          double *sub, double *out, int *s_flag) {
+    const int G = gridDim.x;
     __syncthreads();
-    double *slot = a.part + (size_t)(gen & 1) * G;
-    if (threadIdx.x == 0) {
+    double *slot = a.part + (size_t)(gen & 1) * kLrdVec * G;
+    if (threadIdx.x < nv) {
         double t = 0.0;
-        for (int w = 0; w < kTrdWarps; ++w) t += red[w];
-        slot[blockIdx.x] = t;
+        for (int w = 0; w < kTrdWarps; ++w) t += red[w][threadIdx.x];
+        slot[(size_t)threadIdx.x * G + blockIdx.x] = t;
     }
     if (!grid_barrier(a.bar, gen++, (unsigned)G, a.err, s_flag)) return false;
-    if (threadIdx.x < 32) {
+    if (threadIdx.x < nv * kLrdSub) {
+        const int v = threadIdx.x / kLrdSub, s = threadIdx.x - v * kLrdSub;
+        const double *src = slot + (size_t)v * G;
         double t = 0.0;
-        for (int g = lane; g < G; g += 32) t += __ldcg(slot + g);
-        t = warp_sum(t);
-        if (lane == 0) *s_tot = t;
+        for (int g = s; g < G; g += kLrdSub) t += __ldcg(src + g);
+        sub[threadIdx.x] = t;
     }
     __syncthreads();
-    *out = *s_tot;
+    if (threadIdx.x < nv) {
+        double t = 0.0;
+        for (int s = 0; s < kLrdSub; ++s) t += sub[threadIdx.x * kLrdSub + s];
+        out[threadIdx.x] = t;
+    }
     __syncthreads();
     return true;
 }
 
-// Householder reduction of the symmetric A (full storage, scaled in place by
-// a power of two) to T = Q^T A Q tridiagonal, column by column (LAPACK's
-// sytd2, lower): for column j, x = A[j+1:, j], beta = -sign(alpha) |x|
-// (alpha <= 0 gives +|x|), tau = (beta - alpha) / beta, v = (1, x[1:] /
-// (alpha - beta)); y = A22 v, w = tau y - (tau^2 / 2)(y . v) v, and
-// A22 -= v w^T + w v^T.  Row r belongs to warp r mod (warps in the grid) for
-// the whole reduction.
-__global__ void __launch_bounds__(kTrdThreads, 1) sytd2_kernel(TrdArgs a) {
-    __shared__ double sv[kTrdChunk], sw[kTrdChunk];
-    __shared__ double red[kTrdWarps];
-    __shared__ double s_tot;
+// One panel of the Householder reduction to tridiagonal form (LAPACK's
+// latrd, lower), in one cooperative launch: the trailing matrix stays as it
+// was at the panel's start and each column is brought up to date with the
+// panel's earlier reflectors through V and W,
+//   a = A[:, j] - V W[j, :]^T - W V[j, :]^T                   (round 1: |x|)
+//   beta = -sign(alpha) |x| (alpha <= 0 gives +|x|), tau = (beta - alpha)/beta,
+//   v = (1, x[1:] / (alpha - beta))
+//   y = A22 v; sums W^T v, V^T v, y . v                       (round 2)
+//   w = tau (y - V (W^T v) - W (V^T v)) - (tau/2)(w . v) v,
+// with w . v = tau (y . v - 2 (W^T v) . (V^T v)).  The caller then updates
+// the trailing matrix with A -= V W^T + W V^T on the GEMM.  Row r belongs to
+// warp r mod (warps in the grid); the reflector goes below the subdiagonal
+// of column j, beta to the subdiagonal.
+__global__ void __launch_bounds__(kTrdThreads, 1) latrd_kernel(LrdArgs a) {
+    __shared__ double sv[kTrdChunk];
+    __shared__ double red[kTrdWarps][kLrdVec];
+    __shared__ double sub[kLrdVec * kLrdSub];
+    __shared__ double tot[kLrdVec];
+    __shared__ double s_vj[kLrdNb], s_wj[kLrdNb];  // row j of V and W
+    __shared__ double s_t1[kLrdNb], s_t2[kLrdNb];  // the previous column's W^T v, V^T v
     __shared__ int s_flag;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int NW = gridDim.x * kTrdWarps, gw = blockIdx.x * kTrdWarps + warp;
-    const int n = a.n;
+    const int n = a.n, p = a.p;
     const int64_t lda = a.lda;
-    double *A = a.A;
-
-    // A power-of-two scale (exact) so that the sums of squares stay in range.
-    const double amax = __longlong_as_double((long long)*a.maxabs);
-    int ex = 0;
-    if (amax > 0.0 && amax <= 1.7976931348623157e308) frexp(amax, &ex);
-    const double sc = ldexp(1.0, -ex);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.scale_exp = ex;
-
+    const double *A = a.A;
     unsigned gen = 0;
-    double p = 0.0;
-    for (int r = gw; r < n; r += NW) {
-        double *row = A + (int64_t)r * lda;
-        for (int c = lane; c < n; c += 32) row[c] *= sc;
-        __syncwarp();
-        if (lane == 0) {
-            const double x = row[0];
-            if (r == 0) a.d[0] = x;
-            if (r >= 1) a.xbuf[r] = x;
-            if (r >= 2) p += x * x;
-        }
-    }
-    double xn2 = 0.0;
-    if (n >= 3 && !trd_grid_sum(p, a, gen, red, &s_tot, &s_flag, &xn2)) return;
+    double tau_prev = 0.0, aw_prev = 0.0;
 
-    for (int j = 0; j + 2 < n; ++j) {
-        const double *xb = a.xbuf + (size_t)(j & 1) * n;
-        double *xnext = a.xbuf + (size_t)((j + 1) & 1) * n;
-        const double alpha = __ldcg(xb + j + 1);
+    for (int i = 0; i < a.jb; ++i) {
+        const int j = p + i;
+        // Row j of the panel's V and W: earlier columns from memory; the
+        // previous column's w_j computed here (its owner wrote it after the
+        // last barrier).
+        if (threadIdx.x < 32) {
+            const int t = lane;
+            double vj = 0.0, wj = 0.0;
+            if (t < i) vj = __ldcg(a.Vp + (size_t)j * kLrdNb + t);
+            if (t + 1 < i) wj = __ldcg(a.Wp + (size_t)j * kLrdNb + t);
+            double corr = 0.0;
+            if (t + 1 < i) corr = vj * s_t1[t] + wj * s_t2[t];
+            corr = warp_sum(corr);
+            if (i > 0 && t == i - 1)
+                wj = tau_prev * (__ldcg(a.ybuf + j) - corr) + aw_prev * vj;
+            s_vj[t] = vj;
+            s_wj[t] = wj;
+        }
+        __syncthreads();
+
+        // The column brought up to date on the owned rows r >= j.
+        double pn = 0.0;
+        int r0 = gw;
+        if (r0 < j) r0 += ((j - r0 + NW - 1) / NW) * NW;
+        for (int r = r0; r < n; r += NW) {
+            double c = 0.0;
+            if (lane < i)
+                c = a.Vp[(size_t)r * kLrdNb + lane] * s_wj[lane] +
+                    a.Wp[(size_t)r * kLrdNb + lane] * s_vj[lane];
+            c = warp_sum(c);
+            const double x = A[(int64_t)r * lda + j] - c;
+            if (lane == 0) {
+                if (r == j) a.d[j] = x;
+                if (r >= j + 1) a.xbuf[r] = x;
+                if (r >= j + 2) pn += x * x;
+            }
+        }
+        if (lane == 0) red[warp][0] = pn;  // lane 0 holds the warp's rows
+        if (!lrd_round(a, gen, 1, red, sub, tot, &s_flag)) return;
+        const double xn2 = tot[0];
+
+        const double alpha = __ldcg(a.xbuf + j + 1);
         double beta, tau, scale;
         if (xn2 == 0.0) {
             beta = alpha;
@@ -199,10 +235,10 @@ __global__ void __launch_bounds__(kTrdThreads, 1) sytd2_kernel(TrdArgs a) {
             a.e[j] = beta;
             a.tau[j] = tau;
         }
-        int r0 = gw;
-        if (r0 < j + 1) r0 += ((j + 1 - r0 + NW - 1) / NW) * NW;
 
-        // y = A22 v for the owned rows, v staged by chunks.
+        // y = A22 v on the owned rows (v staged by chunks), with the sums.
+        r0 = gw;
+        if (r0 < j + 1) r0 += ((j + 1 - r0 + NW - 1) / NW) * NW;
         double acc[kTrdRows];
 #pragma unroll
         for (int t = 0; t < kTrdRows; ++t) acc[t] = 0.0;
@@ -211,7 +247,7 @@ __global__ void __launch_bounds__(kTrdThreads, 1) sytd2_kernel(TrdArgs a) {
             __syncthreads();
             for (int c = threadIdx.x; c < cn; c += kTrdThreads) {
                 const int cc = c0 + c;
-                sv[c] = cc == j + 1 ? 1.0 : __ldcg(xb + cc) * scale;
+                sv[c] = cc == j + 1 ? 1.0 : __ldcg(a.xbuf + cc) * scale;
             }
             __syncthreads();
 #pragma unroll
@@ -231,80 +267,76 @@ __global__ void __launch_bounds__(kTrdThreads, 1) sytd2_kernel(TrdArgs a) {
                 acc[t] += (s0 + s1) + (s2 + s3);
             }
         }
-        double vr[kTrdRows], wr[kTrdRows];
-        double pyv = 0.0;
+        double t1 = 0.0, t2 = 0.0, yv = 0.0;  // lane t: W[:, t]^T v, V[:, t]^T v
+        double yr[kTrdRows], vr[kTrdRows];
 #pragma unroll
         for (int t = 0; t < kTrdRows; ++t) {
             const int r = r0 + t * NW;
-            vr[t] = wr[t] = 0.0;
+            yr[t] = vr[t] = 0.0;
             if (r >= n) break;
             const double y = warp_sum(acc[t]);
-            const double v = r == j + 1 ? 1.0 : __ldcg(xb + r) * scale;
+            const double v = r == j + 1 ? 1.0 : __ldcg(a.xbuf + r) * scale;
+            yr[t] = y;
             vr[t] = v;
-            wr[t] = y;  // tau y + aw v once aw is known
-            pyv += y * v;
+            yv += y * v;
+            if (lane < i) {
+                t1 += a.Wp[(size_t)r * kLrdNb + lane] * v;
+                t2 += a.Vp[(size_t)r * kLrdNb + lane] * v;
+            }
             if (lane == 0) {
                 a.ybuf[r] = y;
-                A[(int64_t)r * lda + j] = r == j + 1 ? beta : v;  // the reflector's storage
+                a.Vp[(size_t)r * kLrdNb + i] = v;
+                a.A[(int64_t)r * lda + j] = r == j + 1 ? beta : v;  // the reflector's storage
             }
         }
-        if (lane != 0) pyv = 0.0;
-        double yv = 0.0;
-        if (!trd_grid_sum(pyv, a, gen, red, &s_tot, &s_flag, &yv)) return;
-        const double aw = -0.5 * tau * tau * yv;
-#pragma unroll
-        for (int t = 0; t < kTrdRows; ++t) wr[t] = tau * wr[t] + aw * vr[t];
+        red[warp][lane] = lane < i ? t1 : 0.0;
+        red[warp][kLrdNb + lane] = lane < i ? t2 : 0.0;
+        if (lane == 0) red[warp][2 * kLrdNb] = yv;
+        if (!lrd_round(a, gen, kLrdVec, red, sub, tot, &s_flag)) return;
 
-        // A22 -= v w^T + w v^T on the owned rows; then the next column.
-        for (int c0 = j + 1; c0 < n; c0 += kTrdChunk) {
-            const int cn = min(kTrdChunk, n - c0);
-            __syncthreads();
-            for (int c = threadIdx.x; c < cn; c += kTrdThreads) {
-                const int cc = c0 + c;
-                const double v = cc == j + 1 ? 1.0 : __ldcg(xb + cc) * scale;
-                sv[c] = v;
-                sw[c] = tau * __ldcg(a.ybuf + cc) + aw * v;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int t = 0; t < kTrdRows; ++t) {
-                const int r = r0 + t * NW;
-                if (r >= n) break;
-                double *row = A + (int64_t)r * lda + c0;
-                const double v = vr[t], w = wr[t];
-                int c = lane;
-                for (; c + 96 < cn; c += 128) {
-                    const double a0 = row[c], a1 = row[c + 32], a2 = row[c + 64], a3 = row[c + 96];
-                    row[c] = a0 - fma(v, sw[c], w * sv[c]);
-                    row[c + 32] = a1 - fma(v, sw[c + 32], w * sv[c + 32]);
-                    row[c + 64] = a2 - fma(v, sw[c + 64], w * sv[c + 64]);
-                    row[c + 96] = a3 - fma(v, sw[c + 96], w * sv[c + 96]);
-                }
-                for (; c < cn; c += 32) row[c] -= fma(v, sw[c], w * sv[c]);
-            }
-        }
-        __syncwarp();
-        double p2 = 0.0;
+        // w on the owned rows.
+        double t12 = 0.0;
+        for (int t = 0; t < i; ++t) t12 += tot[t] * tot[kLrdNb + t];
+        const double aw = -0.5 * tau * tau * (tot[2 * kLrdNb] - 2.0 * t12);
 #pragma unroll
         for (int t = 0; t < kTrdRows; ++t) {
             const int r = r0 + t * NW;
             if (r >= n) break;
-            if (lane == 0) {
-                const double x = A[(int64_t)r * lda + j + 1];
-                if (r == j + 1) a.d[j + 1] = x;
-                if (r >= j + 2) xnext[r] = x;
-                if (r >= j + 3) p2 += x * x;
-            }
+            double c = 0.0;
+            if (lane < i)
+                c = a.Vp[(size_t)r * kLrdNb + lane] * tot[lane] +
+                    a.Wp[(size_t)r * kLrdNb + lane] * tot[kLrdNb + lane];
+            c = warp_sum(c);
+            if (lane == 0) a.Wp[(size_t)r * kLrdNb + i] = tau * (yr[t] - c) + aw * vr[t];
         }
-        if (!trd_grid_sum(p2, a, gen, red, &s_tot, &s_flag, &xn2)) return;
+        if (threadIdx.x < kLrdNb) {
+            s_t1[threadIdx.x] = tot[threadIdx.x];
+            s_t2[threadIdx.x] = tot[kLrdNb + threadIdx.x];
+        }
+        tau_prev = tau;
+        aw_prev = aw;
+        __syncthreads();
     }
-    // The trailing 2 x 2 (or 1 x 1) as it stands.
-    if (n >= 2 && gw == (n - 1) % NW && lane == 0) {
-        const double *row = A + (int64_t)(n - 1) * lda;
-        a.d[n - 1] = row[n - 1];
-        a.e[n - 2] = row[n - 2];
-        a.tau[n - 2] = 0.0;
+}
+
+// The trailing 2 x 2 (or 1 x 1) once every panel's update is in.
+__global__ void trd_tail_kernel(const double *A, int64_t lda, int n, double *d, double *e,
+                                double *tau) {
+    if (threadIdx.x != 0) return;
+    if (n == 1) {
+        d[0] = A[0];
+        return;
     }
+    d[n - 2] = A[(int64_t)(n - 2) * lda + n - 2];
+    d[n - 1] = A[(int64_t)(n - 1) * lda + n - 1];
+    e[n - 2] = A[(int64_t)(n - 1) * lda + n - 2];
+    tau[n - 2] = 0.0;
+}
+
+// A *= 2^-ex (exact), ex from max |a_ij|, so the sums of squares stay in range.
+__global__ void scale_kernel(double *A, int64_t n2, int ex) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n2) A[e] = ldexp(A[e], -ex);
 }
 
 // ---- 3a. eigenvalues by bisection --------------------------------------------
@@ -648,7 +680,7 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
 
     // Cooperative grid of the tridiagonalization: one CTA per SM.
     int per_sm = 0;
-    NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sytd2_kernel, kTrdThreads, 0));
+    NMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, latrd_kernel, kTrdThreads, 0));
     const int G = std::min(ctx->sm_count, std::max(per_sm, 0) * ctx->sm_count);
     if (G < 1 || (int64_t)(n - 1) > (int64_t)kTrdRows * G * kTrdWarps) {
         set_error("eigh: order %d exceeds the cooperative tridiagonalization's %d rows", n,
@@ -661,7 +693,7 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
     for (int m : plan.level_mmax) mmax = std::max(mmax, m);
     const size_t nn = (size_t)n * n, nm = (size_t)n * mmax;
     // Work copy, vectors and scalars; then the divide and conquer's buffers.
-    size_t doubles = nn + 8 * (size_t)n + 2 * (size_t)G + 64;
+    size_t doubles = nn + 5 * (size_t)n + 2 * (size_t)kLrdNb * n + 2 * (size_t)kLrdVec * G + 64;
     if (vectors)
         doubles += nn + 3 * nm + 12 * (size_t)n + plan.merges.size() * 2 + 16;
     size_t ints = 8 * (size_t)n + 3 * plan.merges.size() + 64;
@@ -671,9 +703,10 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
     NMX_TRY(ctx->ensure_slot(kWsEig, bytes, &wsv));
     double *ws = static_cast<double *>(wsv);
     double *Aw = ws;
-    double *d = Aw + nn, *e = d + n, *tau = e + n, *xbuf = tau + n, *ybuf = xbuf + 2 * (size_t)n;
-    double *part = ybuf + n;
-    double *cur = part + 2 * (size_t)G;
+    double *d = Aw + nn, *e = d + n, *tau = e + n, *xbuf = tau + n, *ybuf = xbuf + n;
+    double *Vp = ybuf + n, *Wp = Vp + (size_t)kLrdNb * n;
+    double *part = Wp + (size_t)kLrdNb * n;
+    double *cur = part + 2 * (size_t)kLrdVec * G;
     DcBuf b{};
     if (vectors) {
         b.Qa = cur;
@@ -739,11 +772,31 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
         return 0;
     }
 
-    // 2. tridiagonalization.
-    TrdArgs ta{Aw, (int64_t)n, n, d, e, tau, xbuf, ybuf, part, bar, err, maxabs, scale_exp};
-    void *args[] = {&ta};
-    NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)sytd2_kernel, dim3(G), dim3(kTrdThreads), args,
-                                             0, st));
+    // 2. tridiagonalization: an exact power-of-two scale, then the panels.
+    int ex = 0;
+    if (amax > 0.0) std::frexp(amax, &ex);
+    NMX_CUDA_TRY(cudaMemcpyAsync(scale_exp, &ex, sizeof(int), cudaMemcpyHostToDevice, st));
+    if (ex != 0) {
+        scale_kernel<<<(unsigned)ceil_div((int64_t)n * n, 256), 256, 0, st>>>(Aw, (int64_t)n * n, ex);
+        NMX_CUDA_TRY(cudaGetLastError());
+    }
+    for (int p = 0; p + 2 < n; p += kLrdNb) {
+        const int jb = std::min(kLrdNb, n - 2 - p);
+        NMX_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(unsigned), st));
+        LrdArgs la{Aw, (int64_t)n, n, p, jb, d, e, tau, Vp, Wp, xbuf, ybuf, part, bar, err};
+        void *args[] = {&la};
+        NMX_CUDA_TRY(cudaLaunchCooperativeKernel((void *)latrd_kernel, dim3(G), dim3(kTrdThreads),
+                                                 args, 0, st));
+        const int q = p + jb, M = n - q;
+        const size_t off = (size_t)q * kLrdNb;
+        double *C = Aw + (size_t)q * n + q;
+        NMX_TRY(gemm_cc<double>(st, false, true, M, M, jb, -1.0, Vp + off, kLrdNb, Wp + off, kLrdNb,
+                                1.0, C, n));
+        NMX_TRY(gemm_cc<double>(st, false, true, M, M, jb, -1.0, Wp + off, kLrdNb, Vp + off, kLrdNb,
+                                1.0, C, n));
+    }
+    trd_tail_kernel<<<1, 32, 0, st>>>(Aw, n, n, d, e, tau);
+    NMX_CUDA_TRY(cudaGetLastError());
 
     if (!vectors) {
         bisect_kernel<T><<<(unsigned)ceil_div(n, 128), 128, 0, st>>>(n, d, e, scale_exp, W);
