@@ -373,11 +373,14 @@ def run_lu_ir(n, kappas, dev, seed=SEED):
     return out
 
 
-def run_dense(dev, orders=(4096, 8192, 16384), nrhs=16, qr_m=262144, qr_n=256, seed=SEED):
+def run_dense(dev, orders=(4096, 8192, 16384), nrhs=16, qr_m=262144, qr_n=256, seed=SEED,
+              eigh_n=4096):
     """The dense factorizations at the single-matrix configs: FP64 LU + 16-RHS
     solve and FP64 Cholesky + 16-RHS solve at each order, FP32 Householder QR
-    (geqrf, then orgqr) of qr_m x qr_n.  Device time (CUDA events) of one
-    call each after a warm-up call; rates in TF/s (LAPACK flop counts)."""
+    (geqrf, then orgqr) of qr_m x qr_n; FP64 eigh / eigvalsh of one
+    eigh_n x eigh_n symmetric matrix (0 skips it).  Device time (CUDA events)
+    of one call each after a warm-up call; rates in TF/s (LAPACK flop
+    counts)."""
     import torch
     from numax_b200 import _lib
     ctx = _lib.context(dev.index)
@@ -446,7 +449,51 @@ def run_dense(dev, orders=(4096, 8192, 16384), nrhs=16, qr_m=262144, qr_n=256, s
     orth = float((qq.T.double() @ qq.double() - torch.eye(qr_n, dtype=torch.float64, device=dev)).abs().max())
     out["qr_f32"] = {"m": qr_m, "n": qr_n, "geqrf_ms": ms, "tflops": fl / ms / 1e9,
                      "orgqr_ms": ms_q, "q_orthogonality_err": orth}
+    del q, f, qq
+    torch.cuda.empty_cache()
+    if eigh_n:
+        out["eigh_f64"] = run_eigh_dense(dev, eigh_n, gen)
     return out
+
+
+def run_eigh_dense(dev, n, gen):
+    """Symmetric eigendecomposition of one n x n FP64 matrix (G + G^T)/2:
+    eigh (values and vectors: tridiagonalization, divide and conquer, Q Z)
+    and eigvalsh (tridiagonalization, bisection), device time of one call
+    after a warm-up call.  The tridiagonalization reads the trailing matrix
+    once per column: n^3 / 3 doubles in all, its algorithmic bytes.
+    torch.linalg.eigh (cuSOLVER) on the same matrix is timed beside it for
+    context only."""
+    import torch
+    from numax_b200 import linalg as L
+    stream = torch.cuda.current_stream(dev)
+    g = torch.randn((n, n), generator=gen, dtype=torch.float64, device=dev)
+    a = (g + g.T) / 2
+    del g
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1), out
+    ms, r = timed(lambda: L.eigh(a))
+    ms_v, w = timed(lambda: L.eigvalsh(a))
+    ms_ref, (wr, _) = timed(lambda: torch.linalg.eigh(a))
+    V, W = r.vectors, r.values
+    resid = float(torch.linalg.matrix_norm(a @ V - V * W, 2) / torch.linalg.matrix_norm(a, 2))
+    orth = float((V.T @ V - torch.eye(n, dtype=torch.float64, device=dev)).abs().max())
+    tri_bytes = 8.0 * n ** 3 / 3
+    return {"n": n, "eigh_ms": ms, "eigvalsh_ms": ms_v, "residual": resid,
+            "orthogonality_err": orth,
+            "values_err_vs_cusolver": float((W - wr).abs().max() / wr.abs().max()),
+            "eigvalsh_err_vs_cusolver": float((w - wr).abs().max() / wr.abs().max()),
+            "tridiagonalization_algorithmic_gb": tri_bytes / 1e9,
+            "eigvalsh_gbs": tri_bytes / ms_v / 1e6,
+            "cusolver_eigh_ms": ms_ref}
 
 
 def make_eigh_batch(count, dev, seed=SEED):
@@ -985,6 +1032,8 @@ def main():
                     help="GiB of the .npy save/load leg (0 skips it)")
     ap.add_argument("--only-npy", action="store_true",
                     help="run only the .npy save/load leg")
+    ap.add_argument("--only-eigh", type=int, default=0,
+                    help="run only the dense FP64 eigh / eigvalsh leg at this order, for profiling")
     ap.add_argument("--only-big", action="store_true",
                     help="run only the n in 97..128 bucket of the batch (the dominant kernel), "
                          "default schedule, for profiling")
@@ -997,7 +1046,7 @@ def main():
         import torch
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
         torch.cuda.set_device(dev)
-        print(json.dumps({"dense": run_dense(dev, orders=())}), flush=True)
+        print(json.dumps({"dense": run_dense(dev, orders=(), eigh_n=0)}), flush=True)
         return 0
     if args.only_npy:
         import torch
@@ -1006,6 +1055,14 @@ def main():
         ns, seed = shard(0, args.count, 1)
         A, _ = make_batch_torch(ns, NRHS, torch.float64, dev, seed)
         print(json.dumps({"npy": run_npy(dev, A, args.npy_gib)}), flush=True)
+        return 0
+    if args.only_eigh:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED + 41)
+        print(json.dumps({"eigh_f64": run_eigh_dense(dev, args.only_eigh, gen)}), flush=True)
         return 0
     if args.only_dense:
         import torch

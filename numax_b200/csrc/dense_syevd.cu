@@ -45,7 +45,7 @@ namespace {
 constexpr int kTrdThreads = 512;
 constexpr int kTrdWarps = kTrdThreads / 32;
 constexpr int kTrdRows = 8;      // rows a warp owns at most: n - 1 <= 8 x warps in the grid
-constexpr int kTrdChunk = 2048;  // columns of v and w staged in shared memory at once
+constexpr int kTrdChunk = 4096;  // columns of v staged in shared memory at once
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
