@@ -255,16 +255,18 @@ __global__ void __launch_bounds__(kTrdThreads, 1) latrd_kernel(LrdArgs a) {
                 const int r = r0 + t * NW;
                 if (r >= n) break;
                 const double *row = A + (int64_t)r * lda + c0;
-                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                // Eight loads in flight per lane before any is used.
+                double s[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                 int c = lane;
-                for (; c + 96 < cn; c += 128) {
-                    s0 = fma(row[c], sv[c], s0);
-                    s1 = fma(row[c + 32], sv[c + 32], s1);
-                    s2 = fma(row[c + 64], sv[c + 64], s2);
-                    s3 = fma(row[c + 96], sv[c + 96], s3);
+                for (; c + 224 < cn; c += 256) {
+                    double x[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) x[u] = row[c + 32 * u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) s[u] = fma(x[u], sv[c + 32 * u], s[u]);
                 }
-                for (; c < cn; c += 32) s0 = fma(row[c], sv[c], s0);
-                acc[t] += (s0 + s1) + (s2 + s3);
+                for (; c < cn; c += 32) s[0] = fma(row[c], sv[c], s[0]);
+                acc[t] += ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
             }
         }
         double t1 = 0.0, t2 = 0.0, yv = 0.0;  // lane t: W[:, t]^T v, V[:, t]^T v
@@ -799,7 +801,8 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
     NMX_CUDA_TRY(cudaGetLastError());
 
     if (!vectors) {
-        bisect_kernel<T><<<(unsigned)ceil_div(n, 128), 128, 0, st>>>(n, d, e, scale_exp, W);
+        // One thread per eigenvalue in 32-thread CTAs: every SM gets work.
+        bisect_kernel<T><<<(unsigned)ceil_div(n, 32), 32, 0, st>>>(n, d, e, scale_exp, W);
         NMX_CUDA_TRY(cudaGetLastError());
     } else {
         // 3. divide and conquer.
@@ -821,8 +824,10 @@ int syevd(nmx_ctx ctx, int64_t n64, const T *A, int64_t lda, T *W, T *V, int64_t
             bl.kc = b.kc + 3 * off;
             dc_deflate_kernel<<<cnt, 128, 0, st>>>(mgl, n, bl);
             dc_rotate_kernel<<<dim3((unsigned)ceil_div(mm, 8), cnt), 256, 0, st>>>(mgl, n, bl);
-            dc_secular_kernel<<<dim3((unsigned)ceil_div(mm, 128), cnt), 128, 0, st>>>(mgl, bl);
-            dc_zhat_kernel<<<dim3((unsigned)ceil_div(mm, 128), cnt), 128, 0, st>>>(mgl, bl);
+            // One thread per root (per z-hat entry) in 32-thread CTAs, so
+            // the top levels' few merges still spread over every SM.
+            dc_secular_kernel<<<dim3((unsigned)ceil_div(mm, 32), cnt), 32, 0, st>>>(mgl, bl);
+            dc_zhat_kernel<<<dim3((unsigned)ceil_div(mm, 32), cnt), 32, 0, st>>>(mgl, bl);
             dc_vec_kernel<<<dim3(mm, cnt), 128, 0, st>>>(mgl, mmax, bl);
             dc_gather_kernel<<<dim3((unsigned)ceil_div((int64_t)mm * mm, 256), cnt), 256, 0, st>>>(
                 mgl, n, mmax, bl);
