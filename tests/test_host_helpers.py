@@ -46,3 +46,27 @@ def test_algorithmic_bytes_and_flops():
     assert bench.algorithmic_bytes(ns, nrhs, 8) == want
     assert bench.algorithmic_flops(ns, nrhs) == pytest.approx(
         float(sum(n ** 3 / 3 + 2 * nrhs * n ** 2 for n in ns)))
+
+
+def test_syevd_and_npy_argument_checks_need_no_device():
+    """Argument errors come back as -(index) before any CUDA call."""
+    import ctypes as C
+    from numax_b200 import _lib
+    lib = _lib.load()
+    info = C.c_int32()
+    # ctx NULL is argument 1; n < 0 is argument 2 (checked after ctx).
+    assert lib.nmx_syevd_f64(None, 4, None, 4, None, None, 4, C.byref(info), None) == -1
+    assert lib.nmx_syevd_f32(None, 4, None, 4, None, None, 4, C.byref(info), None) == -1
+    fake_ctx = C.c_void_p(1)
+    assert lib.nmx_syevd_f64(fake_ctx, -1, None, 4, None, None, 4, C.byref(info), None) == -2
+    assert lib.nmx_syevd_f64(fake_ctx, 4, None, 4, None, None, 4, C.byref(info), None) == -3
+    buf = (C.c_double * 16)()
+    assert lib.nmx_syevd_f64(fake_ctx, 4, buf, 3, buf, None, 4, C.byref(info), None) == -4
+    assert lib.nmx_syevd_f64(fake_ctx, 4, buf, 4, buf, buf, 2, C.byref(info), None) == -7
+    assert lib.nmx_syevd_f64(fake_ctx, 4, buf, 4, buf, None, 4, None, None) == -8
+    shape = (C.c_int64 * 2)(2, 2)
+    assert lib.nmx_npy_load(None, None, 0, 2, shape, None, 0, None) == -2
+    assert lib.nmx_npy_load(None, b"x.npy", 99, 2, shape, None, 0, None) == -3
+    assert lib.nmx_npy_load(None, b"x.npy", 0, 65, shape, None, 0, None) == -4
+    assert lib.nmx_npy_save(None, b"x.npy", 1, 1, (C.c_int64 * 1)(-3), None, None) == -5
+    assert lib.nmx_npy_header(None, None, None, None, 0, None) == -1
