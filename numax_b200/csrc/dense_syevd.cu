@@ -343,10 +343,9 @@ __global__ void scale_kernel(double *A, int64_t n2, int ex) {
 
 // ---- 3a. eigenvalues by bisection --------------------------------------------
 
-// Eigenvalue k (ascending) of the tridiagonal (d, e) by bisection on the
-// Sturm count (the number of negative pivots of T - x I), inside the
-// Gershgorin interval, to a width of 2 eps max(|lo|, |hi|) + pivmin; the
-// result is scaled by 2^scale_exp.
+// Eigenvalue k (ascending) of the tridiagonal (d, e): dc::sturm_kth's
+// multisection on the Sturm count inside the Gershgorin interval (widened
+// by the rounding of the counts), scaled back by 2^scale_exp.
 template <typename T>
 __global__ void bisect_kernel(int n, const double *d, const double *e, const int *scale_exp,
                               T *W) {
@@ -363,26 +362,7 @@ __global__ void bisect_kernel(int n, const double *d, const double *e, const int
     const double tnorm = fmax(fabs(lo), fabs(hi));
     lo -= 2.0 * dc::kEps * tnorm * n + pivmin;
     hi += 2.0 * dc::kEps * tnorm * n + pivmin;
-    for (int it = 0; it < 200; ++it) {
-        const double mid = 0.5 * (lo + hi);
-        if (hi - lo <= 2.0 * dc::kEps * fmax(fabs(lo), fabs(hi)) + pivmin || mid <= lo ||
-            mid >= hi)
-            break;
-        int cnt = 0;
-        double q = d[0] - mid;
-        if (fabs(q) < pivmin) q = -pivmin;
-        cnt += q < 0.0;
-        for (int i = 1; i < n; ++i) {
-            q = (d[i] - mid) - e[i - 1] * e[i - 1] / q;
-            if (fabs(q) < pivmin) q = -pivmin;
-            cnt += q < 0.0;
-        }
-        if (cnt > k)
-            hi = mid;
-        else
-            lo = mid;
-    }
-    W[k] = (T)ldexp(0.5 * (lo + hi), *scale_exp);
+    W[k] = (T)ldexp(dc::sturm_kth(n, d, e, k, lo, hi, pivmin), *scale_exp);
 }
 
 // ---- 3b. divide and conquer --------------------------------------------------

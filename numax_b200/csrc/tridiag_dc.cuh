@@ -228,5 +228,51 @@ __host__ __device__ inline int merged_rank(int k, int ndef, const double *dl, co
     return r;
 }
 
+// Eigenvalue k (0-based, ascending) of the symmetric tridiagonal (d, e),
+// e[i] coupling i and i+1, inside [lo, hi] (which must hold it), by
+// multisection on the Sturm count -- the number of negative pivots of
+// T - x I, i.e. of eigenvalues below x.  Each pass counts at three interior
+// points at once (three independent division chains) and keeps the quarter
+// holding eigenvalue k, until the interval is 2 eps max(|lo|, |hi|) + pivmin
+// wide; a pivot smaller than pivmin in magnitude is replaced by -pivmin.
+__host__ __device__ inline double sturm_kth(int n, const double *d, const double *e, int k,
+                                            double lo, double hi, double pivmin) {
+    for (int it = 0; it < 128; ++it) {
+        if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+        const double w = hi - lo;
+        const double x0 = lo + 0.25 * w, x1 = lo + 0.5 * w, x2 = lo + 0.75 * w;
+        if (!(lo < x0 && x0 < x1 && x1 < x2 && x2 < hi)) break;
+        double q0 = d[0] - x0, q1 = d[0] - x1, q2 = d[0] - x2;
+        if (fabs(q0) < pivmin) q0 = -pivmin;
+        if (fabs(q1) < pivmin) q1 = -pivmin;
+        if (fabs(q2) < pivmin) q2 = -pivmin;
+        int c0 = q0 < 0.0, c1 = q1 < 0.0, c2 = q2 < 0.0;
+        for (int i = 1; i < n; ++i) {
+            const double e2 = e[i - 1] * e[i - 1];
+            q0 = (d[i] - x0) - e2 / q0;
+            q1 = (d[i] - x1) - e2 / q1;
+            q2 = (d[i] - x2) - e2 / q2;
+            if (fabs(q0) < pivmin) q0 = -pivmin;
+            if (fabs(q1) < pivmin) q1 = -pivmin;
+            if (fabs(q2) < pivmin) q2 = -pivmin;
+            c0 += q0 < 0.0;
+            c1 += q1 < 0.0;
+            c2 += q2 < 0.0;
+        }
+        if (c0 > k) {
+            hi = x0;
+        } else if (c1 > k) {
+            lo = x0;
+            hi = x1;
+        } else if (c2 > k) {
+            lo = x1;
+            hi = x2;
+        } else {
+            lo = x2;
+        }
+    }
+    return 0.5 * (lo + hi);
+}
+
 }  // namespace dc
 }  // namespace nmx

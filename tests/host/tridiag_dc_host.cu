@@ -113,3 +113,20 @@ extern "C" int dc_host_solve(int n, const double *d0, const double *e0, double *
     std::memcpy(Z, Q.data(), sizeof(double) * (size_t)n * n);
     return 0;
 }
+
+// Every eigenvalue of (d, e[0 .. n-2]) by dc::sturm_kth, as the values-only
+// kernel computes them (one call per k, Gershgorin interval).
+extern "C" void sturm_host_values(int n, const double *d, const double *e, double *W) {
+    double lo = d[0], hi = d[0], emax2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double r = (i > 0 ? std::fabs(e[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(e[i]) : 0.0);
+        lo = std::fmin(lo, d[i] - r);
+        hi = std::fmax(hi, d[i] + r);
+        if (i + 1 < n) emax2 = std::fmax(emax2, e[i] * e[i]);
+    }
+    const double pivmin = 2.2250738585072014e-308 * std::fmax(1.0, emax2);
+    const double tnorm = std::fmax(std::fabs(lo), std::fabs(hi));
+    lo -= 2.0 * kEps * tnorm * n + pivmin;
+    hi += 2.0 * kEps * tnorm * n + pivmin;
+    for (int k = 0; k < n; ++k) W[k] = sturm_kth(n, d, e, k, lo, hi, pivmin);
+}

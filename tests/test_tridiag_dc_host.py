@@ -70,3 +70,22 @@ def test_divide_and_conquer_matches_lapack(dc, name, d, e):
     assert np.abs(z.T @ z - np.eye(n)).max() < 1e-13
     assert np.abs(T @ z - z * w).max() / scale < 1e-13
     assert it <= 60  # the one-pole rational steps converge in a handful
+
+
+@pytest.mark.parametrize("name,d,e", [c for c in cases() if c[0] not in ("huge", "tiny")],
+                         ids=[c[0] for c in cases() if c[0] not in ("huge", "tiny")])
+def test_sturm_multisection_matches_lapack(dc, name, d, e):
+    """The values-only path's multisection (sturm_kth): every eigenvalue to
+    a few ulps of max |lambda| (the kernel runs it on the scaled matrix, so
+    the extreme-scale cases are the scaling's business, not the count's)."""
+    n = len(d)
+    T = np.diag(d) + np.diag(e[:n - 1], 1) + np.diag(e[:n - 1], -1)
+    dd = np.ascontiguousarray(d, dtype=np.float64)
+    ee = np.ascontiguousarray(np.concatenate([e[:n - 1], [0.0]]), dtype=np.float64)
+    w = np.zeros(n)
+    dc.sturm_host_values(n, dd.ctypes.data_as(C.c_void_p), ee.ctypes.data_as(C.c_void_p),
+                         w.ctypes.data_as(C.c_void_p))
+    want = np.linalg.eigvalsh(T)
+    scale = max(np.abs(want).max(), np.finfo(float).tiny)
+    assert np.all(np.diff(w) >= 0)
+    assert np.abs(w - want).max() / scale < 1e-13
