@@ -101,7 +101,7 @@ __global__ void sym_lower_kernel(const T *A, int64_t lda, int n, double *W, int6
 
 constexpr int kLrdNb = 32;              // panel width (columns per launch)
 constexpr int kLrdVec = 2 * kLrdNb + 1;  // W^T v, V^T v and y . v: one round's sums
-constexpr int kLrdSub = 4;              // threads per value in the cross-CTA sum
+constexpr int kLrdSub = 7;              // threads per value in the cross-CTA sum (65 x 7 <= 512)
 
 struct LrdArgs {
     double *A;  // the symmetric work matrix (full storage), scaled
@@ -291,10 +291,24 @@ __global__ void __launch_bounds__(kTrdThreads, 1) latrd_kernel(LrdArgs a) {
                 a.A[(int64_t)r * lda + j] = r == j + 1 ? beta : v;  // the reflector's storage
             }
         }
-        red[warp][lane] = lane < i ? t1 : 0.0;
-        red[warp][kLrdNb + lane] = lane < i ? t2 : 0.0;
-        if (lane == 0) red[warp][2 * kLrdNb] = yv;
-        if (!lrd_round(a, gen, kLrdVec, red, sub, tot, &s_flag)) return;
+        // The round's vector holds only what is nonzero: W^T v (i values),
+        // V^T v (i values), y . v.
+        if (lane < i) {
+            red[warp][lane] = t1;
+            red[warp][i + lane] = t2;
+        }
+        if (lane == 0) red[warp][2 * i] = yv;
+        if (!lrd_round(a, gen, 2 * i + 1, red, sub, tot, &s_flag)) return;
+        if (threadIdx.x < kLrdNb) {
+            const double u1 = threadIdx.x < i ? tot[threadIdx.x] : 0.0;
+            const double u2 = threadIdx.x < i ? tot[i + threadIdx.x] : 0.0;
+            const double yvt = tot[2 * i];
+            __syncwarp();
+            tot[threadIdx.x] = u1;
+            tot[kLrdNb + threadIdx.x] = u2;
+            if (threadIdx.x == 0) tot[2 * kLrdNb] = yvt;
+        }
+        __syncthreads();
 
         // w on the owned rows.
         double t12 = 0.0;
