@@ -217,3 +217,13 @@ def test_save_rejects_bfloat16(npx, tmp_path):
     np.save(p, np.zeros(3, np.float32))
     with pytest.raises(NpyError, match="bfloat16 has no NumPy dtype"):
         npx.load(p, torch.bfloat16, 3)
+
+
+def test_save_of_a_strided_tensor_writes_its_c_order(npx, tmp_path):
+    # numax writes a tensor in row-major order whatever its view; a
+    # transposed torch view is saved as its C-order copy.
+    a = torch.arange(12, dtype=torch.float64).reshape(3, 4).t()
+    p = tmp_path / "t.npy"
+    npx.save(a, p)
+    assert p.read_bytes() == np_bytes(np.ascontiguousarray(a.numpy()))
+    assert npx.load(p, torch.float64, 4, 3).tolist() == a.tolist()
